@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""FP64-accurate GEMM throughput on B200: emulated DGEMM (Ozaki INT8 slices on tcgen05)
+next to the native FP64 DMMA kernel, at M = N = K = 8192.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--r R]
+
+One step = one C = A*B product (NN, column-major, alpha = 1, beta = 0) of 8192^3 with
+entries u*2^e, u ~ U[-1,1], e ~ U{-r..r} (r = 0 by default), through the library's
+public entry points:
+  * value: eb2_dgemm_device on device-resident inputs (the product path with its
+    a-posteriori accuracy check), device time from CUDA events on the launching stream,
+    max over ranks;
+  * e2e:   dgemm_ (the Fortran BLAS ABI Eigen binds) on pinned host buffers: the H2D copy
+    of A and B, the product and the D2H copy of C are inside the timed region;
+  * roofline: the main tcgen05 GEMM kernel, timed by CUDA events recorded around it on
+    its own stream;
+  * cpu_baseline: Eigen's own multithreaded CPU GEMM (operator*, OpenMP) built from the
+    reference sources (oracle/_ref), on a bounded sample, rank 0 only.
+Multi-GPU: replicas only (every rank computes its own product; no collective on the data
+path); the barrier and the MAX over ranks of the step time use NCCL.
+`--impl reference` times the reference's CPU implementation on the same config.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import datetime
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "FP64-accurate GEMM TFLOP/s (emulated vs native, 8192^3); grouped-batch GFLOP/s"
+UNIT = "TFLOP/s"
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_BF16_TFLOPS = 1590.0
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=8192)
+    ap.add_argument("--r", type=int, default=0, help="exponent range of the synthetic entries")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-native", action="store_true")
+    a = ap.parse_args()
+    a.warmup = max(a.warmup, 3)
+    a.steps = max(a.steps, 1)
+    return a
+
+
+def workload_config(a) -> dict:
+    s = a.size
+    return {
+        "workload": f"emulated DGEMM {s}^3 NN column-major, alpha=1, beta=0, entries u*2^e (u~U[-1,1], e~U{{-{a.r}..{a.r}}})",
+        "m": s, "n": s, "k": s, "dtype_inputs": "f64", "exponent_range_r": a.r,
+        "l2": f"inputs larger than L2 ({s * s * 8 / 1e6:.0f} MB per operand vs 126 MB L2), no flush",
+        "parallelism": f"replicas x{a.gpus}",
+    }
+
+
+# ------------------------------------------------------------------------ distributed
+def dist_setup(a):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def host_cpu_info():
+    model, flags = "unknown", ""
+    try:
+        txt = Path("/proc/cpuinfo").read_text()
+        m = re.search(r"^model name\s*:\s*(.*)$", txt, re.M)
+        model = m.group(1).strip() if m else model
+        f = re.search(r"^flags\s*:\s*(.*)$", txt, re.M)
+        flags = f.group(1) if f else ""
+    except OSError:
+        pass
+    return model, flags
+
+
+def ref_bench_binary():
+    _, flags = host_cpu_info()
+    v4 = ROOT / "oracle" / "_ref" / "eigen_ref_bench_v4"
+    v3 = ROOT / "oracle" / "_ref" / "eigen_ref_bench_v3"
+    if "avx512f" in flags.split() and v4.exists():
+        return v4
+    return v3 if v3.exists() else None
+
+
+def run_ref_bench(args_list, timeout=600):
+    exe = ref_bench_binary()
+    if exe is None:
+        return None, "oracle/_ref/eigen_ref_bench_* not built (make -C oracle ref)"
+    env = dict(os.environ)
+    threads = os.cpu_count() or 1
+    env.setdefault("OMP_NUM_THREADS", str(threads))
+    r = subprocess.run([str(exe), *args_list], capture_output=True, text=True, timeout=timeout, env=env)
+    if r.returncode != 0:
+        return None, f"eigen_ref_bench failed: {r.stderr.strip()[:200]}"
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1]
+    return json.loads(line), None
+
+
+def cpu_sample(a, reps, warmup):
+    """Eigen operator* on the box's cores: the full M=N=size product with K cut so one
+    repetition stays near a second; throughput (TFLOP/s) is what is compared."""
+    probe, err = run_ref_bench(["--mode", "gemm", "--m", str(a.size), "--n", str(a.size), "--k", "256", "--reps", "1",
+                                "--warmup", "1"])
+    if probe is None:
+        return None, err
+    gflops = max(probe["gflops"], 1.0)
+    k_for_1s = int(gflops * 1e9 / (2.0 * a.size * a.size))
+    k = max(256, min(a.size, (k_for_1s // 256) * 256))
+    res, err = run_ref_bench(["--mode", "gemm", "--m", str(a.size), "--n", str(a.size), "--k", str(k), "--reps",
+                              str(reps), "--warmup", str(warmup), "--max-seconds", "25"])
+    if res is None:
+        return None, err
+    res["k_sample"] = k
+    return res, None
+
+
+# ------------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_id: str | None):
+        self.proc = None
+        self.out = None
+        self.device_id = device_id
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.device_id:
+            cmd += ["-i", self.device_id]
+        try:
+            self.out = open(os.devnull, "w") if False else None
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        rows = [r.split(",") for r in out.strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
+        loaded = sorted(sm)[len(sm) // 2:] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------ peaks / profiles
+def peaks():
+    try:
+        p = json.loads(PEAKS_FILE.read_text())
+        return float(p["bf16_tflops"]), float(p["bf16_tflops_sustained"]), float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_BF16_TFLOPS, 1400.0, FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(size: int):
+    """DRAM bytes per launch of the main GEMM kernel from the committed ncu summary
+    (profiles/ozaki_gemm_i8.md: 'dram_bytes_per_launch: <bytes> at <size>')."""
+    f = ROOT / "profiles" / "ozaki_gemm_i8.md"
+    try:
+        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)\s*at\s*(\d+)", f.read_text())
+    except OSError:
+        return None
+    if not m:
+        return None
+    b, at = float(m.group(1)), int(m.group(2))
+    return b * (size / at) ** 3 if at != size else b
+
+
+# ------------------------------------------------------------------------ arms
+def reference_arm(a, world, rank):
+    cfg = workload_config(a)
+    if rank != 0:
+        return 0
+    model, _ = host_cpu_info()
+    res, err = run_ref_bench(["--mode", "gemm", "--m", str(a.size), "--n", str(a.size), "--k", "256", "--reps", "1"])
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return 0
+    gflops = max(res["gflops"], 1.0)
+    k = max(256, min(a.size, (int(gflops * 1e9 / (2.0 * a.size * a.size)) // 256) * 256))
+    res, err = run_ref_bench(["--mode", "gemm", "--m", str(a.size), "--n", str(a.size), "--k", str(k), "--reps",
+                              str(a.steps), "--warmup", str(a.warmup), "--max-seconds", "150"])
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return 0
+    tflops = res["gflops"] / 1e3
+    sample = (f"Eigen operator* (OpenMP, {res['threads']} threads, {model}) on {a.size}x{a.size}x{k} per step "
+              f"(K cut from {a.size} to bound the step), {res['reps']} steps, median")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(tflops, 4), "unit": UNIT, "n_gpus": a.gpus,
+        "steps": res["reps"], "warmup": a.warmup, "ms_per_step": round(res["seconds_median"] * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": cfg,
+        "cpu_baseline": {"value": round(tflops, 4), "unit": UNIT, "cores": res["threads"], "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(tflops, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def our_arm(a, world, rank, local):
+    import torch
+    import torch.distributed as dist
+
+    import eigen_b200 as eb
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    props = torch.cuda.get_device_properties(dev)
+    pci = None
+    if hasattr(props, "pci_bus_id"):
+        pci = f"{getattr(props, 'pci_domain_id', 0):08X}:{props.pci_bus_id:02X}:{getattr(props, 'pci_device_id', 0):02X}.0"
+    eb.load()
+    S = a.size
+    flops = 2.0 * S ** 3
+    g = torch.Generator(device=dev)
+    g.manual_seed(1234 + rank)
+
+    def synth(rows, cols):
+        # column-major rows x cols == row-major (cols, rows) tensor
+        x = torch.rand((cols, rows), dtype=torch.float64, device=dev, generator=g) * 2 - 1
+        if a.r:
+            e = torch.randint(-a.r, a.r + 1, (cols, rows), device=dev, generator=g, dtype=torch.int32)
+            x = torch.ldexp(x, e.to(torch.float64))
+        return x
+
+    A = synth(S, S)
+    B = synth(S, S)
+    C = torch.zeros((S, S), dtype=torch.float64, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    eb.set_dgemm_method(eb.METHOD_AUTO)
+    eb.set_timing(True)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def run_device(method, steps):
+        eb.set_dgemm_method(method)
+        infos = []
+        with torch.cuda.stream(stream):
+            for _ in range(a.warmup):
+                rc = eb.dgemm_device("N", "N", S, S, S, 1.0, A, S, B, S, 0.0, C, S, stream=stream.cuda_stream,
+                                     check_accuracy=True)
+                assert rc == eb.EB2_OK, eb.last_error()
+            stream.synchronize()
+            barrier()
+            torch.cuda.synchronize()
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            for _ in range(steps):
+                rc = eb.dgemm_device("N", "N", S, S, S, 1.0, A, S, B, S, 0.0, C, S, stream=stream.cuda_stream,
+                                     check_accuracy=True)
+                assert rc == eb.EB2_OK, eb.last_error()
+                infos.append(eb.last_call_info())
+            ev1.record(stream)
+            stream.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / steps
+        return ms, infos
+
+    clocks = ClockSampler(pci)
+    clocks.start()
+    time.sleep(0.3)
+    ms_emu, infos = run_device(eb.METHOD_AUTO, a.steps)
+    clk = clocks.stop()
+    ms_emu_max = max_over_ranks(ms_emu)
+    C_emu = C.clone()
+    gemm_ms = [i["gemm_kernel_ms"] for i in infos if i["gemm_kernel_ms"] > 0]
+    gemm_ms_avg = max_over_ranks(sum(gemm_ms) / len(gemm_ms)) if gemm_ms else None
+    slices = infos[-1]["slices"]
+    launches = sum(i["launches"] for i in infos)
+
+    native = None
+    if not a.no_native:
+        nsteps = min(a.steps, 5)
+        ms_nat, _ = run_device(eb.METHOD_NATIVE, nsteps)
+        ms_nat = max_over_ranks(ms_nat)
+        diff = float(torch.linalg.norm(C_emu - C) / torch.linalg.norm(C))
+        native = {"tflops": round(world * flops / (ms_nat * 1e-3) / 1e12, 3), "ms_per_step": round(ms_nat, 3),
+                  "steps": nsteps, "kernel": "dgemm_dmma (mma.sync f64)", "rel_diff_emulated_vs_native": diff}
+        eb.set_dgemm_method(eb.METHOD_AUTO)
+
+    e2e = None
+    if not a.no_e2e:
+        hA = torch.empty((S, S), dtype=torch.float64, pin_memory=True)
+        hB = torch.empty((S, S), dtype=torch.float64, pin_memory=True)
+        hC = torch.empty((S, S), dtype=torch.float64, pin_memory=True)
+        hA.copy_(A)
+        hB.copy_(B)
+        e2e_steps = min(a.steps, 5)
+        for _ in range(1):
+            eb.dgemm("N", "N", S, S, S, 1.0, hA, S, hB, S, 0.0, hC, S)
+        barrier()
+        times = []
+        for _ in range(e2e_steps):
+            t0 = time.perf_counter()
+            eb.dgemm("N", "N", S, S, S, 1.0, hA, S, hB, S, 0.0, hC, S)
+            times.append(time.perf_counter() - t0)
+        barrier()
+        t_step = max_over_ranks(sum(times) / len(times))
+        e2e = {"value": round(world * flops / t_step / 1e12, 3), "unit": UNIT,
+               "h2d_bytes_per_step": 2 * S * S * 8, "d2h_bytes_per_step": S * S * 8,
+               "ms_per_step": round(t_step * 1e3, 3), "steps": e2e_steps,
+               "api": "dgemm_ (Fortran BLAS ABI) on pinned host buffers; synchronous call timed on the host"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        model, _ = host_cpu_info()
+        res, err = cpu_sample(a, reps=3, warmup=1)
+        if res is not None:
+            cpu = {"value": round(res["gflops"] / 1e3, 4), "unit": UNIT, "cores": res["threads"], "kind": "reference",
+                   "sample": f"Eigen operator* (OpenMP, {model}) on {S}x{S}x{res['k_sample']} DGEMM, "
+                             f"{res['reps']} reps median after 1 warm-up"}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": err}
+
+    bf16, bf16_sus, hbm, basis = peaks()
+    products = slices * (slices + 1) // 2
+    roof = None
+    if gemm_ms_avg:
+        achieved = flops / (gemm_ms_avg * 1e-3) / 1e12  # FP64-equivalent TFLOP/s of the GEMM kernel
+        int8_peak = 2.0 * bf16  # dense int8 rate is twice the dense bf16 rate on sm_100
+        peak = int8_peak / products  # the FP64-equivalent ceiling of an int8 kernel doing `products` GEMMs
+        roof = {"bound": "tensor", "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": UNIT,
+                "frac": round(achieved / peak, 4), "traffic": profiled_traffic(S),
+                "kernel": f"ozaki_gemm_kernel<256,4> (tcgen05.mma kind::i8), {gemm_ms_avg:.3f} ms/launch",
+                "pipe": {"achieved_tops": round(achieved * products, 1), "peak_tops": round(int8_peak, 1),
+                         "basis": f"peak = 2 x {basis} dense bf16 ({bf16} TFLOP/s burst), of {basis}; "
+                                  f"{products} int8 slice products of 2*M*N*K each"}}
+
+    value = world * flops / (ms_emu_max * 1e-3) / 1e12
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(ms_emu_max, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int8 slices (s32 accumulate) -> f64", "data": "synthetic",
+            "config": dict(workload_config(a), slices=slices, tile_n=infos[-1]["tile_n"],
+                           err_estimate=infos[-1]["err_estimate"], escalations=infos[-1]["escalations"]),
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk, "native_fp64": native,
+            "emulated_over_native": round(value / native["tflops"], 3) if native else None,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = parse_args()
+    world, rank, local = dist_setup(a)
+    if a.impl == "reference":
+        return reference_arm(a, world, rank)
+    return our_arm(a, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,185 @@
+"""eigen_b200 -- B200 (sm_100a) drop-in for Eigen's dense matrix-matrix product.
+
+The product is the C-ABI shared library ``lib/libeigen_b200.so`` (built by
+``python -m eigen_b200.build``).  It exports the Fortran BLAS symbols ``sgemm_`` /
+``dgemm_`` (and ILP64 ``_64_`` variants) that Eigen binds for its ``operator*``
+under ``EIGEN_USE_BLAS`` (Eigen/src/Core/products/GeneralMatrixMatrix_BLAS.h:53-118),
+plus ``eb2_*`` extension calls.  This module is a thin ctypes mirror of that ABI
+for Python callers, tests and benchmarks: the call ``dgemm(...)`` takes the same
+arguments, in the same order and with the same meaning, as Eigen's
+``dgemm_`` (blas/level3_impl.h:12-96), and argument errors surface the same way,
+through ``xerbla_``.
+
+Nothing here computes a product: if the library is missing, loading fails.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "lib" / "libeigen_b200.so"
+HEADER_PATH = _PKG.parent / "include" / "eigen_b200" / "blas.h"
+
+EB2_OK = 0
+EB2_ERR_CUDA = -1
+EB2_ERR_ALLOC = -2
+EB2_ERR_TIMEOUT = -3
+EB2_ERR_ARG = -4
+EB2_ERR_NO_DEVICE = -5
+EB2_ERR_ACCURACY = -6
+
+METHOD_AUTO = 0
+METHOD_NATIVE = 1
+METHOD_EMULATED = 2
+
+_lib = None
+
+
+class CallInfo(ctypes.Structure):
+    _fields_ = [
+        ("dtype", ctypes.c_int),
+        ("method", ctypes.c_int),
+        ("slices", ctypes.c_int),
+        ("tile_n", ctypes.c_int),
+        ("escalations", ctypes.c_int),
+        ("nonfinite", ctypes.c_int),
+        ("staged", ctypes.c_int),
+        ("err_estimate", ctypes.c_double),
+        ("kernel_ms", ctypes.c_double),
+        ("gemm_kernel_ms", ctypes.c_double),
+        ("launches", ctypes.c_int),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {f: getattr(self, f) for f, _ in self._fields_}
+        d["dtype"] = chr(self.dtype) if self.dtype else ""
+        return d
+
+
+def load(path: str | os.PathLike | None = None, mode: int = ctypes.RTLD_GLOBAL) -> ctypes.CDLL:
+    """Load libeigen_b200.so (once) and declare its signatures.  Raises if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is missing: build it with `python -m eigen_b200.build`")
+    lib = ctypes.CDLL(str(p), mode=mode)
+    c_int_p = ctypes.POINTER(ctypes.c_int)
+    c_i64_p = ctypes.POINTER(ctypes.c_int64)
+    vp = ctypes.c_void_p
+    for name, ip in (("dgemm_", c_int_p), ("sgemm_", c_int_p), ("dgemm_64_", c_i64_p), ("sgemm_64_", c_i64_p)):
+        f = getattr(lib, name)
+        f.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ip, ip, ip, vp, vp, ip, vp, ip, vp, vp, ip]
+        f.restype = None
+    lib.eb2_set_dgemm_method.argtypes = [ctypes.c_int]
+    lib.eb2_set_sgemm_method.argtypes = [ctypes.c_int]
+    lib.eb2_set_dgemm_slices.argtypes = [ctypes.c_int]
+    lib.eb2_set_dgemm_tolerance.argtypes = [ctypes.c_double]
+    lib.eb2_set_tile_n.argtypes = [ctypes.c_int]
+    lib.eb2_set_timing.argtypes = [ctypes.c_int]
+    lib.eb2_last_error_string.restype = ctypes.c_char_p
+    lib.eb2_last_call_info.argtypes = [ctypes.POINTER(CallInfo)]
+    lib.eb2_version.restype = ctypes.c_char_p
+    lib.eb2_dgemm_device.argtypes = [ctypes.c_char, ctypes.c_char, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                     ctypes.c_double, vp, ctypes.c_int64, vp, ctypes.c_int64, ctypes.c_double, vp,
+                                     ctypes.c_int64, vp, ctypes.c_int]
+    lib.eb2_sgemm_device.argtypes = [ctypes.c_char, ctypes.c_char, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                     ctypes.c_float, vp, ctypes.c_int64, vp, ctypes.c_int64, ctypes.c_float, vp,
+                                     ctypes.c_int64, vp]
+    _lib = lib
+    return lib
+
+
+def _ptr(x) -> int | None:
+    """Address of a numpy array, torch tensor, or a raw integer address."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return int(x.data_ptr())
+    if hasattr(x, "ctypes"):
+        return int(x.ctypes.data)
+    raise TypeError(f"cannot take the address of {type(x)!r}")
+
+
+def _gemm(name, ctype, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, ilp64=False):
+    lib = load()
+    it = ctypes.c_int64 if ilp64 else ctypes.c_int
+    f = getattr(lib, name + ("_64_" if ilp64 else "_"))
+    ta = transa.encode() if isinstance(transa, str) else bytes(transa)
+    tb = transb.encode() if isinstance(transb, str) else bytes(transb)
+    al, be = ctype(alpha), ctype(beta)
+    args = [it(v) for v in (m, n, k, lda, ldb, ldc)]
+    f(ta, tb, ctypes.byref(args[0]), ctypes.byref(args[1]), ctypes.byref(args[2]), ctypes.cast(ctypes.byref(al), ctypes.c_void_p),
+      _ptr(a), ctypes.byref(args[3]), _ptr(b), ctypes.byref(args[4]), ctypes.cast(ctypes.byref(be), ctypes.c_void_p), _ptr(c),
+      ctypes.byref(args[5]))
+
+
+def dgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, ilp64=False):
+    """C := alpha*op(A)*op(B) + beta*C through the exported ``dgemm_`` (column-major).
+
+    a, b, c: numpy arrays / torch tensors (host or CUDA) or raw addresses."""
+    _gemm("dgemm", ctypes.c_double, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, ilp64)
+
+
+def sgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, ilp64=False):
+    """Single-precision counterpart through ``sgemm_``."""
+    _gemm("sgemm", ctypes.c_float, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, ilp64)
+
+
+def dgemm_device(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream=0, check_accuracy=True) -> int:
+    """Stream-ordered DGEMM on device pointers (``eb2_dgemm_device``); returns an EB2_* status."""
+    return load().eb2_dgemm_device(transa.encode(), transb.encode(), m, n, k, alpha, _ptr(a), lda, _ptr(b), ldb, beta,
+                                   _ptr(c), ldc, stream or None, 1 if check_accuracy else 0)
+
+
+def sgemm_device(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream=0) -> int:
+    return load().eb2_sgemm_device(transa.encode(), transb.encode(), m, n, k, alpha, _ptr(a), lda, _ptr(b), ldb, beta,
+                                   _ptr(c), ldc, stream or None)
+
+
+def set_dgemm_method(method: int) -> int:
+    return load().eb2_set_dgemm_method(method)
+
+
+def set_sgemm_method(method: int) -> int:
+    return load().eb2_set_sgemm_method(method)
+
+
+def set_dgemm_slices(slices: int) -> int:
+    return load().eb2_set_dgemm_slices(slices)
+
+
+def set_dgemm_tolerance(tol: float) -> int:
+    return load().eb2_set_dgemm_tolerance(tol)
+
+
+def set_tile_n(tile_n: int) -> int:
+    return load().eb2_set_tile_n(tile_n)
+
+
+def set_timing(on: bool) -> int:
+    return load().eb2_set_timing(1 if on else 0)
+
+
+def last_error() -> tuple[int, str]:
+    lib = load()
+    return lib.eb2_last_error(), lib.eb2_last_error_string().decode()
+
+
+def clear_error() -> None:
+    load().eb2_clear_error()
+
+
+def last_call_info() -> dict:
+    ci = CallInfo()
+    load().eb2_last_call_info(ctypes.byref(ci))
+    return ci.as_dict()
+
+
+def version() -> str:
+    return load().eb2_version().decode()

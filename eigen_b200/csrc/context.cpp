@@ -1,0 +1,128 @@
+// context.cpp -- see context.h.
+#include "context.h"
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+namespace eb2 {
+
+namespace {
+thread_local int t_error = EB2_OK;
+thread_local char t_message[512] = "";
+thread_local eb2_call_info t_info = {0, 0, 0, 0, 0, 0, 0, -1.0, -1.0, -1.0, 0};
+thread_local Context* t_pending = nullptr;
+thread_local bool t_pending_gemm = false;
+
+constexpr int kMaxDevices = 64;
+std::mutex g_ctx_mu;
+Context* g_ctx[kMaxDevices] = {};
+}  // namespace
+
+Settings& settings() {
+  static Settings s;
+  return s;
+}
+
+void set_error(int code, const char* fmt, ...) {
+  t_error = code;
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(t_message, sizeof(t_message), fmt, ap);
+  va_end(ap);
+}
+
+int last_error() { return t_error; }
+const char* last_error_string() { return t_message; }
+eb2_call_info& call_info() { return t_info; }
+
+void set_pending_timing(Context* cx, bool gemm_timed) {
+  t_pending = cx;
+  t_pending_gemm = gemm_timed;
+}
+
+void resolve_timing() {
+  Context* cx = t_pending;
+  if (!cx) return;
+  t_pending = nullptr;
+  float ms = 0.f;
+  if (cudaEventSynchronize(cx->ev_stop) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return;
+  }
+  if (cudaEventElapsedTime(&ms, cx->ev_start, cx->ev_stop) == cudaSuccess) t_info.kernel_ms = ms;
+  if (t_pending_gemm && cudaEventElapsedTime(&ms, cx->ev_gemm0, cx->ev_gemm1) == cudaSuccess) t_info.gemm_kernel_ms = ms;
+  (void)cudaGetLastError();
+}
+
+bool DeviceBuffer::ensure(size_t bytes) {
+  if (bytes <= cap) return true;
+  const size_t gran = size_t(2) << 20;
+  size_t want = bytes + bytes / 8;
+  want = (want + gran - 1) / gran * gran;
+  void* p = nullptr;
+  if (cudaMalloc(&p, want) != cudaSuccess) {
+    (void)cudaGetLastError();
+    want = (bytes + gran - 1) / gran * gran;
+    if (cudaMalloc(&p, want) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return false;
+    }
+  }
+  if (ptr) cudaFree(ptr);  // implicitly waits for work still using the old buffer
+  ptr = p;
+  cap = want;
+  return true;
+}
+
+Context* current_context() {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    (void)cudaGetLastError();
+    set_error(EB2_ERR_NO_DEVICE, "no CUDA device is available");
+    return nullptr;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    (void)cudaGetLastError();
+    set_error(EB2_ERR_NO_DEVICE, "cudaGetDevice failed");
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(g_ctx_mu);
+  if (g_ctx[dev]) return g_ctx[dev];
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    set_error(EB2_ERR_NO_DEVICE, "cudaGetDeviceProperties failed for device %d", dev);
+    return nullptr;
+  }
+  if (prop.major != 10 || prop.minor != 0) {
+    set_error(EB2_ERR_NO_DEVICE, "device %d is sm_%d%d; this library is built for sm_100a (B200) only", dev,
+              prop.major, prop.minor);
+    return nullptr;
+  }
+  Context* c = new Context();
+  c->device = dev;
+  c->num_sms = prop.multiProcessorCount;
+  c->cc_major = prop.major;
+  c->cc_minor = prop.minor;
+  bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess;
+  ok = ok && cudaEventCreate(&c->ev_start) == cudaSuccess;
+  ok = ok && cudaEventCreate(&c->ev_stop) == cudaSuccess;
+  ok = ok && cudaEventCreate(&c->ev_gemm0) == cudaSuccess;
+  ok = ok && cudaEventCreate(&c->ev_gemm1) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->dflags, sizeof(DeviceFlags)) == cudaSuccess;
+  ok = ok && cudaHostAlloc(&c->hflags, sizeof(DeviceFlags), cudaHostAllocDefault) == cudaSuccess;
+  if (!ok) {
+    set_error(EB2_ERR_CUDA, "creating the device context failed: %s", cudaGetErrorString(cudaGetLastError()));
+    delete c;  // the few handles that were created are reclaimed at process exit
+    return nullptr;
+  }
+  std::memset(c->hflags, 0, sizeof(DeviceFlags));
+  g_ctx[dev] = c;
+  return c;
+}
+
+}  // namespace eb2
+
+extern "C" const char* eb2_last_error_string(void) { return eb2::last_error_string(); }

@@ -1,0 +1,70 @@
+// context.h -- per-device state of the library: the stream BLAS calls run on,
+// grow-only device workspaces, the small device/pinned flag block the kernels
+// report through, and the thread-local error / call-info records.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+
+#include "eigen_b200/blas.h"
+
+namespace eb2 {
+
+// Grow-only device allocation (never shrinks; freed at process exit).
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t cap = 0;
+  // Returns false (and leaves the old buffer) if the allocation fails.
+  bool ensure(size_t bytes);
+};
+
+// Flags the kernels write; mirrored into pinned host memory after a call.
+struct DeviceFlags {
+  int nonfinite;
+  uint32_t status;
+  double err_sq[2];
+};
+
+struct Context {
+  int device = -1;
+  int num_sms = 0;
+  int cc_major = 0, cc_minor = 0;
+  cudaStream_t stream = nullptr;  // stream of the synchronous BLAS entry points
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;  // around all product kernels
+  cudaEvent_t ev_gemm0 = nullptr, ev_gemm1 = nullptr;  // around the main GEMM kernel
+  std::mutex mu;                  // one product at a time per device
+  DeviceBuffer ws;                // emulation workspace (digits, exponents, scan results)
+  DeviceBuffer stage_a, stage_b, stage_c;  // device copies of host operands
+  DeviceFlags* dflags = nullptr;  // device
+  DeviceFlags* hflags = nullptr;  // pinned host mirror
+};
+
+// Context of the calling thread's current device, created on first use.
+// Returns nullptr (and sets the thread's error) when no usable device exists.
+Context* current_context();
+
+struct Settings {
+  std::atomic<int> dgemm_method{EB2_METHOD_AUTO};
+  std::atomic<int> sgemm_method{EB2_METHOD_AUTO};
+  std::atomic<int> dgemm_slices{0};
+  std::atomic<int> tile_n{0};
+  std::atomic<double> dgemm_tol{1.1102230246251565e-16};  // 2^-53
+  std::atomic<int> timing{0};
+};
+Settings& settings();
+
+// Thread-local sticky error.
+void set_error(int code, const char* fmt, ...);
+int last_error();
+const char* last_error_string();
+eb2_call_info& call_info();
+// The context whose events hold the calling thread's last timed call (or null);
+// `gemm_timed` tells whether ev_gemm0/ev_gemm1 bracket a kernel in that call.
+void set_pending_timing(Context* cx, bool gemm_timed);
+// Resolves pending event times into call_info() (waits for the events).
+void resolve_timing();
+
+}  // namespace eb2

@@ -1,0 +1,258 @@
+// gemm_driver.cpp -- device-level product drivers: choose the method, lay out the
+// workspace, launch the kernels in order and run the a-posteriori accuracy check.
+//
+// The role matches Eigen's general_matrix_matrix_product<...>::run
+// (Eigen/src/Core/products/GeneralMatrixMatrix.h:119-246) plus the blocking choice
+// of computeProductBlockingSizes (Eigen/src/Core/products/GeneralBlockPanelKernel.h:202-452):
+// here "blocking" is the tcgen05 tile width and the number of digit slices.
+#include "gemm_driver.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "kernels.h"
+
+namespace eb2 {
+
+namespace {
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+bool check_cuda(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return true;
+  (void)cudaGetLastError();
+  set_error(EB2_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return false;
+}
+
+// Views of op(A) (m x k) and op(B)^T (n x k): row r, column l (l runs along K).
+StridedView<double> view_a(bool ta, const double* A, int64_t lda, int64_t m, int64_t k) {
+  // op(A)(i,l) = A[i + l*lda] (N) or A[l + i*lda] (T)
+  return ta ? StridedView<double>{A, m, k, lda, 1} : StridedView<double>{A, m, k, 1, lda};
+}
+StridedView<double> view_bt(bool tb, const double* B, int64_t ldb, int64_t n, int64_t k) {
+  // op(B)(l,j) = B[l + j*ldb] (N) or B[j + l*ldb] (T); row j of op(B)^T
+  return tb ? StridedView<double>{B, n, k, 1, ldb} : StridedView<double>{B, n, k, ldb, 1};
+}
+
+}  // namespace
+
+int choose_tile_n(const Context& cx, int64_t m, int64_t n) {
+  const int forced = settings().tile_n.load();
+  if (forced == 128 || forced == 256) return forced;
+  if (n <= 128) return 128;
+  const int64_t tiles256 = ((m + 127) / 128) * ((n + 255) / 256);
+  return tiles256 < cx.num_sms ? 128 : 256;
+}
+
+int choose_slices(int64_t m, int64_t n, int64_t k) {
+  (void)m;
+  (void)n;
+  (void)k;
+  const int forced = settings().dgemm_slices.load();
+  if (forced >= 2 && forced <= kOzakiMaxSlices) return forced;
+  return 8;
+}
+
+int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
+                    int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
+                    cudaStream_t st, const DgemmOptions& opt, eb2_call_info& info) {
+  info.dtype = 'd';
+  info.slices = 0;
+  info.tile_n = 0;
+  info.escalations = 0;
+  info.nonfinite = 0;
+  info.err_estimate = -1.0;
+  info.kernel_ms = -1.0;
+  info.gemm_kernel_ms = -1.0;
+  info.launches = 0;
+  set_pending_timing(nullptr, false);
+  if (m == 0 || n == 0) return EB2_OK;
+  if (k == 0 || alpha == 0.0) {
+    info.method = EB2_METHOD_NATIVE;
+    if (beta == 1.0) return EB2_OK;
+    info.launches = 1;
+    return check_cuda(launch_scale_matrix_d(m, n, beta, C, ldc, st), "scale C") ? EB2_OK : EB2_ERR_CUDA;
+  }
+  int method = opt.method ? opt.method : settings().dgemm_method.load();
+  if (method == EB2_METHOD_AUTO) method = EB2_METHOD_EMULATED;
+  info.method = method;
+
+  if (opt.timed) cudaEventRecord(cx.ev_start, st);
+  if (method == EB2_METHOD_NATIVE) {
+    if (opt.timed) cudaEventRecord(cx.ev_gemm0, st);
+    if (!check_cuda(launch_dgemm_native(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, st),
+                    "native DGEMM"))
+      return EB2_ERR_CUDA;
+    info.launches = 1;
+    if (opt.timed) {
+      cudaEventRecord(cx.ev_gemm1, st);
+      cudaEventRecord(cx.ev_stop, st);
+      set_pending_timing(&cx, true);
+    }
+    if (opt.sync && !check_cuda(cudaStreamSynchronize(st), "DGEMM")) return EB2_ERR_CUDA;
+    return EB2_OK;
+  }
+
+  // ---------------------------------------------------------- Ozaki emulation
+  const int tile_n = opt.tile_n ? opt.tile_n : choose_tile_n(cx, m, n);
+  int s = opt.slices ? opt.slices : choose_slices(m, n, k);
+  const bool check = opt.check_accuracy;
+  const int smax = check ? std::min(kOzakiMaxSlices, s + 3) : s;
+  const int64_t m_pad = round_up(m, kOzakiBM), n_pad = round_up(n, tile_n), k_pad = round_up(k, kOzakiKBlock);
+
+  size_t off = 0;
+  const size_t o_dig_a = off;
+  off = align256(off + size_t(smax) * m_pad * k_pad);
+  const size_t o_dig_b = off;
+  off = align256(off + size_t(smax) * n_pad * k_pad);
+  const size_t o_exp_a = off;
+  off = align256(off + size_t(m_pad) * 4);
+  const size_t o_exp_b = off;
+  off = align256(off + size_t(n_pad) * 4);
+  const size_t o_mb_a = off;
+  off = align256(off + size_t(m) * 8);
+  const size_t o_mb_b = off;
+  off = align256(off + size_t(n) * 8);
+  if (!cx.ws.ensure(off)) {
+    set_error(EB2_ERR_ALLOC, "could not allocate %zu bytes of emulation workspace", off);
+    return EB2_ERR_ALLOC;
+  }
+  uint8_t* ws = static_cast<uint8_t*>(cx.ws.ptr);
+  OzakiOperand oa{reinterpret_cast<int8_t*>(ws + o_dig_a), reinterpret_cast<int32_t*>(ws + o_exp_a),
+                  reinterpret_cast<uint64_t*>(ws + o_mb_a), nullptr, m, m_pad, k, k_pad, smax};
+  OzakiOperand ob{reinterpret_cast<int8_t*>(ws + o_dig_b), reinterpret_cast<int32_t*>(ws + o_exp_b),
+                  reinterpret_cast<uint64_t*>(ws + o_mb_b), nullptr, n, n_pad, k, k_pad, smax};
+  const StridedView<double> va = view_a(ta, A, lda, m, k);
+  const StridedView<double> vb = view_bt(tb, B, ldb, n, k);
+  DeviceFlags* df = cx.dflags;
+
+  bool ok = check_cuda(cudaMemsetAsync(df, 0, sizeof(DeviceFlags), st), "reset flags");
+  ok = ok && check_cuda(launch_ozaki_scan_reset(oa, st), "scan reset A");
+  ok = ok && check_cuda(launch_ozaki_scan_reset(ob, st), "scan reset B");
+  ok = ok && check_cuda(launch_ozaki_scan(va, oa, &df->nonfinite, st), "scan A");
+  ok = ok && check_cuda(launch_ozaki_scan(vb, ob, &df->nonfinite, st), "scan B");
+  ok = ok && check_cuda(launch_ozaki_split(va, oa, 0, s, st), "split A");
+  ok = ok && check_cuda(launch_ozaki_split(vb, ob, 0, s, st), "split B");
+  OzakiGemmArgs g{};
+  g.m = m;
+  g.n = n;
+  g.k = k;
+  g.alpha = alpha;
+  g.beta = beta;
+  g.C = C;
+  g.ldc = ldc;
+  g.slices = s;
+  g.diag_lo = 2;
+  g.diag_hi = s + 1;
+  g.first_writes = true;
+  g.skip_if_flag = &df->nonfinite;
+  g.err_sq = df->err_sq;
+  g.status = &df->status;
+  g.tile_n = tile_n;
+  g.num_sms = cx.num_sms;
+  if (opt.timed) cudaEventRecord(cx.ev_gemm0, st);
+  ok = ok && check_cuda(launch_ozaki_gemm(oa, ob, g, st), "Ozaki GEMM");
+  if (opt.timed) cudaEventRecord(cx.ev_gemm1, st);
+  // IEEE semantics for NaN/Inf inputs: the FP64 kernel runs only when the scan saw one.
+  ok = ok && check_cuda(launch_dgemm_native(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, &df->nonfinite,
+                                            st),
+                        "non-finite fallback");
+  if (!ok) return EB2_ERR_CUDA;
+  info.launches = 6;  // 2 scans, 2 splits, GEMM, non-finite fallback (exits at once when unused)
+  if (opt.timed) {
+    cudaEventRecord(cx.ev_stop, st);
+    set_pending_timing(&cx, true);
+  }
+  info.slices = s;
+  info.tile_n = tile_n;
+  if (!opt.sync && !check) return EB2_OK;
+
+  // ---------------------------------------------------------- a-posteriori check
+  const double tol = opt.tol > 0 ? opt.tol : settings().dgemm_tol.load();
+  double lo_energy = 0.0;
+  for (;;) {
+    if (!check_cuda(cudaMemcpyAsync(cx.hflags, df, sizeof(DeviceFlags), cudaMemcpyDeviceToHost, st), "read flags") ||
+        !check_cuda(cudaStreamSynchronize(st), "DGEMM"))
+      return EB2_ERR_CUDA;
+    const DeviceFlags hf = *cx.hflags;
+    if (hf.status != 0) {
+      set_error(EB2_ERR_TIMEOUT, "a kernel wait timed out (device status 0x%x); C is invalid", hf.status);
+      return EB2_ERR_TIMEOUT;
+    }
+    if (hf.nonfinite) {
+      info.nonfinite = 1;
+      break;
+    }
+    if (info.escalations == 0) lo_energy = hf.err_sq[1];
+    const double est = lo_energy > 0.0 ? std::sqrt(hf.err_sq[0] / lo_energy) * std::ldexp(1.0, -7) *
+                                             std::sqrt(double(s + 1) / double(s))
+                                       : 0.0;
+    info.err_estimate = est;
+    if (!check || est <= tol) break;
+    if (s >= smax) {
+      set_error(EB2_ERR_ACCURACY, "emulated DGEMM estimate %.3g above target %.3g at %d slices", est, tol, s);
+      break;
+    }
+    // add digit s+1 of both operands and the diagonal t = s+2 (pairs p+q = s+2)
+    ok = check_cuda(cudaMemsetAsync(df->err_sq, 0, sizeof(double), st), "reset estimate");
+    ok = ok && check_cuda(launch_ozaki_split(va, oa, s, s + 1, st), "split A");
+    ok = ok && check_cuda(launch_ozaki_split(vb, ob, s, s + 1, st), "split B");
+    g.slices = s + 1;
+    g.diag_lo = g.diag_hi = s + 2;
+    g.first_writes = false;
+    ok = ok && check_cuda(launch_ozaki_gemm(oa, ob, g, st), "Ozaki GEMM (added slice)");
+    if (!ok) return EB2_ERR_CUDA;
+    info.launches += 3;
+    if (opt.timed) {
+      cudaEventRecord(cx.ev_stop, st);
+      set_pending_timing(&cx, false);  // the GEMM events cover only the first pass
+    }
+    ++s;
+    ++info.escalations;
+    info.slices = s;
+  }
+  return EB2_OK;
+}
+
+int sgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, float alpha, const float* A,
+                    int64_t lda, const float* B, int64_t ldb, float beta, float* C, int64_t ldc, cudaStream_t st,
+                    const SgemmOptions& opt, eb2_call_info& info) {
+  info.dtype = 's';
+  info.slices = 0;
+  info.tile_n = 0;
+  info.escalations = 0;
+  info.nonfinite = 0;
+  info.err_estimate = -1.0;
+  info.kernel_ms = -1.0;
+  info.gemm_kernel_ms = -1.0;
+  info.launches = 0;
+  set_pending_timing(nullptr, false);
+  if (m == 0 || n == 0) return EB2_OK;
+  if (k == 0 || alpha == 0.0f) {
+    info.method = EB2_METHOD_NATIVE;
+    if (beta == 1.0f) return EB2_OK;
+    info.launches = 1;
+    return check_cuda(launch_scale_matrix_s(m, n, beta, C, ldc, st), "scale C") ? EB2_OK : EB2_ERR_CUDA;
+  }
+  info.method = EB2_METHOD_NATIVE;
+  if (opt.timed) {
+    cudaEventRecord(cx.ev_start, st);
+    cudaEventRecord(cx.ev_gemm0, st);
+  }
+  if (!check_cuda(launch_sgemm_native(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, st),
+                  "native SGEMM"))
+    return EB2_ERR_CUDA;
+  info.launches = 1;
+  if (opt.timed) {
+    cudaEventRecord(cx.ev_gemm1, st);
+    cudaEventRecord(cx.ev_stop, st);
+    set_pending_timing(&cx, true);
+  }
+  if (opt.sync && !check_cuda(cudaStreamSynchronize(st), "SGEMM")) return EB2_ERR_CUDA;
+  return EB2_OK;
+}
+
+}  // namespace eb2

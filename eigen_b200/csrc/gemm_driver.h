@@ -1,0 +1,38 @@
+// gemm_driver.h -- device-level product drivers (device pointers, one stream).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "context.h"
+
+namespace eb2 {
+
+struct DgemmOptions {
+  int method = 0;        // EB2_METHOD_*; 0 = settings
+  int slices = 0;        // 0 = chosen per call
+  int tile_n = 0;        // 0 = chosen per call
+  double tol = 0.0;      // 0 = settings
+  bool check_accuracy = true;  // a-posteriori estimate + added slices (needs a host sync)
+  bool sync = true;      // wait for the stream before returning
+  bool timed = false;    // record kernel time in call_info
+};
+
+struct SgemmOptions {
+  int method = 0;
+  bool sync = true;
+  bool timed = false;
+};
+
+int choose_tile_n(const Context& cx, int64_t m, int64_t n);
+int choose_slices(int64_t m, int64_t n, int64_t k);
+
+// C = alpha*op(A)op(B) + beta*C on device pointers.  Returns EB2_*.
+int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
+                    int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
+                    cudaStream_t st, const DgemmOptions& opt, eb2_call_info& info);
+int sgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, float alpha, const float* A,
+                    int64_t lda, const float* B, int64_t ldb, float beta, float* C, int64_t ldc, cudaStream_t st,
+                    const SgemmOptions& opt, eb2_call_info& info);
+
+}  // namespace eb2

@@ -1,0 +1,130 @@
+/*
+ * eigen_b200/blas.h -- C ABI of libeigen_b200.so, a B200 (sm_100a) drop-in for
+ * Eigen's dense matrix-matrix product path.
+ *
+ * The Fortran-convention symbols below are the ones Eigen binds for its product
+ * when compiled with EIGEN_USE_BLAS, and the ones Eigen's own BLAS library
+ * exports, so this library serves both:
+ *   - Eigen's Matrix operator* (Eigen/src/Core/products/GeneralMatrixMatrix_BLAS.h:53-118
+ *     calls EIGEN_BLAS_SYM(dgemm)/EIGEN_BLAS_SYM(sgemm) with beta = 1);
+ *   - any C/Fortran caller of ?gemm_ (blas/level3_impl.h:12-96, declared in
+ *     blas/blas.h:384-388 and Eigen/src/misc/blas.h:61-66).
+ * All matrices are column-major.  Pointers may be host memory (pageable or
+ * pinned: the library stages them through device memory) or device/managed
+ * memory (used in place).  The calls are synchronous like any BLAS: C is final
+ * when they return.
+ */
+#ifndef EIGEN_B200_BLAS_H
+#define EIGEN_B200_BLAS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- BLAS ABI */
+
+/* C := alpha*op(A)*op(B) + beta*C, op(X) in {X, X^T, X^H} chosen by 'N'/'T'/'C'
+ * (case-insensitive).  Replaces Eigen's dgemm_ (blas/level3_impl.h:12-96, instantiated
+ * by blas/double.cpp:12-21).  Argument errors call xerbla_("DGEMM ", &info, 6) with
+ * info 1,2,3,4,5,8,10,13 exactly as blas/level3_impl.h:61-78; m == 0 or n == 0
+ * returns without touching C; beta == 0 sets C to exact zeros; alpha == 0 or k == 0
+ * leaves beta*C and does not read A or B (Eigen/src/Core/products/GeneralMatrixMatrix.h:130). */
+void dgemm_(const char* transa, const char* transb, const int* m, const int* n, const int* k, const double* alpha,
+            const double* a, const int* lda, const double* b, const int* ldb, const double* beta, double* c,
+            const int* ldc);
+
+/* Single precision; replaces Eigen's sgemm_ (blas/level3_impl.h:12-96 via blas/single.cpp:11-20). */
+void sgemm_(const char* transa, const char* transb, const int* m, const int* n, const int* k, const float* alpha,
+            const float* a, const int* lda, const float* b, const int* ldb, const float* beta, float* c,
+            const int* ldc);
+
+/* 64-bit-integer (ILP64) variants: the symbols Eigen binds with EIGEN_64BIT_BLAS and
+ * EIGEN_BLAS_SYMBOL_SUFFIX=_64 (Eigen/src/Core/util/MKL_support.h:118-147). */
+void dgemm_64_(const char* transa, const char* transb, const int64_t* m, const int64_t* n, const int64_t* k,
+               const double* alpha, const double* a, const int64_t* lda, const double* b, const int64_t* ldb,
+               const double* beta, double* c, const int64_t* ldc);
+void sgemm_64_(const char* transa, const char* transb, const int64_t* m, const int64_t* n, const int64_t* k,
+               const float* alpha, const float* a, const int64_t* lda, const float* b, const int64_t* ldb,
+               const float* beta, float* c, const int64_t* ldc);
+
+/* Argument-error hook, weak like blas/xerbla.cpp:18-20: prints
+ * "Eigen BLAS ERROR #<info>: <name>" unless the program defines its own. */
+void xerbla_(const char* name, int* info, size_t len);
+
+/* ---------------------------------------------------------------- extensions */
+
+/* Status codes of the eb2_* calls and of eb2_last_error(). */
+enum {
+  EB2_OK = 0,
+  EB2_ERR_CUDA = -1,      /* a CUDA runtime call failed (message in eb2_last_error_string) */
+  EB2_ERR_ALLOC = -2,     /* device or pinned memory could not be allocated */
+  EB2_ERR_TIMEOUT = -3,   /* a kernel's bounded wait ran out; results are invalid */
+  EB2_ERR_ARG = -4,       /* invalid argument to an eb2_* call (BLAS calls use xerbla_) */
+  EB2_ERR_NO_DEVICE = -5, /* no CUDA device, or not an sm_100 device */
+  EB2_ERR_ACCURACY = -6   /* the emulated product missed its accuracy target at the maximum slice count */
+};
+
+/* Method used for DGEMM / SGEMM. */
+enum {
+  EB2_METHOD_AUTO = 0,     /* DGEMM: Ozaki INT8 emulation; SGEMM: split-BF16 on tcgen05 */
+  EB2_METHOD_NATIVE = 1,   /* DGEMM: FP64 DMMA kernel; SGEMM: FP32 FFMA kernel */
+  EB2_METHOD_EMULATED = 2  /* force the emulated method */
+};
+
+int eb2_set_dgemm_method(int method);
+int eb2_set_sgemm_method(int method);
+/* Digit slices per operand for the emulated DGEMM (2..12); 0 = chosen per call. */
+int eb2_set_dgemm_slices(int slices);
+/* Accuracy target of the emulated DGEMM: the a-posteriori estimate of
+ * ||C - C_exact||_F / ||alpha*op(A)op(B)||_F must not exceed it (default 2^-53);
+ * slices are added one at a time until it holds or 12 are used. */
+int eb2_set_dgemm_tolerance(double tol);
+/* Output-tile width of the tcgen05 kernels: 128, 256 or 0 (= chosen per call). */
+int eb2_set_tile_n(int tile_n);
+
+/* Sticky last error of this thread (EB2_OK if none) and its message. */
+int eb2_last_error(void);
+const char* eb2_last_error_string(void);
+void eb2_clear_error(void);
+
+/* Details of the last product computed by this thread. */
+typedef struct eb2_call_info {
+  int dtype;          /* 'd' or 's' */
+  int method;         /* EB2_METHOD_NATIVE or EB2_METHOD_EMULATED */
+  int slices;         /* digit slices (DGEMM emulated) or BF16 products (SGEMM emulated) */
+  int tile_n;         /* tcgen05 tile width, 0 for native kernels */
+  int escalations;    /* slices added by the a-posteriori check */
+  int nonfinite;      /* 1 if NaN/Inf inputs sent the call to the native kernel */
+  int staged;         /* 1 if host buffers were staged through device memory */
+  double err_estimate; /* a-posteriori relative error estimate (emulated DGEMM), else -1 */
+  double kernel_ms;   /* device time of all product kernels (ms), -1 if not measured */
+  double gemm_kernel_ms; /* device time of the main GEMM kernel alone (ms), -1 if not measured */
+  int launches;       /* kernels this library launched for the call */
+} eb2_call_info;
+int eb2_last_call_info(eb2_call_info* out);
+
+/* Record CUDA events around every product (1) or not (0, default for the
+ * eb2_*_device calls; the BLAS entry points always time).  The times appear in
+ * eb2_last_call_info (which waits for the events) until the next call on the device. */
+int eb2_set_timing(int on);
+
+/* Stream-ordered product on device pointers; no host synchronisation unless the
+ * a-posteriori check of the emulated DGEMM needs one (check_accuracy != 0).
+ * `stream` is a cudaStream_t (NULL = the legacy default stream).  Returns EB2_*. */
+int eb2_dgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, double alpha, const double* a,
+                     int64_t lda, const double* b, int64_t ldb, double beta, double* c, int64_t ldc, void* stream,
+                     int check_accuracy);
+int eb2_sgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, float alpha, const float* a,
+                     int64_t lda, const float* b, int64_t ldb, float beta, float* c, int64_t ldc, void* stream);
+
+/* Library version string. */
+const char* eb2_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EIGEN_B200_BLAS_H */
