@@ -79,7 +79,9 @@ def load(path: str | os.PathLike | None = None, mode: int = ctypes.RTLD_GLOBAL) 
     lib.eb2_set_dgemm_slices.argtypes = [ctypes.c_int]
     lib.eb2_set_dgemm_tolerance.argtypes = [ctypes.c_double]
     lib.eb2_set_tile_n.argtypes = [ctypes.c_int]
+    lib.eb2_set_sgemm_pieces.argtypes = [ctypes.c_int]
     lib.eb2_set_timing.argtypes = [ctypes.c_int]
+    lib.eb2_set_slice_tuning.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.eb2_last_error_string.restype = ctypes.c_char_p
     lib.eb2_last_call_info.argtypes = [ctypes.POINTER(CallInfo)]
     lib.eb2_version.restype = ctypes.c_char_p
@@ -154,12 +156,20 @@ def set_dgemm_slices(slices: int) -> int:
     return load().eb2_set_dgemm_slices(slices)
 
 
+def set_sgemm_pieces(pieces: int) -> int:
+    return load().eb2_set_sgemm_pieces(pieces)
+
+
 def set_dgemm_tolerance(tol: float) -> int:
     return load().eb2_set_dgemm_tolerance(tol)
 
 
 def set_tile_n(tile_n: int) -> int:
     return load().eb2_set_tile_n(tile_n)
+
+
+def set_slice_tuning(group_m: int, prefetch: int) -> int:
+    return load().eb2_set_slice_tuning(group_m, prefetch)
 
 
 def set_timing(on: bool) -> int:

@@ -235,6 +235,12 @@ int eb2_set_dgemm_slices(int slices) {
   return EB2_OK;
 }
 
+int eb2_set_sgemm_pieces(int pieces) {
+  if (pieces != 2 && pieces != 3) return EB2_ERR_ARG;
+  eb2::settings().sgemm_pieces = pieces;
+  return EB2_OK;
+}
+
 int eb2_set_dgemm_tolerance(double tol) {
   if (!(tol > 0.0)) return EB2_ERR_ARG;
   eb2::settings().dgemm_tol = tol;
@@ -250,6 +256,13 @@ int eb2_set_tile_n(int tile_n) {
 int eb2_last_error(void) { return eb2::last_error(); }
 
 void eb2_clear_error(void) { eb2::set_error(EB2_OK, ""); }
+
+int eb2_set_slice_tuning(int group_m, int prefetch) {
+  if (group_m < 0 || prefetch < 0 || prefetch > 64) return EB2_ERR_ARG;
+  eb2::tuning().group_m = group_m;
+  eb2::tuning().prefetch = prefetch;
+  return EB2_OK;
+}
 
 int eb2_set_timing(int on) {
   eb2::settings().timing = on ? 1 : 0;

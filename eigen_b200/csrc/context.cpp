@@ -1,5 +1,6 @@
 // context.cpp -- see context.h.
 #include "context.h"
+#include "kernels.h"
 
 #include <cstdarg>
 #include <cstdio>
@@ -18,6 +19,11 @@ constexpr int kMaxDevices = 64;
 std::mutex g_ctx_mu;
 Context* g_ctx[kMaxDevices] = {};
 }  // namespace
+
+SliceTuning& tuning() {
+  static SliceTuning t;
+  return t;
+}
 
 Settings& settings() {
   static Settings s;

@@ -17,6 +17,8 @@ namespace eb2 {
 
 namespace {
 
+constexpr int64_t kSliceBMHost = 128;
+
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
@@ -237,21 +239,82 @@ int sgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
     info.launches = 1;
     return check_cuda(launch_scale_matrix_s(m, n, beta, C, ldc, st), "scale C") ? EB2_OK : EB2_ERR_CUDA;
   }
-  info.method = EB2_METHOD_NATIVE;
-  if (opt.timed) {
-    cudaEventRecord(cx.ev_start, st);
-    cudaEventRecord(cx.ev_gemm0, st);
+  int method = opt.method ? opt.method : settings().sgemm_method.load();
+  if (method == EB2_METHOD_AUTO) method = EB2_METHOD_EMULATED;
+  info.method = method;
+  if (opt.timed) cudaEventRecord(cx.ev_start, st);
+  if (method == EB2_METHOD_NATIVE) {
+    if (opt.timed) cudaEventRecord(cx.ev_gemm0, st);
+    if (!check_cuda(launch_sgemm_native(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, st),
+                    "native SGEMM"))
+      return EB2_ERR_CUDA;
+    info.launches = 1;
+    if (opt.timed) {
+      cudaEventRecord(cx.ev_gemm1, st);
+      cudaEventRecord(cx.ev_stop, st);
+      set_pending_timing(&cx, true);
+    }
+    if (opt.sync && !check_cuda(cudaStreamSynchronize(st), "SGEMM")) return EB2_ERR_CUDA;
+    return EB2_OK;
   }
-  if (!check_cuda(launch_sgemm_native(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, st),
-                  "native SGEMM"))
-    return EB2_ERR_CUDA;
-  info.launches = 1;
+
+  // ---------------------------------------------------------- split-BF16 emulation
+  const int tile_n = opt.tile_n ? opt.tile_n : choose_tile_n(cx, m, n);
+  const int pieces = opt.pieces ? opt.pieces : settings().sgemm_pieces.load();
+  const int64_t m_pad = round_up(m, kSliceBMHost), n_pad = round_up(n, tile_n), k_pad = round_up(k, 64);
+  size_t off = 0;
+  const size_t o_a = off;
+  off = align256(off + size_t(3) * m_pad * k_pad * 2);
+  const size_t o_b = off;
+  off = align256(off + size_t(3) * n_pad * k_pad * 2);
+  if (!cx.ws.ensure(off)) {
+    set_error(EB2_ERR_ALLOC, "could not allocate %zu bytes of emulation workspace", off);
+    return EB2_ERR_ALLOC;
+  }
+  uint8_t* ws = static_cast<uint8_t*>(cx.ws.ptr);
+  Bf16Operand oa{ws + o_a, m, m_pad, k, k_pad};
+  Bf16Operand ob{ws + o_b, n, n_pad, k, k_pad};
+  const StridedView<float> va = ta ? StridedView<float>{A, m, k, lda, 1} : StridedView<float>{A, m, k, 1, lda};
+  const StridedView<float> vb = tb ? StridedView<float>{B, n, k, 1, ldb} : StridedView<float>{B, n, k, ldb, 1};
+  DeviceFlags* df = cx.dflags;
+  bool ok = check_cuda(cudaMemsetAsync(df, 0, sizeof(DeviceFlags), st), "reset flags");
+  ok = ok && check_cuda(launch_bf16_split(va, oa, &df->nonfinite, st), "split A");
+  ok = ok && check_cuda(launch_bf16_split(vb, ob, &df->nonfinite, st), "split B");
+  SgemmSplitArgs g{};
+  g.m = m;
+  g.n = n;
+  g.k = k;
+  g.alpha = alpha;
+  g.beta = beta;
+  g.C = C;
+  g.ldc = ldc;
+  g.pieces = pieces;
+  g.skip_if_flag = &df->nonfinite;
+  g.status = &df->status;
+  g.tile_n = tile_n;
+  g.num_sms = cx.num_sms;
+  if (opt.timed) cudaEventRecord(cx.ev_gemm0, st);
+  ok = ok && check_cuda(launch_sgemm_split_bf16(oa, ob, g, st), "split-BF16 GEMM");
+  if (opt.timed) cudaEventRecord(cx.ev_gemm1, st);
+  ok = ok && check_cuda(launch_sgemm_native(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, &df->nonfinite, st),
+                        "non-finite fallback");
+  if (!ok) return EB2_ERR_CUDA;
+  info.launches = 4;  // 2 splits, GEMM, non-finite fallback (exits at once when unused)
+  info.slices = pieces * (pieces + 1) / 2;
+  info.tile_n = tile_n;
   if (opt.timed) {
-    cudaEventRecord(cx.ev_gemm1, st);
     cudaEventRecord(cx.ev_stop, st);
     set_pending_timing(&cx, true);
   }
-  if (opt.sync && !check_cuda(cudaStreamSynchronize(st), "SGEMM")) return EB2_ERR_CUDA;
+  if (!opt.sync) return EB2_OK;
+  if (!check_cuda(cudaMemcpyAsync(cx.hflags, df, sizeof(DeviceFlags), cudaMemcpyDeviceToHost, st), "read flags") ||
+      !check_cuda(cudaStreamSynchronize(st), "SGEMM"))
+    return EB2_ERR_CUDA;
+  if (cx.hflags->status != 0) {
+    set_error(EB2_ERR_TIMEOUT, "a kernel wait timed out (device status 0x%x); C is invalid", cx.hflags->status);
+    return EB2_ERR_TIMEOUT;
+  }
+  info.nonfinite = cx.hflags->nonfinite ? 1 : 0;
   return EB2_OK;
 }
 

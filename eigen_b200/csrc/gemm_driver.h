@@ -20,6 +20,8 @@ struct DgemmOptions {
 
 struct SgemmOptions {
   int method = 0;
+  int pieces = 0;  // BF16 pieces per operand (2 or 3); 0 = settings
+  int tile_n = 0;
   bool sync = true;
   bool timed = false;
 };

@@ -8,6 +8,13 @@
 
 namespace eb2 {
 
+// Launch-shape knobs of the tcgen05 slice GEMM (set by the tuner; process-wide).
+struct SliceTuning {
+  int group_m = 0;   // row-tiles per raster group; 0 = all (column-major tile order)
+  int prefetch = 0;  // L2 prefetch distance in K blocks; 0 = off
+};
+SliceTuning& tuning();
+
 // A strided view of op(X) as a rows x cols matrix: element (r, l) at X[r*sr + l*sl].
 template <typename T>
 struct StridedView {
@@ -70,5 +77,28 @@ struct OzakiGemmArgs {
 };
 cudaError_t launch_ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, const OzakiGemmArgs& args,
                               cudaStream_t stream);
+
+// ------------------------------------------------------------ split-BF16 (emulated FP32)
+struct Bf16Operand {
+  void* pieces;  // [3][rows_pad][k_pad] bf16: hi, mid, lo pieces, row r contiguous along k
+  int64_t rows, rows_pad, k, k_pad;
+};
+// Split op(X) (rows x k view) into its three BF16 pieces; sets *nonfinite on NaN/Inf.
+cudaError_t launch_bf16_split(const StridedView<float>& x, const Bf16Operand& op, int* nonfinite,
+                              cudaStream_t stream);
+
+struct SgemmSplitArgs {
+  int64_t m, n, k;
+  float alpha, beta;
+  float* C;
+  int64_t ldc;
+  int pieces;  // s: 2 -> 3 products (hh, hm, mh), 3 -> 6 products (+ mm, hl, lh)
+  const int* skip_if_flag;
+  uint32_t* status;
+  int tile_n;
+  int num_sms;
+};
+cudaError_t launch_sgemm_split_bf16(const Bf16Operand& a, const Bf16Operand& b, const SgemmSplitArgs& args,
+                                    cudaStream_t stream);
 
 }  // namespace eb2

@@ -82,8 +82,16 @@ int eb2_set_dgemm_slices(int slices);
  * ||C - C_exact||_F / ||alpha*op(A)op(B)||_F must not exceed it (default 2^-53);
  * slices are added one at a time until it holds or 12 are used. */
 int eb2_set_dgemm_tolerance(double tol);
+/* BF16 pieces per FP32 operand for the emulated SGEMM: 2 keeps the three products
+ * hi*hi + hi*mid + mid*hi ("bf16x3"), 3 adds mid*mid + hi*lo + lo*hi ("bf16x6", default). */
+int eb2_set_sgemm_pieces(int pieces);
 /* Output-tile width of the tcgen05 kernels: 128, 256 or 0 (= chosen per call). */
 int eb2_set_tile_n(int tile_n);
+
+/* Launch-shape knobs of the tcgen05 kernels (normally set by the tuner): row-tiles per
+ * raster group (0 = column-major tile order) and the L2 prefetch distance in K blocks
+ * (0 = off). */
+int eb2_set_slice_tuning(int group_m, int prefetch);
 
 /* Sticky last error of this thread (EB2_OK if none) and its message. */
 int eb2_last_error(void);

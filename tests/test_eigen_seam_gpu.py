@@ -1,0 +1,29 @@
+"""Eigen's own Matrix operator*, compiled with EIGEN_USE_BLAS, runs on libeigen_b200.so.
+
+tests/eigen_seam/eigen_seam_demo.cpp is built against the reference's Eigen headers
+(tests/eigen_seam/Makefile) and linked with libeigen_b200.so first; this test runs it and
+checks its self-verification plus the library's own call record."""
+from __future__ import annotations
+
+import json
+import subprocess
+from pathlib import Path
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+DEMO = Path(__file__).resolve().parent / "eigen_seam" / "_bin" / "eigen_seam_demo"
+
+
+@pytest.mark.parametrize("m,n,k", [(300, 200, 250), (1000, 517, 129)])
+def test_eigen_operator_product_routes_to_library(m, n, k):
+    if not DEMO.exists():
+        pytest.fail(f"{DEMO} missing: build it with `make -C tests/eigen_seam if-present`")
+    r = subprocess.run([str(DEMO), str(m), str(n), str(k)], capture_output=True, text=True, timeout=300)
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert line, r.stdout + r.stderr
+    out = json.loads(line[-1])
+    assert r.returncode == 0, out
+    assert out["err_AB"] < 1e-14 and out["err_alpha_AtB"] < 1e-14 and out["err_float"] < 1e-5
+    assert out["dgemm_launches"] > 0 and out["sgemm_launches"] > 0  # the products ran in the library
+    assert out["dgemm_method"] == 2 and out["dgemm_slices"] >= 8     # emulated DGEMM by default

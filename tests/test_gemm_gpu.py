@@ -30,6 +30,7 @@ def _defaults():
     eb.set_dgemm_slices(0)
     eb.set_dgemm_tolerance(U64)
     eb.set_tile_n(0)
+    eb.set_sgemm_pieces(3)
     eb.clear_error()
     yield
     eb.set_dgemm_method(eb.METHOD_AUTO)
@@ -72,6 +73,7 @@ def test_dgemm_golden_parity(method, device):
 
 @pytest.mark.parametrize("device", [False, True])
 def test_sgemm_golden_parity(device):
+    eb.set_sgemm_method(eb.METHOD_NATIVE)
     cases, _ = golden()
     for case in cases:
         if case["dtype"] != "s":
@@ -159,7 +161,9 @@ def test_dgemm_test_ratio(ta, tb, method):
 
 
 @pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T"), ("T", "T")])
-def test_sgemm_test_ratio(ta, tb):
+@pytest.mark.parametrize("method", [eb.METHOD_NATIVE, eb.METHOD_EMULATED])
+def test_sgemm_test_ratio(ta, tb, method):
+    eb.set_sgemm_method(method)
     m, n, k = 261, 135, 300
     A, lda, B, ldb, C, ldc = make_operands(m, n, k, ta, tb, pad=5, seed=19, dtype=np.float32)
     Cg = C.copy(order="F")
@@ -245,3 +249,63 @@ def test_device_entry_on_a_torch_stream():
     Cg = np.asfortranarray(tC.cpu().numpy().T)
     hi, lo = dd_reference("N", "N", m, n, k, 1.0, A, lda, B, ldb, 0.0, None, ldc)
     assert rel_error_vs_dd(Cg[:m, :n], hi, lo) < 4 * U64
+
+
+# ---------------------------------------------------------------- split-BF16 SGEMM
+@pytest.mark.parametrize("device", [False, True])
+def test_sgemm_emulated_golden_parity(device):
+    """bf16x6 (default) meets the FP32 product bound on every golden case."""
+    eb.set_sgemm_method(eb.METHOD_EMULATED)
+    eb.set_sgemm_pieces(3)
+    cases, _ = golden()
+    for case in cases:
+        if case["dtype"] != "s":
+            continue
+        C = _call(case, case["Cin"].copy(order="F"), device)
+        check_against_reference(case, C)
+
+
+def _sgemm_rel_err(m, n, k, ta, tb, seed, r=0):
+    A, lda, B, ldb, C, ldc = make_operands(m, n, k, ta, tb, pad=3, r=r, seed=seed, dtype=np.float32)
+    Cg = C.copy(order="F")
+    eb.sgemm(ta, tb, m, n, k, 1.0, A, lda, B, ldb, 0.0, Cg, ldc)
+    A64, B64 = A.astype(np.float64), B.astype(np.float64)
+    hi, lo = dd_reference(ta, tb, m, n, k, 1.0, A64, lda, B64, ldb, 0.0, None, ldc)
+    return rel_error_vs_dd(Cg[:m, :n].astype(np.float64), hi, lo)
+
+
+@pytest.mark.parametrize("ta,tb,m,n,k", [("N", "N", 640, 384, 1024), ("T", "N", 300, 517, 700),
+                                         ("N", "T", 129, 1, 2000), ("T", "T", 257, 260, 64)])
+def test_sgemm_split_bf16_accuracy(ta, tb, m, n, k):
+    """bf16x6 is about as accurate as the native FP32 kernel (within 4x); bf16x3 loses
+    about 8 bits (relative error below 2^-15)."""
+    eb.set_sgemm_method(eb.METHOD_NATIVE)
+    e_nat = _sgemm_rel_err(m, n, k, ta, tb, seed=5)
+    eb.set_sgemm_method(eb.METHOD_EMULATED)
+    eb.set_sgemm_pieces(3)
+    e6 = _sgemm_rel_err(m, n, k, ta, tb, seed=5)
+    info = eb.last_call_info()
+    assert info["method"] == eb.METHOD_EMULATED and info["slices"] == 6
+    eb.set_sgemm_pieces(2)
+    e3 = _sgemm_rel_err(m, n, k, ta, tb, seed=5)
+    assert eb.last_call_info()["slices"] == 3
+    eb.set_sgemm_pieces(3)
+    # FP32 accumulation inside the tensor core is not the FFMA kernel's sequential
+    # round-to-nearest chain; both stay far inside the lam*sqrt(k)*eps product bound
+    assert e6 <= max(4 * e_nat, 2.0 ** -19), (e6, e_nat)
+    assert e3 < 2.0 ** -15, e3
+
+
+def test_sgemm_emulated_nonfinite_falls_back():
+    m, n, k = 70, 40, 90
+    A, lda, B, ldb, C, ldc = make_operands(m, n, k, "N", "N", seed=43, dtype=np.float32)
+    A[3, 5] = np.nan
+    B[7, 2] = np.inf
+    eb.set_sgemm_method(eb.METHOD_EMULATED)
+    Cg = C.copy(order="F")
+    eb.sgemm("N", "N", m, n, k, 1.0, A, lda, B, ldb, 0.0, Cg, ldc)
+    assert eb.last_call_info()["nonfinite"] == 1
+    Co = C.copy(order="F")
+    oracle().oracle_sgemm(b"N", b"N", m, n, k, 1.0, P(A), lda, P(B), ldb, 0.0, P(Co), ldc)
+    np.testing.assert_array_equal(np.isnan(Cg), np.isnan(Co))
+    np.testing.assert_array_equal(np.isinf(Cg), np.isinf(Co))
