@@ -55,6 +55,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-native", action="store_true")
+    ap.add_argument("--no-grouped", action="store_true")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     a.steps = max(a.steps, 1)
@@ -141,15 +142,13 @@ class ClockSampler:
 
     def __init__(self, device_id: str | None):
         self.proc = None
-        self.out = None
         self.device_id = device_id
 
     def start(self):
-        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "50"]
         if self.device_id:
             cmd += ["-i", self.device_id]
         try:
-            self.out = open(os.devnull, "w") if False else None
             self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -196,6 +195,79 @@ def profiled_traffic(size: int):
         return None
     b, at = float(m.group(1)), int(m.group(2))
     return b * (size / at) ** 3 if at != size else b
+
+
+# ------------------------------------------------------------------------ grouped batch
+def batch_sizes(count, seed):
+    """m, n, k each round(exp(U[ln 3, ln 256])); with probability 0.2 all three from {3,4,6,8}."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        if rng.random() < 0.2:
+            s = int(rng.choice([3, 4, 6, 8]))
+            out.append((s, s, s))
+        else:
+            out.append(tuple(int(round(float(np.exp(rng.uniform(np.log(3.0), np.log(256.0)))))) for _ in range(3)))
+    return out
+
+
+def grouped_bench(eb, torch, dev, stream, steps, warmup, count=10000, seed=7):
+    """10,000 uneven products per dtype: one graph-captured grouped launch vs one plain
+    launch of the native kernel per product (eb2_gemm_each); both device-timed."""
+    sizes = batch_sizes(count, seed)
+    res = {}
+    for dtype, tdt in (("d", torch.float64), ("s", torch.float32)):
+        na = sum(m * k for m, n, k in sizes)
+        nb = sum(k * n for m, n, k in sizes)
+        nc = sum(m * n for m, n, k in sizes)
+        g = torch.Generator(device=dev)
+        g.manual_seed(seed)
+        bufA = torch.rand(na + 2 * count, dtype=tdt, device=dev, generator=g) * 2 - 1
+        bufB = torch.rand(nb + 2 * count, dtype=tdt, device=dev, generator=g) * 2 - 1
+        bufC = torch.zeros(nc + 2 * count, dtype=tdt, device=dev)
+        es = bufA.element_size()
+        oa = ob = oc = 0
+        probs = []
+        for (m, n, k) in sizes:
+            probs.append(dict(m=m, n=n, k=k, alpha=1.0, beta=0.0, a=bufA.data_ptr() + oa * es, lda=m,
+                              b=bufB.data_ptr() + ob * es, ldb=k, c=bufC.data_ptr() + oc * es, ldc=m))
+            oa += m * k + (m * k) % 2
+            ob += k * n + (k * n) % 2
+            oc += m * n + (m * n) % 2
+        arr = eb.problems_array(probs)
+        flops = float(sum(2.0 * m * n * k for m, n, k in sizes))
+        plan = eb.GroupedPlan(dtype, arr)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                plan.execute(stream.cuda_stream)
+            stream.synchronize()
+            ev0.record(stream)
+            for _ in range(steps):
+                plan.execute(stream.cuda_stream)
+            ev1.record(stream)
+            stream.synchronize()
+            ms_grouped = ev0.elapsed_time(ev1) / steps
+            eb.gemm_each(dtype, arr, stream.cuda_stream)  # warm-up of the per-call path
+            stream.synchronize()
+            reps = max(1, min(3, steps))
+            ev0.record(stream)
+            for _ in range(reps):
+                eb.gemm_each(dtype, arr, stream.cuda_stream)
+            ev1.record(stream)
+            stream.synchronize()
+            ms_each = ev0.elapsed_time(ev1) / reps
+        plan.close()
+        res["fp64" if dtype == "d" else "fp32"] = {
+            "gflops": round(flops / (ms_grouped * 1e-3) / 1e9, 1), "ms": round(ms_grouped, 4),
+            "per_call_ms": round(ms_each, 3), "per_call_gflops": round(flops / (ms_each * 1e-3) / 1e9, 2),
+            "speedup_vs_per_call": round(ms_each / ms_grouped, 1), "problems": count, "flops": flops,
+            "launches": 1, "per_call_launches": count,
+        }
+        del bufA, bufB, bufC
+    return res
 
 
 # ------------------------------------------------------------------------ arms
@@ -348,6 +420,10 @@ def our_arm(a, world, rank, local):
                "ms_per_step": round(t_step * 1e3, 3), "steps": e2e_steps,
                "api": "dgemm_ (Fortran BLAS ABI) on pinned host buffers; synchronous call timed on the host"}
 
+    grouped = None
+    if not a.no_grouped:
+        grouped = grouped_bench(eb, torch, dev, stream, a.steps, a.warmup)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         model, _ = host_cpu_info()
@@ -382,7 +458,7 @@ def our_arm(a, world, rank, local):
             "config": dict(workload_config(a), slices=slices, tile_n=infos[-1]["tile_n"],
                            err_estimate=infos[-1]["err_estimate"], escalations=infos[-1]["escalations"]),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk, "native_fp64": native,
+            "clocks": clk, "native_fp64": native, "grouped_batch": grouped,
             "emulated_over_native": round(value / native["tflops"], 3) if native else None,
         }
         print(json.dumps(line))

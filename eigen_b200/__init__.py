@@ -58,6 +58,26 @@ class CallInfo(ctypes.Structure):
         return d
 
 
+class GemmProblem(ctypes.Structure):
+    """eb2_gemm_problem: one product of a grouped launch (device pointers)."""
+
+    _fields_ = [
+        ("transa", ctypes.c_char),
+        ("transb", ctypes.c_char),
+        ("m", ctypes.c_int64),
+        ("n", ctypes.c_int64),
+        ("k", ctypes.c_int64),
+        ("alpha", ctypes.c_double),
+        ("beta", ctypes.c_double),
+        ("a", ctypes.c_void_p),
+        ("lda", ctypes.c_int64),
+        ("b", ctypes.c_void_p),
+        ("ldb", ctypes.c_int64),
+        ("c", ctypes.c_void_p),
+        ("ldc", ctypes.c_int64),
+    ]
+
+
 def load(path: str | os.PathLike | None = None, mode: int = ctypes.RTLD_GLOBAL) -> ctypes.CDLL:
     """Load libeigen_b200.so (once) and declare its signatures.  Raises if absent."""
     global _lib
@@ -91,6 +111,12 @@ def load(path: str | os.PathLike | None = None, mode: int = ctypes.RTLD_GLOBAL) 
     lib.eb2_sgemm_device.argtypes = [ctypes.c_char, ctypes.c_char, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                      ctypes.c_float, vp, ctypes.c_int64, vp, ctypes.c_int64, ctypes.c_float, vp,
                                      ctypes.c_int64, vp]
+    pp = ctypes.POINTER(GemmProblem)
+    lib.eb2_grouped_plan_create.argtypes = [ctypes.c_char, ctypes.c_int64, pp, ctypes.POINTER(ctypes.c_void_p)]
+    lib.eb2_grouped_plan_execute.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    lib.eb2_grouped_plan_destroy.argtypes = [ctypes.c_void_p]
+    lib.eb2_gemm_grouped.argtypes = [ctypes.c_char, ctypes.c_int64, pp, ctypes.c_void_p]
+    lib.eb2_gemm_each.argtypes = [ctypes.c_char, ctypes.c_int64, pp, ctypes.c_void_p]
     _lib = lib
     return lib
 
@@ -189,6 +215,53 @@ def last_call_info() -> dict:
     ci = CallInfo()
     load().eb2_last_call_info(ctypes.byref(ci))
     return ci.as_dict()
+
+
+def problems_array(problems) -> "ctypes.Array":
+    """Build a GemmProblem array from dicts with keys transa, transb, m, n, k, alpha, beta,
+    a, lda, b, ldb, c, ldc (a/b/c: CUDA tensors or device addresses)."""
+    arr = (GemmProblem * len(problems))()
+    for i, p in enumerate(problems):
+        arr[i] = GemmProblem(p.get("transa", "N").encode(), p.get("transb", "N").encode(), p["m"], p["n"], p["k"],
+                             p.get("alpha", 1.0), p.get("beta", 0.0), _ptr(p["a"]), p["lda"], _ptr(p["b"]), p["ldb"],
+                             _ptr(p["c"]), p["ldc"])
+    return arr
+
+
+class GroupedPlan:
+    """A captured grouped launch (eb2_grouped_plan_*); execute() replays it."""
+
+    def __init__(self, dtype: str, problems):
+        self._arr = problems if isinstance(problems, ctypes.Array) else problems_array(problems)
+        self._h = ctypes.c_void_p()
+        rc = load().eb2_grouped_plan_create(dtype.encode(), len(self._arr), self._arr, ctypes.byref(self._h))
+        if rc != EB2_OK:
+            raise RuntimeError(f"eb2_grouped_plan_create failed: {rc} {last_error()[1]}")
+
+    def execute(self, stream=0) -> int:
+        return load().eb2_grouped_plan_execute(self._h, stream or None)
+
+    def close(self):
+        if self._h:
+            load().eb2_grouped_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def gemm_grouped(dtype: str, problems, stream=0) -> int:
+    arr = problems if isinstance(problems, ctypes.Array) else problems_array(problems)
+    return load().eb2_gemm_grouped(dtype.encode(), len(arr), arr, stream or None)
+
+
+def gemm_each(dtype: str, problems, stream=0) -> int:
+    """One plain native launch per product (the per-call baseline of the grouped path)."""
+    arr = problems if isinstance(problems, ctypes.Array) else problems_array(problems)
+    return load().eb2_gemm_each(dtype.encode(), len(arr), arr, stream or None)
 
 
 def version() -> str:

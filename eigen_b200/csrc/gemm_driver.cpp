@@ -17,7 +17,9 @@ namespace eb2 {
 
 namespace {
 
-constexpr int64_t kSliceBMHost = 128;
+// Rows / columns of C covered by one tile of a tile configuration.
+int64_t tile_m_of(int cfg) { return cfg == kTilePair ? 256 : 128; }
+int64_t tile_n_of(int cfg) { return cfg == kTilePair ? 256 : cfg; }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
@@ -43,7 +45,7 @@ StridedView<double> view_bt(bool tb, const double* B, int64_t ldb, int64_t n, in
 
 int choose_tile_n(const Context& cx, int64_t m, int64_t n) {
   const int forced = settings().tile_n.load();
-  if (forced == 128 || forced == 256) return forced;
+  if (forced == 128 || forced == 256 || forced == kTilePair) return forced;
   if (n <= 128) return 128;
   const int64_t tiles256 = ((m + 127) / 128) * ((n + 255) / 256);
   return tiles256 < cx.num_sms ? 128 : 256;
@@ -103,7 +105,8 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   int s = opt.slices ? opt.slices : choose_slices(m, n, k);
   const bool check = opt.check_accuracy;
   const int smax = check ? std::min(kOzakiMaxSlices, s + 3) : s;
-  const int64_t m_pad = round_up(m, kOzakiBM), n_pad = round_up(n, tile_n), k_pad = round_up(k, kOzakiKBlock);
+  const int64_t m_pad = round_up(m, tile_m_of(tile_n)), n_pad = round_up(n, tile_n_of(tile_n)),
+                k_pad = round_up(k, kOzakiKBlock);
 
   size_t off = 0;
   const size_t o_dig_a = off;
@@ -261,7 +264,7 @@ int sgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   // ---------------------------------------------------------- split-BF16 emulation
   const int tile_n = opt.tile_n ? opt.tile_n : choose_tile_n(cx, m, n);
   const int pieces = opt.pieces ? opt.pieces : settings().sgemm_pieces.load();
-  const int64_t m_pad = round_up(m, kSliceBMHost), n_pad = round_up(n, tile_n), k_pad = round_up(k, 64);
+  const int64_t m_pad = round_up(m, tile_m_of(tile_n)), n_pad = round_up(n, tile_n_of(tile_n)), k_pad = round_up(k, 64);
   size_t off = 0;
   const size_t o_a = off;
   off = align256(off + size_t(3) * m_pad * k_pad * 2);

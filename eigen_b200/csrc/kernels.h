@@ -39,6 +39,9 @@ cudaError_t launch_scale_matrix_s(int64_t m, int64_t n, float beta, float* C, in
 
 // ------------------------------------------------------------ Ozaki (emulated FP64)
 constexpr int kOzakiMaxSlices = 12;
+// Tile configurations of the tcgen05 kernels: 128 / 256 = one CTA computing 128 x 128 /
+// 128 x 256 tiles; kTilePair = a CTA pair (cluster of 2) computing 256 x 256 tiles.
+constexpr int kTilePair = 512;
 constexpr int kOzakiKBlock = 128;  // bytes of K per pipeline stage (int8 digits)
 constexpr int kOzakiBM = 128;
 
@@ -72,7 +75,7 @@ struct OzakiGemmArgs {
   const int* skip_if_flag;  // non-null: the kernel returns at once when *flag != 0
   double* err_sq;      // [2]: += squared contribution of diagonal diag_hi, and of diagonal 2 (may be null)
   uint32_t* status;    // device status word (EB2_DEV_*)
-  int tile_n;          // 128 or 256
+  int tile_n;          // 128, 256 or kTilePair
   int num_sms;
 };
 cudaError_t launch_ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, const OzakiGemmArgs& args,

@@ -193,6 +193,40 @@ cudaError_t launch_gemm_tiles(const OzakiOperand& a, const OzakiOperand& b, cons
   return cudaGetLastError();
 }
 
+cudaError_t launch_gemm_pair(const OzakiOperand& a, const OzakiOperand& b, const OzakiGemmArgs& args,
+                             cudaStream_t stream) {
+  constexpr int kStages = 6;
+  CUtensorMap tmA, tmB;
+  if (!make_tensor_map_3d(&tmA, a.digits, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, uint64_t(a.k_pad), uint64_t(a.rows_pad),
+                          uint64_t(a.smax), kSliceKBytes, kSliceBM))
+    return cudaErrorInvalidValue;
+  if (!make_tensor_map_3d(&tmB, b.digits, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, uint64_t(b.k_pad), uint64_t(b.rows_pad),
+                          uint64_t(b.smax), kSliceKBytes, kPairBN / 2))
+    return cudaErrorInvalidValue;
+  SliceGemmParams P{};
+  P.m = args.m;
+  P.n = args.n;
+  P.num_kb = int(a.k_pad / kSliceKBytes);
+  P.tiles_m = int(a.rows_pad / (2 * kSliceBM));
+  P.tiles_n = int(b.rows_pad / kPairBN);
+  P.slices = args.slices;
+  P.diag_lo = args.diag_lo;
+  P.diag_hi = args.diag_hi;
+  P.first_writes = args.first_writes ? 1 : 0;
+  P.alpha = args.alpha;
+  P.beta = args.beta;
+  P.C = args.C;
+  P.ldc = args.ldc;
+  P.expA = a.exps;
+  P.expB = b.exps;
+  P.skip_if_flag = args.skip_if_flag;
+  P.err_sq = args.err_sq;
+  P.status = args.status;
+  P.group_m = tuning().group_m > 0 ? tuning().group_m : P.tiles_m;
+  P.prefetch = 0;
+  return launch_slice_pair<kModeOzakiI8, kStages>(tmA, tmB, P, args.num_sms, stream);
+}
+
 }  // namespace
 
 cudaError_t launch_ozaki_scan_reset(const OzakiOperand& op, cudaStream_t stream) {
@@ -229,6 +263,10 @@ cudaError_t launch_ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, cons
   if (args.slices < 1 || args.slices > a.smax || args.slices > b.smax) return cudaErrorInvalidValue;
   if (a.k_pad != b.k_pad || a.k_pad % kSliceKBytes != 0 || a.rows_pad % kSliceBM != 0)
     return cudaErrorInvalidValue;
+  if (args.tile_n == kTilePair) {
+    if (b.rows_pad % kPairBN != 0 || a.rows_pad % (2 * kSliceBM) != 0) return cudaErrorInvalidValue;
+    return launch_gemm_pair(a, b, args, stream);
+  }
   if (args.tile_n == 256) {
     if (b.rows_pad % 256 != 0) return cudaErrorInvalidValue;
     return launch_gemm_tiles<256, 4>(a, b, args, stream);

@@ -91,13 +91,13 @@ __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, 
 
 // Walks the (tile, diagonal, pair, k-block) schedule in issue order.
 struct BlockIter {
-  int tile, t, f, p_lo, total;
+  int tile, t, f, p_lo, total, stride;
   bool valid;
   __device__ __forceinline__ void settle(const SliceGemmParams& P, int num_tiles) {
     valid = false;
     while (tile < num_tiles) {
       if (t < P.diag_lo) {
-        tile += gridDim.x;
+        tile += stride;
         t = P.diag_hi;
         f = 0;
         continue;
@@ -111,8 +111,9 @@ struct BlockIter {
       return;
     }
   }
-  __device__ __forceinline__ void start(const SliceGemmParams& P, int num_tiles) {
-    tile = blockIdx.x;
+  __device__ __forceinline__ void start(const SliceGemmParams& P, int num_tiles, int first, int step) {
+    tile = first;
+    stride = step;
     t = P.diag_hi;
     f = 0;
     settle(P, num_tiles);
@@ -148,8 +149,8 @@ __device__ __forceinline__ void slice_producer(const CUtensorMap* tmA, const CUt
   constexpr int ke = SliceTraits<MODE>::kKElems;  // innermost coordinate step (elements)
   const int num_tiles = P.tiles_m * P.tiles_n;
   BlockIter it, pf;
-  it.start(P, num_tiles);
-  pf.start(P, num_tiles);
+  it.start(P, num_tiles, blockIdx.x, gridDim.x);
+  pf.start(P, num_tiles, blockIdx.x, gridDim.x);
   for (int i = 0; i < P.prefetch && pf.valid; ++i) {
     int tm, tn;
     tile_coords(pf.tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
@@ -272,7 +273,17 @@ __device__ __forceinline__ void slice_mma(uint8_t* smem, uint64_t* full, uint64_
 // ------------------------------------------------------------------ epilogues
 // Ozaki: C(i,j) (+)= alpha * 2^(e_i + f_j - 12 - 7(t-2)) * D_t(i,j), diagonals from the
 // smallest weight up; the first unit of a tile applies beta (beta == 0 never reads C).
-template <int BN, int STAGES>
+// PAIR: the CTA is half of a 256-row pair tile (rows rank*128 .. +127) and releases the
+// accumulator on the pair leader's barrier; otherwise it owns a 128-row tile.
+template <int BN, bool PAIR>
+__device__ __forceinline__ void acc_release(uint64_t* tempty_buf) {
+  if (PAIR)
+    mbar_arrive_cluster(mapa_shared(smem_u32(tempty_buf), 0));
+  else
+    mbar_arrive(tempty_buf);
+}
+
+template <int BN, bool PAIR>
 __device__ __forceinline__ void ozaki_epilogue(uint32_t tmem_base, uint64_t* tfull, uint64_t* tempty, int* col_exp,
                                                volatile int* abort_flag, const SliceGemmParams& P) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -285,10 +296,13 @@ __device__ __forceinline__ void ozaki_epilogue(uint32_t tmem_base, uint64_t* tfu
   uint32_t ephase = 0u;
   double err_hi = 0.0, err_lo = 0.0;
   bool ok = true;
-  for (int tile = blockIdx.x; tile < num_tiles && ok; tile += gridDim.x) {
+  const int first = PAIR ? int(blockIdx.x >> 1) : int(blockIdx.x);
+  const int step = PAIR ? int(gridDim.x >> 1) : int(gridDim.x);
+  const int row_base = PAIR ? int(cluster_ctarank()) * kSliceBM : 0;
+  for (int tile = first; tile < num_tiles && ok; tile += step) {
     int tm, tn;
     tile_coords(tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
-    const int64_t m0 = int64_t(tm) * kSliceBM;
+    const int64_t m0 = int64_t(tm) * (PAIR ? 2 * kSliceBM : kSliceBM) + row_base;
     const int64_t n0 = int64_t(tn) * BN;
     for (int j = et; j < BN; j += 128) {
       const int64_t col = n0 + j;
@@ -338,7 +352,7 @@ __device__ __forceinline__ void ozaki_epilogue(uint32_t tmem_base, uint64_t* tfu
           }
         }
         tc_fence_before();
-        mbar_arrive(&tempty[buf]);
+        acc_release<BN, PAIR>(&tempty[buf]);
         ephase ^= 1u << buf;
         buf ^= 1;
         first = false;
@@ -358,7 +372,7 @@ __device__ __forceinline__ void ozaki_epilogue(uint32_t tmem_base, uint64_t* tfu
 }
 
 // Split-BF16: C = alpha * acc + beta * C in FP32, one unit per tile.
-template <int BN, int STAGES>
+template <int BN, bool PAIR>
 __device__ __forceinline__ void bf16_epilogue(uint32_t tmem_base, uint64_t* tfull, uint64_t* tempty,
                                               volatile int* abort_flag, const SliceGemmParams& P) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -368,10 +382,13 @@ __device__ __forceinline__ void bf16_epilogue(uint32_t tmem_base, uint64_t* tful
   float* C = static_cast<float*>(P.C);
   int buf = 0;
   uint32_t ephase = 0u;
-  for (int tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
+  const int first = PAIR ? int(blockIdx.x >> 1) : int(blockIdx.x);
+  const int step = PAIR ? int(gridDim.x >> 1) : int(gridDim.x);
+  const int row_base = PAIR ? int(cluster_ctarank()) * kSliceBM : 0;
+  for (int tile = first; tile < num_tiles; tile += step) {
     int tm, tn;
     tile_coords(tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
-    const int64_t m0 = int64_t(tm) * kSliceBM;
+    const int64_t m0 = int64_t(tm) * (PAIR ? 2 * kSliceBM : kSliceBM) + row_base;
     const int64_t n0 = int64_t(tn) * BN;
     if (!mbar_wait(&tfull[buf], (ephase >> buf) & 1u, abort_flag, P.status)) break;
     tc_fence_after();
@@ -395,7 +412,7 @@ __device__ __forceinline__ void bf16_epilogue(uint32_t tmem_base, uint64_t* tful
       }
     }
     tc_fence_before();
-    mbar_arrive(&tempty[buf]);
+    acc_release<BN, PAIR>(&tempty[buf]);
     ephase ^= 1u << buf;
     buf ^= 1;
   }
@@ -455,9 +472,9 @@ __global__ void __launch_bounds__(192, 1)
     if (lane == 0) slice_mma<MODE, BN, STAGES>(smem, full, empty, tfull, tempty, drain, tmem_base, abort_flag, P);
   } else {
     if (MODE == kModeOzakiI8)
-      ozaki_epilogue<BN, STAGES>(tmem_base, tfull, tempty, col_exp, abort_flag, P);
+      ozaki_epilogue<BN, false>(tmem_base, tfull, tempty, col_exp, abort_flag, P);
     else
-      bf16_epilogue<BN, STAGES>(tmem_base, tfull, tempty, abort_flag, P);
+      bf16_epilogue<BN, false>(tmem_base, tfull, tempty, abort_flag, P);
   }
 
   tc_fence_before();
@@ -466,4 +483,228 @@ __global__ void __launch_bounds__(192, 1)
   if (warp == 1) tmem_dealloc(tmem_base, 2 * BN);
 }
 
+
+// ======================================================================= CTA pairs
+// A cluster of two CTAs computes a 256 x 256 tile with tcgen05 cta_group::2: each CTA
+// loads its 128 rows of A and its 128 of the 256 rows of B per stage (32 KB, 6 stages)
+// and holds its 128 x 256 half of the accumulator in its own TMEM; the leader (rank 0)
+// issues the M = 256 MMAs.  Per SM this moves 2/3 of the bytes of the single-CTA tile
+// for the same MMA work.  TMA loads carry no multicast; the leader commits separately to
+// both CTAs' barriers.
+constexpr int kPairBN = 256;
+
+template <int STAGES>
+struct SlicePairLayout {
+  static constexpr int kABytes = kSliceBM * kSliceKBytes;          // 128 rows of A
+  static constexpr int kBBytes = (kPairBN / 2) * kSliceKBytes;     // 128 rows of B
+  static constexpr int kAOff = 0;
+  static constexpr int kBOff = kAOff + STAGES * kABytes;
+  static constexpr int kBarOff = kBOff + STAGES * kBBytes;
+  static constexpr int kNumBars = 2 * STAGES + 5;
+  static constexpr int kMiscOff = kBarOff + kNumBars * 8;
+  static constexpr int kColExpOff = kMiscOff + 16;
+  static constexpr int kTotal = kColExpOff + kPairBN * 4;
+  static constexpr int kAlloc = kTotal + 1024;
+};
+
+template <int MODE, int STAGES>
+__device__ __forceinline__ void pair_producer(const CUtensorMap* tmA, const CUtensorMap* tmB, uint8_t* smem,
+                                              uint64_t* full, uint64_t* empty, volatile int* abort_flag,
+                                              const SliceGemmParams& P, uint32_t rank) {
+  using L = SlicePairLayout<STAGES>;
+  constexpr int ke = SliceTraits<MODE>::kKElems;
+  const int num_tiles = P.tiles_m * P.tiles_n;
+  BlockIter it;
+  it.start(P, num_tiles, int(blockIdx.x >> 1), int(gridDim.x >> 1));
+  uint32_t issued = 0;
+  while (it.valid) {
+    int tm, tn;
+    tile_coords(it.tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
+    const int p = it.p_lo + it.f / P.num_kb, kb = it.f % P.num_kb;
+    const int stage = int(issued % STAGES);
+    if (!mbar_wait(&empty[stage], ((issued / STAGES) & 1u) ^ 1u, abort_flag, P.status)) break;
+    const uint32_t leader_full = mapa_shared(smem_u32(&full[stage]), 0);
+    if (rank == 0) mbar_arrive_expect_tx(&full[stage], 2 * (L::kABytes + L::kBBytes));
+    tma_load_3d_pair(smem + L::kAOff + stage * L::kABytes, tmA, leader_full, kb * ke,
+                     tm * 2 * kSliceBM + int(rank) * kSliceBM, p - 1);
+    tma_load_3d_pair(smem + L::kBOff + stage * L::kBBytes, tmB, leader_full, kb * ke,
+                     tn * kPairBN + int(rank) * (kPairBN / 2), it.t - p - 1);
+    ++issued;
+    it.next(P, num_tiles);
+  }
+}
+
+template <int MODE, int STAGES>
+__device__ __forceinline__ void pair_mma(uint8_t* smem, uint64_t* full, uint64_t* empty, uint64_t* tfull,
+                                         uint64_t* tempty, uint64_t* drain, uint32_t tmem_base,
+                                         volatile int* abort_flag, const SliceGemmParams& P) {
+  using L = SlicePairLayout<STAGES>;
+  constexpr uint32_t idesc = MODE == kModeOzakiI8 ? make_idesc(2u, 1u, 1u, 2 * kSliceBM, kPairBN)
+                                                  : make_idesc(1u, 1u, 1u, 2 * kSliceBM, kPairBN);
+  constexpr bool kTileUnit = (MODE == kModeSplitBF16);
+  const int num_tiles = P.tiles_m * P.tiles_n;
+  uint32_t consumed = 0;
+  int buf = 0;
+  uint32_t tphase = 0u;
+  bool ok = true;
+  auto commit_both = [&](uint64_t* bar) {
+    const uint32_t a = smem_u32(bar);
+    mma_commit_pair(mapa_shared(a, 0));
+    mma_commit_pair(mapa_shared(a, 1));
+  };
+  for (int tile = int(blockIdx.x >> 1); tile < num_tiles && ok; tile += int(gridDim.x >> 1)) {
+    bool fresh = true;
+    if (kTileUnit) {
+      if (!mbar_wait(&tempty[buf], ((tphase >> buf) & 1u) ^ 1u, abort_flag, P.status)) break;
+      tc_fence_after();
+    }
+    for (int t = P.diag_hi; t >= P.diag_lo && ok; --t) {
+      int p_lo, total;
+      if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total)) continue;
+      for (int u0 = 0; u0 < total && ok; u0 += kMaxUnitKb) {
+        const int u1 = (kTileUnit || total - u0 <= kMaxUnitKb) ? total : u0 + kMaxUnitKb;
+        if (!kTileUnit) {
+          if (!mbar_wait(&tempty[buf], ((tphase >> buf) & 1u) ^ 1u, abort_flag, P.status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          fresh = true;
+        }
+        const uint32_t d_tmem = tmem_base + uint32_t(buf * kPairBN);
+        for (int f = u0; f < u1; ++f) {
+          const int stage = int(consumed % STAGES);
+          if (!mbar_wait(&full[stage], (consumed / STAGES) & 1u, abort_flag, P.status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint64_t adesc = make_sw128_kmajor_desc(smem_u32(smem + L::kAOff + stage * L::kABytes));
+          const uint64_t bdesc = make_sw128_kmajor_desc(smem_u32(smem + L::kBOff + stage * L::kBBytes));
+#pragma unroll
+          for (int kk = 0; kk < kSliceKBytes / 32; ++kk) {
+            const uint32_t acc = (fresh && kk == 0) ? 0u : 1u;
+            if (MODE == kModeOzakiI8)
+              mma_i8_pair(d_tmem, adesc + uint64_t(2 * kk), bdesc + uint64_t(2 * kk), idesc, acc);
+            else
+              mma_f16_pair(d_tmem, adesc + uint64_t(2 * kk), bdesc + uint64_t(2 * kk), idesc, acc);
+          }
+          fresh = false;
+          commit_both(&empty[stage]);
+          ++consumed;
+        }
+        if (!ok) break;
+        if (!kTileUnit) {
+          commit_both(&tfull[buf]);
+          tphase ^= 1u << buf;
+          buf ^= 1;
+        }
+        if (kTileUnit) u0 = total;
+      }
+    }
+    if (kTileUnit && ok) {
+      commit_both(&tfull[buf]);
+      tphase ^= 1u << buf;
+      buf ^= 1;
+    }
+  }
+  mma_commit_pair(mapa_shared(smem_u32(drain), 0));
+  volatile int no_abort = 0;
+  (void)mbar_wait(drain, 0, &no_abort, P.status);
+}
+
+template <int MODE, int STAGES>
+__global__ void __launch_bounds__(192, 1)
+    slice_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                           const SliceGemmParams P) {
+  using L = SlicePairLayout<STAGES>;
+  // both CTAs of a pair read the same flag, so they leave together
+  if (P.skip_if_flag && *P.skip_if_flag) return;
+
+  extern __shared__ uint8_t pair_smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(pair_smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::kBarOff);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + STAGES;
+  uint64_t* tfull = bars + 2 * STAGES;
+  uint64_t* tempty = bars + 2 * STAGES + 2;
+  uint64_t* drain = bars + 2 * STAGES + 4;
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(smem + L::kMiscOff);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L::kMiscOff + 4);
+  int* col_exp = reinterpret_cast<int*>(smem + L::kColExpOff);
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < STAGES; ++i) {
+      mbar_init(&full[i], 1);   // the leader's expect_tx arrival + both CTAs' bytes
+      mbar_init(&empty[i], 1);  // one commit from the leader's MMA thread
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&tfull[i], 1);
+      mbar_init(&tempty[i], 2 * 128);  // used on the leader: both CTAs' epilogue threads
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+  }
+  if (warp == 0 && lane == 0) {
+    tma_prefetch_desc(&tmA);
+    tma_prefetch_desc(&tmB);
+  }
+  if (warp == 1) {
+    tmem_alloc_pair(tmem_holder, 2 * kPairBN);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  cluster_sync();  // barriers of both CTAs are initialised before any remote arrival
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_holder;
+
+  if (warp == 0) {
+    if (lane == 0) pair_producer<MODE, STAGES>(&tmA, &tmB, smem, full, empty, abort_flag, P, rank);
+  } else if (warp == 1) {
+    if (lane == 0 && rank == 0)
+      pair_mma<MODE, STAGES>(smem, full, empty, tfull, tempty, drain, tmem_base, abort_flag, P);
+  } else {
+    if (MODE == kModeOzakiI8)
+      ozaki_epilogue<kPairBN, true>(tmem_base, tfull, tempty, col_exp, abort_flag, P);
+    else
+      bf16_epilogue<kPairBN, true>(tmem_base, tfull, tempty, abort_flag, P);
+  }
+
+  tc_fence_before();
+  cluster_sync();  // the pair's MMAs are drained and both epilogues are done with TMEM
+  tc_fence_after();
+  if (warp == 1) tmem_dealloc_pair(tmem_base, 2 * kPairBN);
+}
+
+
+// Host-side launch of the pair kernel (grid = 2 CTAs per pair, clusters of 2).
+template <int MODE, int STAGES>
+inline cudaError_t launch_slice_pair(const CUtensorMap& tmA, const CUtensorMap& tmB, const SliceGemmParams& P,
+                                     int num_sms, cudaStream_t stream) {
+  using L = SlicePairLayout<STAGES>;
+  auto kern = slice_gemm_pair_kernel<MODE, STAGES>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kAlloc);
+  if (e != cudaSuccess) return e;
+  const int tiles = P.tiles_m * P.tiles_n;
+  const int pairs = tiles < num_sms / 2 ? tiles : num_sms / 2;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(2 * pairs), 1, 1);
+  cfg.blockDim = dim3(192, 1, 1);
+  cfg.dynamicSmemBytes = L::kAlloc;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, tmA, tmB, P);
+}
+
 }  // namespace eb2
+

@@ -85,7 +85,8 @@ int eb2_set_dgemm_tolerance(double tol);
 /* BF16 pieces per FP32 operand for the emulated SGEMM: 2 keeps the three products
  * hi*hi + hi*mid + mid*hi ("bf16x3"), 3 adds mid*mid + hi*lo + lo*hi ("bf16x6", default). */
 int eb2_set_sgemm_pieces(int pieces);
-/* Output-tile width of the tcgen05 kernels: 128, 256 or 0 (= chosen per call). */
+/* Tile configuration of the tcgen05 kernels: 128 or 256 (one CTA per 128 x 128 or
+ * 128 x 256 tile), 512 (a CTA pair per 256 x 256 tile) or 0 (= chosen per call). */
 int eb2_set_tile_n(int tile_n);
 
 /* Launch-shape knobs of the tcgen05 kernels (normally set by the tuner): row-tiles per
@@ -127,6 +128,42 @@ int eb2_dgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, 
                      int check_accuracy);
 int eb2_sgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, float alpha, const float* a,
                      int64_t lda, const float* b, int64_t ldb, float beta, float* c, int64_t ldc, void* stream);
+
+/* ---------------------------------------------------------------- grouped products
+ * Thousands of independent products C_i = alpha_i*op(A_i)op(B_i) + beta_i*C_i (device
+ * pointers, column-major) in ONE persistent launch.  Eigen has no batch entry point;
+ * this is the batched counterpart of its fixed-size coefficient-based products
+ * (Eigen/src/Core/GeneralProduct.h:76-80) and of per-product GEMM calls.  The math is
+ * native FP64 (DMMA) for dtype 'd' and FP32 (FFMA) for 's', i.e. the same accuracy class
+ * as one plain call per product. */
+typedef struct eb2_gemm_problem {
+  char transa, transb;   /* 'N', 'T' or 'C' */
+  int64_t m, n, k;
+  double alpha, beta;    /* rounded to float for dtype 's' */
+  const void* a;
+  int64_t lda;
+  const void* b;
+  int64_t ldb;
+  void* c;
+  int64_t ldc;
+} eb2_gemm_problem;
+
+typedef struct eb2_grouped_plan* eb2_grouped_plan_t;
+
+/* Validates the problems (BLAS argument rules; EB2_ERR_ARG names the first bad one),
+ * uploads their descriptors and the tile schedule, and captures the launch in a CUDA
+ * graph.  `problems` is a host array; it may be freed after the call. */
+int eb2_grouped_plan_create(char dtype, int64_t count, const eb2_gemm_problem* problems, eb2_grouped_plan_t* plan);
+/* Replays the captured launch on `stream` (stream-ordered, no host synchronisation). */
+int eb2_grouped_plan_execute(eb2_grouped_plan_t plan, void* stream);
+int eb2_grouped_plan_destroy(eb2_grouped_plan_t plan);
+/* One-shot: plan, launch on `stream`, wait, release. */
+int eb2_gemm_grouped(char dtype, int64_t count, const eb2_gemm_problem* problems, void* stream);
+
+/* The same products as separate plain launches of the native kernels, one per product,
+ * stream-ordered: what a caller looping over dgemm_/sgemm_ gets, without the host
+ * synchronisation.  The baseline the grouped launch is measured against. */
+int eb2_gemm_each(char dtype, int64_t count, const eb2_gemm_problem* problems, void* stream);
 
 /* Library version string. */
 const char* eb2_version(void);

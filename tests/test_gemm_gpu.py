@@ -87,7 +87,8 @@ SHAPES = [("N", "N", 130, 300, 257), ("T", "N", 64, 64, 1000), ("N", "T", 333, 1
 
 
 @pytest.mark.parametrize("ta,tb,m,n,k", SHAPES)
-@pytest.mark.parametrize("s,tile_n,beta", [(3, 128, 0.0), (8, 256, 0.0), (8, 128, 0.5), (5, 256, -1.25)])
+@pytest.mark.parametrize("s,tile_n,beta", [(3, 128, 0.0), (8, 256, 0.0), (8, 128, 0.5), (5, 256, -1.25),
+                                          (8, 512, 0.0), (4, 512, 0.75)])
 def test_emulated_bit_exact_vs_oracle_model(ta, tb, m, n, k, s, tile_n, beta):
     """Digit split, INT8 digit products and FP64 recombination equal the oracle's
     model (oracle_ozaki_dgemm) bit for bit."""
@@ -294,6 +295,17 @@ def test_sgemm_split_bf16_accuracy(ta, tb, m, n, k):
     # round-to-nearest chain; both stay far inside the lam*sqrt(k)*eps product bound
     assert e6 <= max(4 * e_nat, 2.0 ** -19), (e6, e_nat)
     assert e3 < 2.0 ** -15, e3
+
+
+@pytest.mark.parametrize("tile_n", [128, 256, 512])
+def test_sgemm_split_bf16_tile_configs(tile_n):
+    """Every tile configuration (one CTA 128x128 / 128x256, CTA pair 256x256) gives the
+    same FP32-level accuracy on odd shapes."""
+    eb.set_sgemm_method(eb.METHOD_EMULATED)
+    eb.set_tile_n(tile_n)
+    e = _sgemm_rel_err(300, 517, 700, "T", "N", seed=7)
+    assert eb.last_call_info()["tile_n"] == tile_n
+    assert e < 2.0 ** -19, e
 
 
 def test_sgemm_emulated_nonfinite_falls_back():
