@@ -50,6 +50,7 @@ class CallInfo(ctypes.Structure):
         ("kernel_ms", ctypes.c_double),
         ("gemm_kernel_ms", ctypes.c_double),
         ("launches", ctypes.c_int),
+        ("spread", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -117,6 +118,17 @@ def load(path: str | os.PathLike | None = None, mode: int = ctypes.RTLD_GLOBAL) 
     lib.eb2_grouped_plan_destroy.argtypes = [ctypes.c_void_p]
     lib.eb2_gemm_grouped.argtypes = [ctypes.c_char, ctypes.c_int64, pp, ctypes.c_void_p]
     lib.eb2_gemm_each.argtypes = [ctypes.c_char, ctypes.c_int64, pp, ctypes.c_void_p]
+    fp = ctypes.POINTER(ctypes.c_float)
+    ip = ctypes.POINTER(ctypes.c_int)
+    lib.eb2_picker_set_weights.argtypes = [vp, ctypes.c_int]
+    lib.eb2_picker_features.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_char, ctypes.c_double,
+                                        ctypes.c_int64, vp]
+    lib.eb2_picker_forward_host.argtypes = [vp, vp, vp]
+    lib.eb2_picker_predict.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_char, ctypes.c_double,
+                                       ctypes.c_int64, ip, ip]
+    lib.eb2_mlp_forward.argtypes = [vp, vp, ctypes.c_int, vp, vp]
+    lib.eb2_mlp_backward.argtypes = [vp, vp, vp, vp, ctypes.c_int, vp, vp, vp]
+    lib.eb2_mlp_adam.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_float, vp]
     _lib = lib
     return lib
 
@@ -196,6 +208,17 @@ def set_tile_n(tile_n: int) -> int:
 
 def set_slice_tuning(group_m: int, prefetch: int) -> int:
     return load().eb2_set_slice_tuning(group_m, prefetch)
+
+
+def set_picker(weights) -> int:
+    """Install picker weights (a float32 array of eb2_mlp_param_count() entries) or None."""
+    lib = load()
+    if weights is None:
+        return lib.eb2_picker_set_weights(None, 0)
+    import numpy as np
+
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    return lib.eb2_picker_set_weights(w.ctypes.data_as(ctypes.c_void_p), int(w.size))
 
 
 def set_timing(on: bool) -> int:

@@ -1,6 +1,7 @@
 // context.cpp -- see context.h.
 #include "context.h"
 #include "kernels.h"
+#include "mlp.h"
 
 #include <cstdarg>
 #include <cstdio>
@@ -11,7 +12,7 @@ namespace eb2 {
 namespace {
 thread_local int t_error = EB2_OK;
 thread_local char t_message[512] = "";
-thread_local eb2_call_info t_info = {0, 0, 0, 0, 0, 0, 0, -1.0, -1.0, -1.0, 0};
+thread_local eb2_call_info t_info = {0, 0, 0, 0, 0, 0, 0, -1.0, -1.0, -1.0, 0, 0.0};
 thread_local Context* t_pending = nullptr;
 thread_local bool t_pending_gemm = false;
 
@@ -126,6 +127,8 @@ Context* current_context() {
   }
   std::memset(c->hflags, 0, sizeof(DeviceFlags));
   g_ctx[dev] = c;
+  static std::once_flag picker_once;
+  std::call_once(picker_once, [&] { picker_autoload(c->num_sms); });
   return c;
 }
 

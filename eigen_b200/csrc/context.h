@@ -26,6 +26,7 @@ struct DeviceFlags {
   int nonfinite;
   uint32_t status;
   double err_sq[2];
+  double spread[2];  // exponent-spread statistic of the scans: sum, count
 };
 
 struct Context {

@@ -12,14 +12,18 @@
 #include <cstring>
 
 #include "kernels.h"
+#include "mlp.h"
 
 namespace eb2 {
 
 namespace {
 
-// Rows / columns of C covered by one tile of a tile configuration.
-int64_t tile_m_of(int cfg) { return cfg == kTilePair ? 256 : 128; }
-int64_t tile_n_of(int cfg) { return cfg == kTilePair ? 256 : cfg; }
+// Rows / columns of C covered by one tile of a tile configuration.  The Ozaki GEMM keeps
+// its FP64 accumulator in registers, so its tiles are 128 columns wide (128 and 256
+// select one CTA / a CTA pair); the split-BF16 GEMM uses 128 / 256 wide single-CTA tiles
+// and 256 x 256 pair tiles.
+int64_t tile_m_of(int cfg, bool ozaki) { return (cfg == kTilePair || (ozaki && cfg == 256)) ? 256 : 128; }
+int64_t tile_n_of(int cfg, bool ozaki) { return ozaki ? 128 : (cfg == kTilePair ? 256 : cfg); }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
@@ -43,9 +47,14 @@ StridedView<double> view_bt(bool tb, const double* B, int64_t ldb, int64_t n, in
 
 }  // namespace
 
-int choose_tile_n(const Context& cx, int64_t m, int64_t n) {
+int choose_tile_n(const Context& cx, int64_t m, int64_t n, bool ozaki) {
   const int forced = settings().tile_n.load();
   if (forced == 128 || forced == 256 || forced == kTilePair) return forced;
+  if (ozaki) {
+    // CTA pairs (256 x 128) unless that leaves most SMs idle
+    const int64_t pair_tiles = ((m + 255) / 256) * ((n + 127) / 128);
+    return 2 * pair_tiles >= cx.num_sms ? kTilePair : 128;
+  }
   if (n <= 128) return 128;
   const int64_t tiles256 = ((m + 127) / 128) * ((n + 255) / 256);
   return tiles256 < cx.num_sms ? 128 : 256;
@@ -72,6 +81,7 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   info.kernel_ms = -1.0;
   info.gemm_kernel_ms = -1.0;
   info.launches = 0;
+  info.spread = 0.0;
   set_pending_timing(nullptr, false);
   if (m == 0 || n == 0) return EB2_OK;
   if (k == 0 || alpha == 0.0) {
@@ -81,16 +91,26 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
     return check_cuda(launch_scale_matrix_d(m, n, beta, C, ldc, st), "scale C") ? EB2_OK : EB2_ERR_CUDA;
   }
   int method = opt.method ? opt.method : settings().dgemm_method.load();
+  // The learned picker decides what is left automatic: method (when AUTO), tile
+  // configuration and slice count.  Stage 1 uses the shape only.
+  const bool auto_method = (method == EB2_METHOD_AUTO);
+  const bool auto_tile = !opt.tile_n && settings().tile_n.load() == 0;
+  const bool auto_slices = !opt.slices && settings().dgemm_slices.load() == 0;
+  const bool use_picker = picker_weights() != nullptr && (auto_method || auto_tile || auto_slices);
+  int pick_cfg = -1, pick_s = 0;
+  if (use_picker && picker_predict(m, n, k, 'd', 0.0, 1, &pick_cfg, &pick_s) && auto_method && pick_cfg == 0)
+    method = EB2_METHOD_NATIVE;
   if (method == EB2_METHOD_AUTO) method = EB2_METHOD_EMULATED;
   info.method = method;
 
-  if (opt.timed) cudaEventRecord(cx.ev_start, st);
-  if (method == EB2_METHOD_NATIVE) {
+  auto run_native = [&](bool from_auto) -> int {
+    info.method = EB2_METHOD_NATIVE;
+    if (opt.timed && !from_auto) cudaEventRecord(cx.ev_start, st);
     if (opt.timed) cudaEventRecord(cx.ev_gemm0, st);
     if (!check_cuda(launch_dgemm_native(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, st),
                     "native DGEMM"))
       return EB2_ERR_CUDA;
-    info.launches = 1;
+    info.launches += 1;
     if (opt.timed) {
       cudaEventRecord(cx.ev_gemm1, st);
       cudaEventRecord(cx.ev_stop, st);
@@ -98,47 +118,70 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
     }
     if (opt.sync && !check_cuda(cudaStreamSynchronize(st), "DGEMM")) return EB2_ERR_CUDA;
     return EB2_OK;
-  }
+  };
+  if (method == EB2_METHOD_NATIVE) return run_native(false);
+  if (opt.timed) cudaEventRecord(cx.ev_start, st);
 
   // ---------------------------------------------------------- Ozaki emulation
-  const int tile_n = opt.tile_n ? opt.tile_n : choose_tile_n(cx, m, n);
-  int s = opt.slices ? opt.slices : choose_slices(m, n, k);
+  // Workspace: scan results first (they must survive the stage-2 decision), then the
+  // exponents and digit panels, sized for the largest tile padding and slice count the
+  // decision can pick.
   const bool check = opt.check_accuracy;
-  const int smax = check ? std::min(kOzakiMaxSlices, s + 3) : s;
-  const int64_t m_pad = round_up(m, tile_m_of(tile_n)), n_pad = round_up(n, tile_n_of(tile_n)),
-                k_pad = round_up(k, kOzakiKBlock);
-
+  const int s_fixed = opt.slices ? opt.slices : (auto_slices ? 0 : choose_slices(m, n, k));
+  const int smax = (use_picker && s_fixed == 0) || check ? kOzakiMaxSlices : std::max(s_fixed, 8);
+  const int64_t m_cap = round_up(m, 256), n_cap = round_up(n, 256), k_pad = round_up(k, kOzakiKBlock);
   size_t off = 0;
-  const size_t o_dig_a = off;
-  off = align256(off + size_t(smax) * m_pad * k_pad);
-  const size_t o_dig_b = off;
-  off = align256(off + size_t(smax) * n_pad * k_pad);
-  const size_t o_exp_a = off;
-  off = align256(off + size_t(m_pad) * 4);
-  const size_t o_exp_b = off;
-  off = align256(off + size_t(n_pad) * 4);
   const size_t o_mb_a = off;
   off = align256(off + size_t(m) * 8);
   const size_t o_mb_b = off;
   off = align256(off + size_t(n) * 8);
+  const size_t o_exp_a = off;
+  off = align256(off + size_t(m_cap) * 4);
+  const size_t o_exp_b = off;
+  off = align256(off + size_t(n_cap) * 4);
+  const size_t o_dig_a = off;
+  off = align256(off + size_t(smax) * m_cap * k_pad);
+  const size_t o_dig_b = off;
+  off = align256(off + size_t(smax) * n_cap * k_pad);
   if (!cx.ws.ensure(off)) {
     set_error(EB2_ERR_ALLOC, "could not allocate %zu bytes of emulation workspace", off);
     return EB2_ERR_ALLOC;
   }
   uint8_t* ws = static_cast<uint8_t*>(cx.ws.ptr);
-  OzakiOperand oa{reinterpret_cast<int8_t*>(ws + o_dig_a), reinterpret_cast<int32_t*>(ws + o_exp_a),
-                  reinterpret_cast<uint64_t*>(ws + o_mb_a), nullptr, m, m_pad, k, k_pad, smax};
-  OzakiOperand ob{reinterpret_cast<int8_t*>(ws + o_dig_b), reinterpret_cast<int32_t*>(ws + o_exp_b),
-                  reinterpret_cast<uint64_t*>(ws + o_mb_b), nullptr, n, n_pad, k, k_pad, smax};
   const StridedView<double> va = view_a(ta, A, lda, m, k);
   const StridedView<double> vb = view_bt(tb, B, ldb, n, k);
   DeviceFlags* df = cx.dflags;
+  OzakiOperand oa{reinterpret_cast<int8_t*>(ws + o_dig_a), reinterpret_cast<int32_t*>(ws + o_exp_a),
+                  reinterpret_cast<uint64_t*>(ws + o_mb_a), nullptr, m, m_cap, k, k_pad, smax};
+  OzakiOperand ob{reinterpret_cast<int8_t*>(ws + o_dig_b), reinterpret_cast<int32_t*>(ws + o_exp_b),
+                  reinterpret_cast<uint64_t*>(ws + o_mb_b), nullptr, n, n_cap, k, k_pad, smax};
 
   bool ok = check_cuda(cudaMemsetAsync(df, 0, sizeof(DeviceFlags), st), "reset flags");
   ok = ok && check_cuda(launch_ozaki_scan_reset(oa, st), "scan reset A");
   ok = ok && check_cuda(launch_ozaki_scan_reset(ob, st), "scan reset B");
-  ok = ok && check_cuda(launch_ozaki_scan(va, oa, &df->nonfinite, st), "scan A");
-  ok = ok && check_cuda(launch_ozaki_scan(vb, ob, &df->nonfinite, st), "scan B");
+  ok = ok && check_cuda(launch_ozaki_scan(va, oa, &df->nonfinite, &df->spread[0], st), "scan A");
+  ok = ok && check_cuda(launch_ozaki_scan(vb, ob, &df->nonfinite, &df->spread[0], st), "scan B");
+  if (!ok) return EB2_ERR_CUDA;
+  info.launches = 2;
+
+  // Stage 2: with the inputs' exponent spread known, pick tile and slices.
+  int tile_n = opt.tile_n ? opt.tile_n : choose_tile_n(cx, m, n, true);
+  int s = s_fixed ? s_fixed : choose_slices(m, n, k);
+  if (use_picker) {
+    if (!check_cuda(cudaMemcpyAsync(cx.hflags, df, sizeof(DeviceFlags), cudaMemcpyDeviceToHost, st), "read scan") ||
+        !check_cuda(cudaStreamSynchronize(st), "scan"))
+      return EB2_ERR_CUDA;
+    const double spread = cx.hflags->spread[1] > 0 ? cx.hflags->spread[0] / cx.hflags->spread[1] : 0.0;
+    info.spread = spread;
+    if (picker_predict(m, n, k, 'd', spread, 1, &pick_cfg, &pick_s)) {
+      if (auto_method && pick_cfg == 0 && !cx.hflags->nonfinite) return run_native(true);
+      if (auto_tile && pick_cfg > 0) tile_n = pick_cfg == 1 ? 128 : (pick_cfg == 2 ? 256 : kTilePair);
+      if (auto_slices) s = std::min(pick_s, smax);
+    }
+  }
+  const int64_t m_pad = round_up(m, tile_m_of(tile_n, true)), n_pad = round_up(n, tile_n_of(tile_n, true));
+  oa.rows_pad = m_pad;
+  ob.rows_pad = n_pad;
   ok = ok && check_cuda(launch_ozaki_split(va, oa, 0, s, st), "split A");
   ok = ok && check_cuda(launch_ozaki_split(vb, ob, 0, s, st), "split B");
   OzakiGemmArgs g{};
@@ -166,7 +209,7 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
                                             st),
                         "non-finite fallback");
   if (!ok) return EB2_ERR_CUDA;
-  info.launches = 6;  // 2 scans, 2 splits, GEMM, non-finite fallback (exits at once when unused)
+  info.launches += 4;  // 2 splits, GEMM, non-finite fallback (exits at once when unused)
   if (opt.timed) {
     cudaEventRecord(cx.ev_stop, st);
     set_pending_timing(&cx, true);
@@ -183,6 +226,7 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
         !check_cuda(cudaStreamSynchronize(st), "DGEMM"))
       return EB2_ERR_CUDA;
     const DeviceFlags hf = *cx.hflags;
+    info.spread = hf.spread[1] > 0 ? hf.spread[0] / hf.spread[1] : 0.0;
     if (hf.status != 0) {
       set_error(EB2_ERR_TIMEOUT, "a kernel wait timed out (device status 0x%x); C is invalid", hf.status);
       return EB2_ERR_TIMEOUT;
@@ -262,9 +306,10 @@ int sgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   }
 
   // ---------------------------------------------------------- split-BF16 emulation
-  const int tile_n = opt.tile_n ? opt.tile_n : choose_tile_n(cx, m, n);
+  const int tile_n = opt.tile_n ? opt.tile_n : choose_tile_n(cx, m, n, false);
   const int pieces = opt.pieces ? opt.pieces : settings().sgemm_pieces.load();
-  const int64_t m_pad = round_up(m, tile_m_of(tile_n)), n_pad = round_up(n, tile_n_of(tile_n)), k_pad = round_up(k, 64);
+  const int64_t m_pad = round_up(m, tile_m_of(tile_n, false)), n_pad = round_up(n, tile_n_of(tile_n, false)),
+                k_pad = round_up(k, 64);
   size_t off = 0;
   const size_t o_a = off;
   off = align256(off + size_t(3) * m_pad * k_pad * 2);

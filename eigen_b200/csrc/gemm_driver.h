@@ -26,7 +26,7 @@ struct SgemmOptions {
   bool timed = false;
 };
 
-int choose_tile_n(const Context& cx, int64_t m, int64_t n);
+int choose_tile_n(const Context& cx, int64_t m, int64_t n, bool ozaki);
 int choose_slices(int64_t m, int64_t n, int64_t k);
 
 // C = alpha*op(A)op(B) + beta*C on device pointers.  Returns EB2_*.

@@ -83,8 +83,8 @@ __device__ void tile_f64(const GroupedProblem& pr, int tm, int tn, int lane) {
           const int64_t col = n0 + j * 8 + tig * 2 + cc;
           if (row < pr.m && col < pr.n) {
             double* dst = C + row + col * pr.ldc;
-            const double v = pr.alpha * acc[i][j][h * 2 + cc];
-            *dst = (pr.beta == 0.0) ? v : pr.beta * *dst + v;
+            const double v = __dmul_rn(pr.alpha, acc[i][j][h * 2 + cc]);
+            *dst = (pr.beta == 0.0) ? v : __fma_rn(pr.beta, *dst, v);
           }
         }
 }
@@ -122,8 +122,8 @@ __device__ void tile_f32(const GroupedProblem& pr, int tm, int tn, int lane) {
       const int64_t row = m0 + i, col = n0 + j;
       if (row < pr.m && col < pr.n) {
         float* dst = C + row + col * pr.ldc;
-        const float v = alpha * acc[i][j];
-        *dst = (beta == 0.f) ? v : beta * *dst + v;
+        const float v = __fmul_rn(alpha, acc[i][j]);
+        *dst = (beta == 0.f) ? v : __fmaf_rn(beta, *dst, v);
       }
     }
 }

@@ -57,8 +57,9 @@ struct OzakiOperand {
 
 // Zero the scan accumulators of one operand (maxbits, abssum).
 cudaError_t launch_ozaki_scan_reset(const OzakiOperand& op, cudaStream_t stream);
-// Row maxima and |x| sums; sets *nonfinite when any NaN/Inf is present.
-cudaError_t launch_ozaki_scan(const StridedView<double>& x, const OzakiOperand& op, int* nonfinite,
+// Row maxima and |x| sums; sets *nonfinite when any NaN/Inf is present; accumulates the
+// exponent-spread statistic into spread[0..1] (sum, count) when spread is non-null.
+cudaError_t launch_ozaki_scan(const StridedView<double>& x, const OzakiOperand& op, int* nonfinite, double* spread,
                               cudaStream_t stream);
 // Digits p in [p_begin, p_end) of every row (including zero padding).
 cudaError_t launch_ozaki_split(const StridedView<double>& x, const OzakiOperand& op, int p_begin, int p_end,

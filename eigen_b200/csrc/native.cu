@@ -170,8 +170,8 @@ __global__ void __launch_bounds__(kDThreads, 1)
           const int64_t col = n0 + wn * 32 + j * 8 + tig * 2 + c;
           if (col >= n) continue;
           double* dst = C + row + col * ldc;
-          const double v = alpha * acc[i][j][h * 2 + c];
-          *dst = (beta == 0.0) ? v : beta * *dst + v;
+          const double v = __dmul_rn(alpha, acc[i][j][h * 2 + c]);
+          *dst = (beta == 0.0) ? v : __fma_rn(beta, *dst, v);
         }
       }
 }
@@ -281,8 +281,8 @@ __global__ void __launch_bounds__(kSThreads)
       const int64_t col = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + j - 4);
       if (col >= n) continue;
       float* dst = C + row + col * ldc;
-      const float v = alpha * acc[i][j];
-      *dst = (beta == 0.f) ? v : beta * *dst + v;
+      const float v = __fmul_rn(alpha, acc[i][j]);
+      *dst = (beta == 0.f) ? v : __fmaf_rn(beta, *dst, v);
     }
   }
 }
@@ -294,7 +294,7 @@ __global__ void scale_matrix_kernel(int64_t m, int64_t n, T beta, T* C, int64_t 
        idx += int64_t(gridDim.x) * blockDim.x) {
     const int64_t i = idx % m, j = idx / m;
     T* p = C + i + j * ldc;
-    *p = (beta == T(0)) ? T(0) : beta * *p;
+    *p = (beta == T(0)) ? T(0) : T(beta * *p);
   }
 }
 

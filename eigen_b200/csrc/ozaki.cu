@@ -36,9 +36,13 @@ constexpr uint64_t kInfBits = 0x7FF0000000000000ull;
 // ------------------------------------------------------------------ scan
 constexpr int kScanTile = 64;
 
+// Besides the row maxima, every 8th column tile contributes to the exponent-spread
+// statistic used by the configuration picker: per row chunk, (largest exponent) minus
+// (mean exponent of its nonzero entries), summed in spread[0] with the chunk count in
+// spread[1].
 __global__ void __launch_bounds__(256) ozaki_scan_kernel(const double* __restrict__ X, int64_t rows, int64_t cols,
                                                          int64_t sr, int64_t sl, unsigned long long* maxbits,
-                                                         double* abssum, int* nonfinite) {
+                                                         double* abssum, int* nonfinite, double* spread) {
   __shared__ double tile[kScanTile][kScanTile + 1];
   const int64_t r0 = int64_t(blockIdx.y) * kScanTile;
   const int64_t l0 = int64_t(blockIdx.x) * kScanTile;
@@ -61,14 +65,35 @@ __global__ void __launch_bounds__(256) ozaki_scan_kernel(const double* __restric
   const int t = threadIdx.x;
   if (t < kScanTile) {
     const int64_t r = r0 + t;
+    double chunk_spread = 0.0, chunk_count = 0.0;
     if (r < rows) {
       unsigned long long mb = 0;
+      int esum = 0, ecnt = 0;
       for (int ll = 0; ll < kScanTile; ++ll) {
         unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(fabs(tile[t][ll])));
         mb = b > mb ? b : mb;
+        if (b) {
+          esum += int(b >> 52);
+          ++ecnt;
+        }
       }
       if (mb >= kInfBits) *nonfinite = 1;
       if (mb) atomicMax(&maxbits[r], mb);
+      if (ecnt > 0 && mb < kInfBits) {
+        chunk_spread = double(int(mb >> 52)) - double(esum) / double(ecnt);
+        chunk_count = 1.0;
+      }
+    }
+    if (spread != nullptr && (blockIdx.x & 7) == 0) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        chunk_spread += __shfl_xor_sync(0xffffffffu, chunk_spread, o);
+        chunk_count += __shfl_xor_sync(0xffffffffu, chunk_count, o);
+      }
+      if ((t & 31) == 0 && chunk_count > 0.0) {
+        atomicAdd(&spread[0], chunk_spread);
+        atomicAdd(&spread[1], chunk_count);
+      }
     }
   } else if (abssum != nullptr && t < 2 * kScanTile) {
     const int ll = t - kScanTile;
@@ -152,22 +177,26 @@ __global__ void __launch_bounds__(256) ozaki_split_kernel(const double* __restri
   }
 }
 
-template <int BN, int STAGES>
-cudaError_t launch_gemm_tiles(const OzakiOperand& a, const OzakiOperand& b, const OzakiGemmArgs& args,
-                              cudaStream_t stream) {
-  using L = SliceSmemLayout<BN, STAGES>;
+// Tile configurations of the Ozaki GEMM (the FP64 accumulator lives in registers, so a
+// CTA's tile is 128 x 128 with 8 epilogue warps): one CTA per 128 x 128 tile, or a CTA
+// pair per 256 x 128 tile (the default; half the B bytes per SM).
+template <int BN, int STAGES, bool PAIR>
+cudaError_t launch_config(const OzakiOperand& a, const OzakiOperand& b, const OzakiGemmArgs& args,
+                          cudaStream_t stream) {
+  constexpr int kRowsPerTile = PAIR ? 2 * kSliceBM : kSliceBM;
+  if (a.rows_pad % kRowsPerTile != 0 || b.rows_pad % BN != 0) return cudaErrorInvalidValue;
   CUtensorMap tmA, tmB;
   if (!make_tensor_map_3d(&tmA, a.digits, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, uint64_t(a.k_pad), uint64_t(a.rows_pad),
                           uint64_t(a.smax), kSliceKBytes, kSliceBM))
     return cudaErrorInvalidValue;
   if (!make_tensor_map_3d(&tmB, b.digits, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, uint64_t(b.k_pad), uint64_t(b.rows_pad),
-                          uint64_t(b.smax), kSliceKBytes, BN))
+                          uint64_t(b.smax), kSliceKBytes, PAIR ? BN / 2 : BN))
     return cudaErrorInvalidValue;
   SliceGemmParams P{};
   P.m = args.m;
   P.n = args.n;
   P.num_kb = int(a.k_pad / kSliceKBytes);
-  P.tiles_m = int(a.rows_pad / kSliceBM);
+  P.tiles_m = int(a.rows_pad / kRowsPerTile);
   P.tiles_n = int(b.rows_pad / BN);
   P.slices = args.slices;
   P.diag_lo = args.diag_lo;
@@ -183,48 +212,7 @@ cudaError_t launch_gemm_tiles(const OzakiOperand& a, const OzakiOperand& b, cons
   P.err_sq = args.err_sq;
   P.status = args.status;
   P.group_m = tuning().group_m > 0 ? tuning().group_m : P.tiles_m;
-  P.prefetch = tuning().prefetch;
-  auto kern = slice_gemm_kernel<kModeOzakiI8, BN, STAGES>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kAlloc);
-  if (e != cudaSuccess) return e;
-  const int tiles = P.tiles_m * P.tiles_n;
-  const int grid = tiles < args.num_sms ? tiles : args.num_sms;
-  kern<<<grid, 192, L::kAlloc, stream>>>(tmA, tmB, P);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_gemm_pair(const OzakiOperand& a, const OzakiOperand& b, const OzakiGemmArgs& args,
-                             cudaStream_t stream) {
-  constexpr int kStages = 6;
-  CUtensorMap tmA, tmB;
-  if (!make_tensor_map_3d(&tmA, a.digits, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, uint64_t(a.k_pad), uint64_t(a.rows_pad),
-                          uint64_t(a.smax), kSliceKBytes, kSliceBM))
-    return cudaErrorInvalidValue;
-  if (!make_tensor_map_3d(&tmB, b.digits, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, uint64_t(b.k_pad), uint64_t(b.rows_pad),
-                          uint64_t(b.smax), kSliceKBytes, kPairBN / 2))
-    return cudaErrorInvalidValue;
-  SliceGemmParams P{};
-  P.m = args.m;
-  P.n = args.n;
-  P.num_kb = int(a.k_pad / kSliceKBytes);
-  P.tiles_m = int(a.rows_pad / (2 * kSliceBM));
-  P.tiles_n = int(b.rows_pad / kPairBN);
-  P.slices = args.slices;
-  P.diag_lo = args.diag_lo;
-  P.diag_hi = args.diag_hi;
-  P.first_writes = args.first_writes ? 1 : 0;
-  P.alpha = args.alpha;
-  P.beta = args.beta;
-  P.C = args.C;
-  P.ldc = args.ldc;
-  P.expA = a.exps;
-  P.expB = b.exps;
-  P.skip_if_flag = args.skip_if_flag;
-  P.err_sq = args.err_sq;
-  P.status = args.status;
-  P.group_m = tuning().group_m > 0 ? tuning().group_m : P.tiles_m;
-  P.prefetch = 0;
-  return launch_slice_pair<kModeOzakiI8, kStages>(tmA, tmB, P, args.num_sms, stream);
+  return launch_slice_gemm<kModeOzakiI8, BN, STAGES, 8, PAIR>(tmA, tmB, P, args.num_sms, stream);
 }
 
 }  // namespace
@@ -235,14 +223,14 @@ cudaError_t launch_ozaki_scan_reset(const OzakiOperand& op, cudaStream_t stream)
   return cudaMemsetAsync(op.abssum, 0, size_t(op.k) * sizeof(double), stream);
 }
 
-cudaError_t launch_ozaki_scan(const StridedView<double>& x, const OzakiOperand& op, int* nonfinite,
+cudaError_t launch_ozaki_scan(const StridedView<double>& x, const OzakiOperand& op, int* nonfinite, double* spread,
                               cudaStream_t stream) {
   if (x.rows == 0 || x.cols == 0) return cudaSuccess;
   dim3 grid(unsigned((x.cols + kScanTile - 1) / kScanTile), unsigned((x.rows + kScanTile - 1) / kScanTile));
   if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
   ozaki_scan_kernel<<<grid, 256, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl,
                                               reinterpret_cast<unsigned long long*>(op.maxbits), op.abssum,
-                                              nonfinite);
+                                              nonfinite, spread);
   return cudaGetLastError();
 }
 
@@ -261,20 +249,9 @@ cudaError_t launch_ozaki_split(const StridedView<double>& x, const OzakiOperand&
 cudaError_t launch_ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, const OzakiGemmArgs& args,
                               cudaStream_t stream) {
   if (args.slices < 1 || args.slices > a.smax || args.slices > b.smax) return cudaErrorInvalidValue;
-  if (a.k_pad != b.k_pad || a.k_pad % kSliceKBytes != 0 || a.rows_pad % kSliceBM != 0)
-    return cudaErrorInvalidValue;
-  if (args.tile_n == kTilePair) {
-    if (b.rows_pad % kPairBN != 0 || a.rows_pad % (2 * kSliceBM) != 0) return cudaErrorInvalidValue;
-    return launch_gemm_pair(a, b, args, stream);
-  }
-  if (args.tile_n == 256) {
-    if (b.rows_pad % 256 != 0) return cudaErrorInvalidValue;
-    return launch_gemm_tiles<256, 4>(a, b, args, stream);
-  }
-  if (args.tile_n == 128) {
-    if (b.rows_pad % 128 != 0) return cudaErrorInvalidValue;
-    return launch_gemm_tiles<128, 6>(a, b, args, stream);
-  }
+  if (a.k_pad != b.k_pad || a.k_pad % kSliceKBytes != 0) return cudaErrorInvalidValue;
+  if (args.tile_n == 128) return launch_config<128, 6, false>(a, b, args, stream);
+  if (args.tile_n == 256 || args.tile_n == kTilePair) return launch_config<128, 8, true>(a, b, args, stream);
   return cudaErrorInvalidValue;
 }
 

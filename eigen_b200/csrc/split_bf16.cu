@@ -73,21 +73,23 @@ __global__ void __launch_bounds__(256) bf16_split_kernel(const float* __restrict
   *reinterpret_cast<uint4*>(pieces + 2 * plane + off) = *reinterpret_cast<const uint4*>(lv);
 }
 
-template <int BN, int STAGES>
-cudaError_t launch_tiles(const Bf16Operand& a, const Bf16Operand& b, const SgemmSplitArgs& args, cudaStream_t stream) {
-  using L = SliceSmemLayout<BN, STAGES>;
+template <int BN, int STAGES, bool PAIR>
+cudaError_t launch_config(const Bf16Operand& a, const Bf16Operand& b, const SgemmSplitArgs& args,
+                          cudaStream_t stream) {
+  constexpr int kRowsPerTile = PAIR ? 2 * kSliceBM : kSliceBM;
+  if (a.rows_pad % kRowsPerTile != 0 || b.rows_pad % BN != 0) return cudaErrorInvalidValue;
   CUtensorMap tmA, tmB;
   if (!make_tensor_map_3d(&tmA, a.pieces, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, uint64_t(a.k_pad),
                           uint64_t(a.rows_pad), 3, kSliceKBytes / 2, kSliceBM))
     return cudaErrorInvalidValue;
   if (!make_tensor_map_3d(&tmB, b.pieces, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, uint64_t(b.k_pad),
-                          uint64_t(b.rows_pad), 3, kSliceKBytes / 2, BN))
+                          uint64_t(b.rows_pad), 3, kSliceKBytes / 2, PAIR ? BN / 2 : BN))
     return cudaErrorInvalidValue;
   SliceGemmParams P{};
   P.m = args.m;
   P.n = args.n;
   P.num_kb = int(a.k_pad / (kSliceKBytes / 2));
-  P.tiles_m = int(a.rows_pad / kSliceBM);
+  P.tiles_m = int(a.rows_pad / kRowsPerTile);
   P.tiles_n = int(b.rows_pad / BN);
   P.slices = args.pieces;
   P.diag_lo = 2;
@@ -100,44 +102,7 @@ cudaError_t launch_tiles(const Bf16Operand& a, const Bf16Operand& b, const Sgemm
   P.skip_if_flag = args.skip_if_flag;
   P.status = args.status;
   P.group_m = tuning().group_m > 0 ? tuning().group_m : P.tiles_m;
-  P.prefetch = tuning().prefetch;
-  auto kern = slice_gemm_kernel<kModeSplitBF16, BN, STAGES>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kAlloc);
-  if (e != cudaSuccess) return e;
-  const int tiles = P.tiles_m * P.tiles_n;
-  const int grid = tiles < args.num_sms ? tiles : args.num_sms;
-  kern<<<grid, 192, L::kAlloc, stream>>>(tmA, tmB, P);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_pair(const Bf16Operand& a, const Bf16Operand& b, const SgemmSplitArgs& args, cudaStream_t stream) {
-  constexpr int kStages = 6;
-  CUtensorMap tmA, tmB;
-  if (!make_tensor_map_3d(&tmA, a.pieces, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, uint64_t(a.k_pad),
-                          uint64_t(a.rows_pad), 3, kSliceKBytes / 2, kSliceBM))
-    return cudaErrorInvalidValue;
-  if (!make_tensor_map_3d(&tmB, b.pieces, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, uint64_t(b.k_pad),
-                          uint64_t(b.rows_pad), 3, kSliceKBytes / 2, kPairBN / 2))
-    return cudaErrorInvalidValue;
-  SliceGemmParams P{};
-  P.m = args.m;
-  P.n = args.n;
-  P.num_kb = int(a.k_pad / (kSliceKBytes / 2));
-  P.tiles_m = int(a.rows_pad / (2 * kSliceBM));
-  P.tiles_n = int(b.rows_pad / kPairBN);
-  P.slices = args.pieces;
-  P.diag_lo = 2;
-  P.diag_hi = args.pieces + 1;
-  P.first_writes = 1;
-  P.alpha_f = args.alpha;
-  P.beta_f = args.beta;
-  P.C = args.C;
-  P.ldc = args.ldc;
-  P.skip_if_flag = args.skip_if_flag;
-  P.status = args.status;
-  P.group_m = tuning().group_m > 0 ? tuning().group_m : P.tiles_m;
-  P.prefetch = 0;
-  return launch_slice_pair<kModeSplitBF16, kStages>(tmA, tmB, P, args.num_sms, stream);
+  return launch_slice_gemm<kModeSplitBF16, BN, STAGES, 4, PAIR>(tmA, tmB, P, args.num_sms, stream);
 }
 
 }  // namespace
@@ -156,12 +121,10 @@ cudaError_t launch_bf16_split(const StridedView<float>& x, const Bf16Operand& op
 cudaError_t launch_sgemm_split_bf16(const Bf16Operand& a, const Bf16Operand& b, const SgemmSplitArgs& args,
                                     cudaStream_t stream) {
   if (args.pieces < 1 || args.pieces > 3) return cudaErrorInvalidValue;
-  if (a.k_pad != b.k_pad || a.k_pad % (kSliceKBytes / 2) != 0 || a.rows_pad % kSliceBM != 0)
-    return cudaErrorInvalidValue;
-  if (args.tile_n == kTilePair && b.rows_pad % kPairBN == 0 && a.rows_pad % (2 * kSliceBM) == 0)
-    return launch_pair(a, b, args, stream);
-  if (args.tile_n == 256 && b.rows_pad % 256 == 0) return launch_tiles<256, 4>(a, b, args, stream);
-  if (args.tile_n == 128 && b.rows_pad % 128 == 0) return launch_tiles<128, 6>(a, b, args, stream);
+  if (a.k_pad != b.k_pad || a.k_pad % (kSliceKBytes / 2) != 0) return cudaErrorInvalidValue;
+  if (args.tile_n == kTilePair) return launch_config<256, 6, true>(a, b, args, stream);
+  if (args.tile_n == 256) return launch_config<256, 4, false>(a, b, args, stream);
+  if (args.tile_n == 128) return launch_config<128, 6, false>(a, b, args, stream);
   return cudaErrorInvalidValue;
 }
 

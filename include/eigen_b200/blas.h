@@ -112,6 +112,8 @@ typedef struct eb2_call_info {
   double kernel_ms;   /* device time of all product kernels (ms), -1 if not measured */
   double gemm_kernel_ms; /* device time of the main GEMM kernel alone (ms), -1 if not measured */
   int launches;       /* kernels this library launched for the call */
+  double spread;      /* emulated DGEMM: mean (largest - mean) binary exponent of 64-entry
+                         row chunks of op(A) and op(B)^T, the picker's data feature; else 0 */
 } eb2_call_info;
 int eb2_last_call_info(eb2_call_info* out);
 
@@ -164,6 +166,31 @@ int eb2_gemm_grouped(char dtype, int64_t count, const eb2_gemm_problem* problems
  * stream-ordered: what a caller looping over dgemm_/sgemm_ gets, without the host
  * synchronisation.  The baseline the grouped launch is measured against. */
 int eb2_gemm_each(char dtype, int64_t count, const eb2_gemm_problem* problems, void* stream);
+
+/* ---------------------------------------------------------------- learned picker
+ * A 3-layer MLP (8 features -> 64 -> 64 -> 11, ReLU, FP32) that plays the role of Eigen's
+ * computeProductBlockingSizes (Eigen/src/Core/products/GeneralBlockPanelKernel.h:202-452):
+ * from log2 m, n, k, the dtype, the inputs' exponent spread and the batch size it scores
+ * 4 kernel configurations (0 native, 1 emulated 128x128, 2 emulated 128x256, 3 emulated
+ * CTA pair 256x256) and 7 digit-slice counts (6..12) of the emulated DGEMM.  Weights are a
+ * flat float array of eb2_mlp_param_count() entries:
+ *   W1[64][8] b1[64] W2[64][64] b2[64] W3[11][64] b3[11]. */
+int eb2_mlp_param_count(void);
+/* Installs the weights the product path consults when method/tile/slices are automatic
+ * (copied; NULL or count 0 removes the picker).  The a-posteriori accuracy check still
+ * adds slices when a prediction falls short. */
+int eb2_picker_set_weights(const float* weights, int count);
+int eb2_picker_features(int64_t m, int64_t n, int64_t k, char dtype, double spread, int64_t batch, float* out8);
+int eb2_picker_forward_host(const float* weights, const float* features8, float* logits11);
+int eb2_picker_predict(int64_t m, int64_t n, int64_t k, char dtype, double spread, int64_t batch, int* config,
+                       int* slices);
+/* Training kernels (device pointers, stream-ordered): forward logits[batch][11];
+ * backward writes the batch-mean gradient (and loss) of the config cross-entropy plus
+ * the slice cross-entropy for samples whose slice label is >= 0; Adam step t >= 1. */
+int eb2_mlp_forward(const float* w, const float* X, int batch, float* logits, void* stream);
+int eb2_mlp_backward(const float* w, const float* X, const int* cfg_label, const int* slice_label, int batch,
+                     float* grads, float* loss, void* stream);
+int eb2_mlp_adam(float* w, const float* grads, float* m, float* v, int step, float lr, void* stream);
 
 /* Library version string. */
 const char* eb2_version(void);

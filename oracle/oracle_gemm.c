@@ -307,8 +307,8 @@ void oracle_ozaki_split(const double* X, long rows, long cols, long sr, long sl,
  * recombination is replayed in the device epilogue's order):
  *   digits of op(A) rows and op(B) columns as in oracle_ozaki_split;
  *   D_t = sum_{p+q=t, 1<=p,q<=s} Dp_A Dq_B^T  (exact, int64 here);
- *   for t = s+1 down to 2:  val = (double(D_t) * 2^(e_i + f_j - 12 - 7(t-2))) * alpha;
- *     first t: C = (beta == 0) ? val : fma(beta, C, val);   later t: C = C + val.
+ *   acc = 0; for t = s+1 down to 2:  acc = acc + double(D_t) * 2^(e_i + f_j - 12 - 7(t-2));
+ *   v = alpha * acc;  C = (beta == 0) ? v : fma(beta, C, v).
  * Rows/columns with a non-finite entry are left to the caller (the device falls back
  * to IEEE FP64 there).  Work arrays are allocated here; sizes are small in tests. */
 #include <stdlib.h>
@@ -337,7 +337,7 @@ int oracle_ozaki_dgemm(char transa, char transb, long m, long n, long k, double 
     for (long i = 0; i < m; ++i) {
       double* c = &C[(size_t)i + (size_t)j * (size_t)ldc];
       if (ea[i] == INT32_MIN || eb[j] == INT32_MIN) continue;
-      int first = 1;
+      double acc = 0.0;
       for (int t = s + 1; t >= 2; --t) {
         long long D = 0;
         for (int p = (t - s > 1 ? t - s : 1); p <= (s < t - 1 ? s : t - 1); ++p) {
@@ -345,13 +345,10 @@ int oracle_ozaki_dgemm(char transa, char transb, long m, long n, long k, double 
           const int8_t* rb = db + ((size_t)(t - p - 1) * (size_t)n + (size_t)j) * (size_t)k;
           for (long l = 0; l < k; ++l) D += (long long)ra[l] * (long long)rb[l];
         }
-        const double val = ((double)D * ldexp(1.0, ea[i] + eb[j] - 12 - 7 * (t - 2))) * alpha;
-        if (first)
-          *c = (beta == 0.0) ? val : fma(beta, *c, val);
-        else
-          *c = *c + val;
-        first = 0;
+        acc = acc + (double)D * ldexp(1.0, ea[i] + eb[j] - 12 - 7 * (t - 2));
       }
+      const double v = alpha * acc;
+      *c = (beta == 0.0) ? v : fma(beta, *c, v);
     }
   free(da);
   free(db);

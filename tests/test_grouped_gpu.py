@@ -49,12 +49,12 @@ def make_batch(sizes, dtype, seed, mixed=True):
         pad = 0 if not mixed else i % 4
         ar, ac = op_shape(ta, m, k)
         br, bc = op_shape(tb, k, n)
-        A = np.asfortranarray(rng.uniform(-1, 1, (ar + pad, max(ac, 1))).astype(npdt))
-        B = np.asfortranarray(rng.uniform(-1, 1, (br + pad, max(bc, 1))).astype(npdt))
-        C = np.asfortranarray(rng.uniform(-1, 1, (m + pad, max(n, 1))).astype(npdt))
+        A = np.asfortranarray(rng.uniform(-1, 1, (max(1, ar + pad), max(ac, 1))).astype(npdt))
+        B = np.asfortranarray(rng.uniform(-1, 1, (max(1, br + pad), max(bc, 1))).astype(npdt))
+        C = np.asfortranarray(rng.uniform(-1, 1, (max(1, m + pad), max(n, 1))).astype(npdt))
         alpha, beta = ((1.0, 0.0) if not mixed else [(1.0, 0.0), (1.5, 0.5), (0.0, 1.3), (-0.7, 1.0)][i % 4])
-        host.append(dict(transa=ta, transb=tb, m=m, n=n, k=k, alpha=alpha, beta=beta, A=A, lda=ar + pad, B=B,
-                         ldb=br + pad, C=C, ldc=m + pad))
+        host.append(dict(transa=ta, transb=tb, m=m, n=n, k=k, alpha=alpha, beta=beta, A=A, lda=max(1, ar + pad), B=B,
+                         ldb=max(1, br + pad), C=C, ldc=max(1, m + pad)))
     return host
 
 
