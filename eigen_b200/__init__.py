@@ -33,6 +33,7 @@ EB2_ERR_ACCURACY = -6
 METHOD_AUTO = 0
 METHOD_NATIVE = 1
 METHOD_EMULATED = 2
+METHOD_CRT = 3
 
 _lib = None
 
@@ -98,6 +99,7 @@ def load(path: str | os.PathLike | None = None, mode: int = ctypes.RTLD_GLOBAL) 
     lib.eb2_set_dgemm_method.argtypes = [ctypes.c_int]
     lib.eb2_set_sgemm_method.argtypes = [ctypes.c_int]
     lib.eb2_set_dgemm_slices.argtypes = [ctypes.c_int]
+    lib.eb2_set_dgemm_moduli.argtypes = [ctypes.c_int]
     lib.eb2_set_dgemm_tolerance.argtypes = [ctypes.c_double]
     lib.eb2_set_tile_n.argtypes = [ctypes.c_int]
     lib.eb2_set_sgemm_pieces.argtypes = [ctypes.c_int]
@@ -192,6 +194,10 @@ def set_sgemm_method(method: int) -> int:
 
 def set_dgemm_slices(slices: int) -> int:
     return load().eb2_set_dgemm_slices(slices)
+
+
+def set_dgemm_moduli(moduli: int) -> int:
+    return load().eb2_set_dgemm_moduli(moduli)
 
 
 def set_sgemm_pieces(pieces: int) -> int:

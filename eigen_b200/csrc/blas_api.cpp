@@ -218,7 +218,7 @@ void sgemm_64_(const char* transa, const char* transb, const int64_t* m, const i
 }
 
 int eb2_set_dgemm_method(int method) {
-  if (method < EB2_METHOD_AUTO || method > EB2_METHOD_EMULATED) return EB2_ERR_ARG;
+  if (method < EB2_METHOD_AUTO || method > EB2_METHOD_CRT) return EB2_ERR_ARG;
   eb2::settings().dgemm_method = method;
   return EB2_OK;
 }
@@ -226,6 +226,12 @@ int eb2_set_dgemm_method(int method) {
 int eb2_set_sgemm_method(int method) {
   if (method < EB2_METHOD_AUTO || method > EB2_METHOD_EMULATED) return EB2_ERR_ARG;
   eb2::settings().sgemm_method = method;
+  return EB2_OK;
+}
+
+int eb2_set_dgemm_moduli(int moduli) {
+  if (moduli != 0 && (moduli < 8 || moduli > eb2::kCrtMaxModuli)) return EB2_ERR_ARG;
+  eb2::settings().dgemm_moduli = moduli;
   return EB2_OK;
 }
 

@@ -51,6 +51,7 @@ struct Settings {
   std::atomic<int> dgemm_method{EB2_METHOD_AUTO};
   std::atomic<int> sgemm_method{EB2_METHOD_AUTO};
   std::atomic<int> dgemm_slices{0};
+  std::atomic<int> dgemm_moduli{0};
   std::atomic<int> sgemm_pieces{3};
   std::atomic<int> tile_n{0};
   std::atomic<double> dgemm_tol{1.1102230246251565e-16};  // 2^-53

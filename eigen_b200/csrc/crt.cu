@@ -1,0 +1,577 @@
+// crt.cu -- FP64 GEMM emulated with integer residues (Ozaki scheme II, CRT form).
+//
+// Method (Ozaki, Uchino & Imamura, "Ozaki Scheme II: A GEMM-oriented emulation of
+// floating-point matrix multiplication using an integer modular technique", 2025), here
+// with exact multi-word integer reconstruction:
+//   * every row i of op(A) is scaled by 2^mu_i and truncated to integers A', every row j
+//     of op(B)^T by 2^nu_j to B', with mu_i, nu_j chosen from upper bounds of the rows'
+//     2-norms so that ||A'_i||_2, ||B'_j||_2 <= 2^b; then |C'_ij| = |A'_i . B'_j| <= 2^(2b)
+//     (Cauchy-Schwarz) and b is the largest integer with 2^(2b+1) < P = p_1 ... p_N, the
+//     product of N pairwise coprime moduli <= 256;
+//   * for each modulus the residues A' mod p, B' mod p (symmetric int8) are multiplied
+//     exactly on the INT8 tensor cores (INT32 accumulation) and reduced mod p: N GEMMs
+//     instead of the s(s+1)/2 of the digit-slice scheme (slice_gemm.cuh, CRT mode);
+//   * C' is recovered from its N residues by the Chinese remainder theorem,
+//     C' = sum_l r_l W_l mod P, W_l = (P/p_l) * ((P/p_l)^-1 mod p_l), in exact 192-bit
+//     integer arithmetic, taken in (-P/2, P/2) (|C'| < P/2, so it is C' itself), rounded
+//     once to FP64 and scaled: C = alpha * (C' 2^-(mu_i + nu_j)) (+ beta * C).
+// The only approximation is the truncation A'_il = trunc(2^mu_i a_il) (error < 1 unit):
+// with 16 moduli b = 62, i.e. 62 bits per row relative to the row's 2-norm.
+//
+// Every step is deterministic (integer norm bounds, exact products), so results are
+// reproducible bit for bit and can be checked against an exact CPU model.
+#include <cuda.h>
+
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "device_common.cuh"
+#include "kernels.h"
+#include "slice_gemm.cuh"
+#include "tma_host.h"
+
+namespace eb2 {
+
+// ------------------------------------------------------------------ host constants
+namespace {
+
+constexpr int kLimbs = kCrtLimbs;  // 192-bit integers, base 2^32
+
+struct Big {
+  uint32_t w[kLimbs] = {0, 0, 0, 0, 0, 0};
+};
+
+void big_mul_small(Big& a, uint32_t s) {
+  uint64_t carry = 0;
+  for (int i = 0; i < kLimbs; ++i) {
+    const uint64_t v = uint64_t(a.w[i]) * s + carry;
+    a.w[i] = uint32_t(v);
+    carry = v >> 32;
+  }
+}
+
+uint32_t big_div_small(Big& a, uint32_t s) {  // a /= s, returns a mod s
+  uint64_t rem = 0;
+  for (int i = kLimbs - 1; i >= 0; --i) {
+    const uint64_t cur = (rem << 32) | a.w[i];
+    a.w[i] = uint32_t(cur / s);
+    rem = cur % s;
+  }
+  return uint32_t(rem);
+}
+
+int big_bits(const Big& a) {  // bit length
+  for (int i = kLimbs - 1; i >= 0; --i)
+    if (a.w[i]) return 32 * i + 32 - __builtin_clz(a.w[i]);
+  return 0;
+}
+
+bool big_is_pow2(const Big& a) {
+  int ones = 0;
+  for (int i = 0; i < kLimbs; ++i) ones += __builtin_popcount(a.w[i]);
+  return ones == 1;
+}
+
+double big_to_double(const Big& a) {
+  double d = 0.0;
+  for (int i = kLimbs - 1; i >= 0; --i) d = d * 4294967296.0 + double(a.w[i]);
+  return d;
+}
+
+uint32_t inverse_mod(uint32_t a, uint32_t p) {  // a^-1 mod p (gcd(a, p) == 1)
+  int64_t t = 0, nt = 1, r = p, nr = a % p;
+  while (nr) {
+    const int64_t q = r / nr;
+    int64_t tmp = t - q * nt;
+    t = nt;
+    nt = tmp;
+    tmp = r - q * nr;
+    r = nr;
+    nr = tmp;
+  }
+  return uint32_t(t < 0 ? t + p : t);
+}
+
+}  // namespace
+
+int crt_bits(int n) {
+  Big P;
+  P.w[0] = 1;
+  for (int l = 0; l < n; ++l) big_mul_small(P, uint32_t(crt_modulus(l)));
+  // largest b with 2^(2b+1) < P: 2b+1 <= bits(P) - 1, minus one more when P = 2^(bits-1)
+  const int L = big_bits(P);
+  int b = (L - 2) / 2;
+  if (big_is_pow2(P) && 2 * b + 1 == L - 1) --b;
+  return b;
+}
+
+const CrtConstants& crt_constants(int n) {
+  static CrtConstants table[kCrtMaxModuli + 1];
+  static bool ready[kCrtMaxModuli + 1] = {};
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  CrtConstants& c = table[n];
+  if (ready[n]) return c;
+  std::memset(&c, 0, sizeof(c));
+  c.n = n;
+  Big P;
+  P.w[0] = 1;
+  for (int l = 0; l < n; ++l) big_mul_small(P, uint32_t(crt_modulus(l)));
+  for (int l = 0; l < n; ++l) {
+    const uint32_t p = uint32_t(crt_modulus(l));
+    Big M = P;
+    (void)big_div_small(M, p);  // M = P / p_l
+    Big Mm = M;
+    const uint32_t m_mod = big_div_small(Mm, p);
+    Big W = M;
+    big_mul_small(W, inverse_mod(m_mod, p));  // (P/p) * inv < P
+    for (int i = 0; i < kLimbs; ++i) c.W[l][i] = W.w[i];
+  }
+  for (int i = 0; i < kLimbs; ++i) c.P[i] = P.w[i];
+  Big half = P;
+  (void)big_div_small(half, 2);
+  for (int i = 0; i < kLimbs; ++i) c.half[i] = half.w[i];
+  c.P_inv = 1.0 / big_to_double(P);
+  c.b = crt_bits(n);
+  ready[n] = true;
+  return c;
+}
+
+// ------------------------------------------------------------------ kernels
+namespace {
+
+constexpr uint64_t kInfBitsCrt = 0x7FF0000000000000ull;
+constexpr int kNormRows = 32;
+constexpr int kNormCols = 128;
+
+// exponent e of a finite nonzero |x| given by its bit pattern: |x| in [2^(e-1), 2^e)
+__device__ __forceinline__ int frexp_exp(unsigned long long mb) {
+  int e;
+  frexp(__longlong_as_double(static_cast<long long>(mb)), &e);
+  return e;
+}
+
+// x * 2^e for |e| <= 2200 as two exact power-of-two products (one rounding at most, in
+// the second product, when the result is subnormal)
+__device__ __forceinline__ double scale2(double x, int e) {
+  const int e1 = e / 2;
+  return __dmul_rn(__dmul_rn(x, exp2_int(e1)), exp2_int(e - e1));
+}
+
+// Deterministic upper bound of sum_l (x_l 2^-e)^2 in units of 2^-32, e the exponent of
+// the row maximum: every nonzero x adds ceil(rn(x'^2) 2^32) + 1, x' = x 2^-e (|x'| < 1);
+// the +1 covers the rounding of x'^2 (and a product that underflows).
+__global__ void __launch_bounds__(256) crt_norm_kernel(const double* __restrict__ X, int64_t rows, int64_t cols,
+                                                       int64_t sr, int64_t sl,
+                                                       const unsigned long long* __restrict__ maxbits,
+                                                       unsigned long long* __restrict__ sumsq) {
+  __shared__ double tile[kNormRows][kNormCols + 1];
+  const int64_t r0 = int64_t(blockIdx.y) * kNormRows;
+  const int64_t l0 = int64_t(blockIdx.x) * kNormCols;
+  const bool rows_contig = (sr == 1);
+  for (int idx = threadIdx.x; idx < kNormRows * kNormCols; idx += blockDim.x) {
+    int rr, ll;
+    if (rows_contig) {
+      rr = idx % kNormRows;
+      ll = idx / kNormRows;
+    } else {
+      ll = idx % kNormCols;
+      rr = idx / kNormCols;
+    }
+    const int64_t r = r0 + rr, l = l0 + ll;
+    tile[rr][ll] = (r < rows && l < cols) ? X[r * sr + l * sl] : 0.0;
+  }
+  __syncthreads();
+  // 8 threads per row, 16 columns each; the 8 partial sums meet in a shuffle reduction
+  const int rr = threadIdx.x >> 3;
+  const int cb = (threadIdx.x & 7) * 16;
+  const int64_t r = r0 + rr;
+  unsigned long long s = 0;
+  const unsigned long long mb = r < rows ? maxbits[r] : 0ull;
+  if (mb != 0 && mb < kInfBitsCrt) {
+    const int e = frexp_exp(mb);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const double x = tile[rr][cb + j];
+      if (x != 0.0) {
+        const double xs = scale2(x, -e);
+        s += static_cast<unsigned long long>(ceil(__dmul_rn(__dmul_rn(xs, xs), 4294967296.0))) + 1ull;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 7) == 0 && s != 0) atomicAdd(&sumsq[r], s);
+}
+
+// Scale exponent of one row: mu = b - c with 2^c >= ||x|| from the bound above:
+// ||x||^2 <= S 2^(2e-32), S <= 2^L (L = bit length of S-1), so c = e - 16 + ceil(L/2).
+__device__ __forceinline__ int row_mu(unsigned long long mb, unsigned long long S, int b) {
+  if (mb == 0 || mb >= kInfBitsCrt || S == 0) return kCrtZeroRow;
+  const int e = frexp_exp(mb);
+  const int L = S > 1 ? 64 - __clzll(static_cast<long long>(S - 1)) : 0;
+  return b - (e - 16 + (L + 1) / 2);
+}
+
+// Per-modulus constants: p, floor((2^32 - 1) / p) for mod_small, and 2^21, 2^42, 2^63 mod p.
+struct CrtModConst {
+  uint32_t p, magic, c21, c42, c63;
+};
+__host__ __device__ constexpr uint32_t pow2_mod_const(int s, uint32_t p) {
+  uint32_t v = 1u % p;
+  for (int i = 0; i < s; ++i) v = (2u * v) % p;
+  return v;
+}
+__host__ __device__ constexpr CrtModConst crt_mod_const(int l) {
+  return CrtModConst{uint32_t(crt_modulus(l)), 0xFFFFFFFFu / uint32_t(crt_modulus(l)),
+                     pow2_mod_const(21, uint32_t(crt_modulus(l))), pow2_mod_const(42, uint32_t(crt_modulus(l))),
+                     pow2_mod_const(63, uint32_t(crt_modulus(l)))};
+}
+static_assert(kCrtMaxModuli == 20, "constant table below");
+__constant__ CrtModConst kModConst[kCrtMaxModuli] = {
+    crt_mod_const(0),  crt_mod_const(1),  crt_mod_const(2),  crt_mod_const(3),  crt_mod_const(4),
+    crt_mod_const(5),  crt_mod_const(6),  crt_mod_const(7),  crt_mod_const(8),  crt_mod_const(9),
+    crt_mod_const(10), crt_mod_const(11), crt_mod_const(12), crt_mod_const(13), crt_mod_const(14),
+    crt_mod_const(15), crt_mod_const(16), crt_mod_const(17), crt_mod_const(18), crt_mod_const(19)};
+
+// |t| < 2^84 (integer-valued) as four 21-bit chunks, |t| = a3 2^63 + a2 2^42 + a1 2^21 + a0;
+// every step is exact in FP64 (power-of-two scalings, floors, and differences that are
+// multiples of the ulp of |t| below the removed power).
+struct Chunks21 {
+  uint32_t a0, a1, a2, a3;
+};
+__device__ __forceinline__ Chunks21 chunks21(double at) {
+  const double h3 = floor(at * 0x1p-63);
+  double r = fma(-h3, 0x1p63, at);
+  const double h2 = floor(r * 0x1p-42);
+  r = fma(-h2, 0x1p42, r);
+  const double h1 = floor(r * 0x1p-21);
+  const double h0 = fma(-h1, 0x1p21, r);
+  return Chunks21{__double2uint_rz(h0), __double2uint_rz(h1), __double2uint_rz(h2), __double2uint_rz(h3)};
+}
+
+// |t| mod p: the chunk sum a0 + a1 c21 + a2 c42 + a3 c63 < 2^21 (1 + 3 * 255) < 2^31
+__device__ __forceinline__ uint32_t residue_of(const Chunks21& c, const CrtModConst& k) {
+  return mod_small(c.a0 + c.a1 * k.c21 + c.a2 * k.c42 + c.a3 * k.c63, k.p, k.magic);
+}
+
+constexpr int kSplitRowsCrt = 32;
+constexpr int kSplitColsCrt = 128;
+
+// Residues of A' = trunc(2^mu_r x) for moduli [0, n): plane l at residues + l*rows_pad*k_pad,
+// row r contiguous along k; symmetric int8 representatives.  Blocks of column 0 write mu_r.
+__global__ void __launch_bounds__(256) crt_split_kernel(const double* __restrict__ X, int64_t rows, int64_t cols,
+                                                        int64_t sr, int64_t sl,
+                                                        const unsigned long long* __restrict__ maxbits,
+                                                        const unsigned long long* __restrict__ sumsq, int b, int n,
+                                                        int8_t* __restrict__ residues, int32_t* __restrict__ mu,
+                                                        int64_t rows_pad, int64_t k_pad) {
+  __shared__ double tile[kSplitRowsCrt][kSplitColsCrt + 1];
+  __shared__ int row_mu_s[kSplitRowsCrt];
+  const int64_t r0 = int64_t(blockIdx.y) * kSplitRowsCrt;
+  const int64_t l0 = int64_t(blockIdx.x) * kSplitColsCrt;
+  const bool rows_contig = (sr == 1);
+  if (threadIdx.x < kSplitRowsCrt) {
+    const int64_t r = r0 + threadIdx.x;
+    const int m = (r < rows) ? row_mu(maxbits[r], sumsq[r], b) : kCrtZeroRow;
+    row_mu_s[threadIdx.x] = m;
+    if (blockIdx.x == 0) mu[r] = m;
+  }
+  for (int idx = threadIdx.x; idx < kSplitRowsCrt * kSplitColsCrt; idx += blockDim.x) {
+    int rr, ll;
+    if (rows_contig) {
+      rr = idx % kSplitRowsCrt;
+      ll = idx / kSplitRowsCrt;
+    } else {
+      ll = idx % kSplitColsCrt;
+      rr = idx / kSplitColsCrt;
+    }
+    const int64_t r = r0 + rr, l = l0 + ll;
+    tile[rr][ll] = (r < rows && l < cols) ? X[r * sr + l * sl] : 0.0;
+  }
+  __syncthreads();
+  const int rr = threadIdx.x >> 3;
+  const int cb = (threadIdx.x & 7) * 16;
+  const int m = row_mu_s[rr];
+  double at[16];
+  uint32_t neg = 0;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    // |v| <= 2^b, an exact integer (0 in zero rows: 2^kCrtZeroRow underflows to 0)
+    const double v = trunc(scale2(tile[rr][cb + j], m));
+    at[j] = fabs(v);
+    neg |= (v < 0.0 ? 1u : 0u) << j;
+  }
+  const int64_t row = r0 + rr;
+  Chunks21 ch[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) ch[j] = chunks21(at[j]);
+  for (int l = 0; l < n; ++l) {
+    const CrtModConst k = kModConst[l];
+    const int hi = int(k.p >> 1) - ((k.p & 1u) ? 0 : 1);  // largest representative kept as is
+    uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      uint32_t res = residue_of(ch[j], k);
+      if (((neg >> j) & 1u) && res) res = k.p - res;  // residue of the negative value
+      const int sres = int(res) > hi ? int(res) - int(k.p) : int(res);  // [-(p/2), (p-1)/2]
+      w[j >> 2] |= (uint32_t(sres) & 0xFFu) << (8 * (j & 3));
+    }
+    uint4* dst = reinterpret_cast<uint4*>(residues + (size_t(l) * size_t(rows_pad) + size_t(row)) * size_t(k_pad) +
+                                          size_t(l0 + cb));
+    *dst = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+struct CrtRecParams {
+  uint32_t W[kCrtMaxModuli][kCrtLimbs];
+  uint32_t P[kCrtLimbs];
+  uint32_t half[kCrtLimbs];
+  double P_inv;
+  int n, b;
+  int64_t m, ncols;
+  double alpha, beta;
+  double* C;
+  int64_t ldc;
+  const uint8_t* res;
+  int64_t ld_res, plane;
+  const int32_t* mu_a;
+  const int32_t* mu_b;
+  double* err_sq;  // [0] += estimated squared error, [1] += squared alpha*A*B entries
+  const int* skip_if_flag;
+  int write_c;
+};
+
+// RN(|R|) of a 192-bit magnitude as d * 2^shift, d an integer-valued double < 2^64:
+// the top 64 bits below the leading one, with a sticky bit for everything under them.
+__device__ __forceinline__ double limbs_to_double(const uint32_t* s, int& shift) {
+  int h = kCrtLimbs - 1;
+  while (h > 0 && s[h] == 0) --h;
+  shift = 0;
+  if (h <= 1) return __ull2double_rn((static_cast<unsigned long long>(h == 1 ? s[1] : 0u) << 32) | s[0]);
+  const int lz = __clz(static_cast<int>(s[h]));
+  unsigned long long u = (static_cast<unsigned long long>(s[h]) << 32) | s[h - 1];
+  uint32_t sticky;
+  if (lz) {
+    u = (u << lz) | (s[h - 2] >> (32 - lz));
+    sticky = s[h - 2] << lz;
+  } else {
+    sticky = s[h - 2];
+  }
+  for (int i = 0; i < h - 2; ++i) sticky |= s[i];
+  shift = 32 * (h - 1) - lz;
+  return __ull2double_rn(u | (sticky ? 1ull : 0ull));
+}
+
+// RN(d 2^e) for an integer-valued d in [1, 2^64): two exact steps, one rounding at most
+__device__ __forceinline__ double scale_exp(double d, int e) {
+  if (e < -1200) return d * 0.0;  // |d 2^e| < 2^-1136
+  if (e > 1100) e = 1100;         // overflows to infinity either way
+  return scale2(d, e);
+}
+
+// One thread per element (i, j): C'_ij from its residues, then C_ij.
+__global__ void __launch_bounds__(256) crt_reconstruct_kernel(const __grid_constant__ CrtRecParams R) {
+  if (R.skip_if_flag && *R.skip_if_flag) return;
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  double e_acc = 0.0, v_acc = 0.0;
+  const double e_scale = 0.816496580927726;  // sqrt(2/3): rms of the truncation error
+  for (int64_t j = blockIdx.y; j < R.ncols; j += gridDim.y) {
+    if (i >= R.m) break;
+    const uint8_t* rp = R.res + j * R.ld_res + i;
+    unsigned long long acc[kCrtLimbs] = {0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
+    // unrolled over the largest modulus count: the weights are immediate constant-bank operands
+#pragma unroll
+    for (int l = 0; l < kCrtMaxModuli; ++l) {
+      if (l < R.n) {
+        const uint32_t r = rp[int64_t(l) * R.plane];
+#pragma unroll
+        for (int q = 0; q < kCrtLimbs; ++q) acc[q] += static_cast<unsigned long long>(r) * R.W[l][q];
+      }
+    }
+    // S = sum r_l W_l < n * 256 * P < 2^192 as six 32-bit limbs
+    uint32_t s[kCrtLimbs];
+    unsigned long long carry = 0;
+#pragma unroll
+    for (int q = 0; q < kCrtLimbs; ++q) {
+      const unsigned long long v = acc[q] + carry;
+      s[q] = uint32_t(v);
+      carry = v >> 32;
+    }
+    // R = S - q P with q = rint(S / P); then R is C' or C' +- P
+    double sd = 0.0;
+#pragma unroll
+    for (int q = kCrtLimbs - 1; q >= 0; --q) sd = fma(sd, 4294967296.0, double(s[q]));
+    const uint32_t qq = uint32_t(rint(sd * R.P_inv));
+    long long borrow = 0;
+    unsigned long long mcarry = 0;
+#pragma unroll
+    for (int q = 0; q < kCrtLimbs; ++q) {
+      const unsigned long long qp = static_cast<unsigned long long>(qq) * R.P[q] + mcarry;
+      mcarry = qp >> 32;
+      const long long d = static_cast<long long>(s[q]) - static_cast<long long>(uint32_t(qp)) + borrow;
+      s[q] = uint32_t(d);
+      borrow = d >> 32;  // 0 or -1
+    }
+    bool negative = (s[kCrtLimbs - 1] >> 31) != 0;
+    if (negative) {  // two's complement negate
+      unsigned long long c = 1;
+#pragma unroll
+      for (int q = 0; q < kCrtLimbs; ++q) {
+        const unsigned long long v = static_cast<unsigned long long>(~s[q]) + c;
+        s[q] = uint32_t(v);
+        c = v >> 32;
+      }
+    }
+    // |R| > P/2: the representative is P - |R| with the opposite sign
+    bool above = false;
+#pragma unroll
+    for (int q = kCrtLimbs - 1; q >= 0; --q) {
+      if (s[q] != R.half[q]) {
+        above = s[q] > R.half[q];
+        break;
+      }
+    }
+    if (above) {
+      long long bw = 0;
+#pragma unroll
+      for (int q = 0; q < kCrtLimbs; ++q) {
+        const long long d = static_cast<long long>(R.P[q]) - static_cast<long long>(s[q]) + bw;
+        s[q] = uint32_t(d);
+        bw = d >> 32;
+      }
+      negative = !negative;
+    }
+    int shift;
+    double d = limbs_to_double(s, shift);
+    if (negative) d = -d;
+    const int mu_i = R.mu_a[i], nu_j = R.mu_b[j];
+    const double val = d != 0.0 ? scale_exp(d, shift - mu_i - nu_j) : 0.0;  // d = 0 in zero rows
+    const double v = __dmul_rn(R.alpha, val);
+    if (R.write_c) {
+      double* c = R.C + j * R.ldc + i;
+      *c = R.beta == 0.0 ? v : __fma_rn(R.beta, *c, v);
+    }
+    if (R.err_sq) {
+      // truncation errors need a nonzero row on both sides
+      if (mu_i != kCrtZeroRow && nu_j != kCrtZeroRow) {
+        const double eij = ldexp(e_scale * fabs(R.alpha), R.b - mu_i - nu_j);
+        e_acc += eij * eij;
+      }
+      v_acc += v * v;
+    }
+  }
+  if (R.err_sq) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      e_acc += __shfl_xor_sync(0xffffffffu, e_acc, o);
+      v_acc += __shfl_xor_sync(0xffffffffu, v_acc, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      if (e_acc != 0.0) atomicAdd(&R.err_sq[0], e_acc);
+      if (v_acc != 0.0) atomicAdd(&R.err_sq[1], v_acc);
+    }
+  }
+}
+
+template <int BN, int STAGES, bool PAIR>
+cudaError_t launch_gemm_config(const CrtOperand& a, const CrtOperand& b, const CrtGemmArgs& args,
+                               cudaStream_t stream) {
+  constexpr int kRowsPerTile = PAIR ? 2 * kSliceBM : kSliceBM;
+  if (a.rows_pad % kRowsPerTile != 0 || b.rows_pad % BN != 0 || args.ld_res != a.rows_pad)
+    return cudaErrorInvalidValue;
+  CUtensorMap tmA, tmB;
+  if (!make_tensor_map_3d(&tmA, a.residues, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, uint64_t(a.k_pad), uint64_t(a.rows_pad),
+                          uint64_t(a.nmax), kSliceKBytes, kSliceBM))
+    return cudaErrorInvalidValue;
+  if (!make_tensor_map_3d(&tmB, b.residues, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, uint64_t(b.k_pad), uint64_t(b.rows_pad),
+                          uint64_t(b.nmax), kSliceKBytes, PAIR ? BN / 2 : BN))
+    return cudaErrorInvalidValue;
+  SliceGemmParams P{};
+  P.m = args.m;
+  P.n = args.n;
+  P.num_kb = int(a.k_pad / kSliceKBytes);
+  P.tiles_m = int(a.rows_pad / kRowsPerTile);
+  P.tiles_n = int(b.rows_pad / BN);
+  P.slices = args.moduli;
+  P.diag_lo = 0;
+  P.diag_hi = args.moduli - 1;
+  P.skip_if_flag = args.skip_if_flag;
+  P.status = args.status;
+  P.group_m = tuning().group_m > 0 ? tuning().group_m : P.tiles_m;
+  P.crt = 1;
+  P.residues = args.cres;
+  P.ld_res = args.ld_res;
+  return launch_slice_gemm<kModeCrtI8, BN, STAGES, 4, PAIR>(tmA, tmB, P, args.num_sms, stream);
+}
+
+}  // namespace
+
+int64_t crt_tile_rows(int tile_n) { return tile_n == kTilePair ? 256 : 128; }
+int64_t crt_tile_cols(int tile_n) { return tile_n == 128 ? 128 : 256; }
+
+cudaError_t launch_crt_norms(const StridedView<double>& x, const CrtOperand& op, cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(op.sumsq, 0, size_t(op.rows) * sizeof(uint64_t), stream);
+  if (e != cudaSuccess || x.rows == 0 || x.cols == 0) return e;
+  dim3 grid(unsigned((x.cols + kNormCols - 1) / kNormCols), unsigned((x.rows + kNormRows - 1) / kNormRows));
+  if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
+  crt_norm_kernel<<<grid, 256, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl,
+                                            reinterpret_cast<const unsigned long long*>(op.maxbits),
+                                            reinterpret_cast<unsigned long long*>(op.sumsq));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_crt_split(const StridedView<double>& x, const CrtOperand& op, int moduli, cudaStream_t stream) {
+  if (moduli < 1 || moduli > op.nmax) return cudaErrorInvalidValue;
+  if (op.k_pad % kSplitColsCrt != 0 || op.rows_pad % kSplitRowsCrt != 0) return cudaErrorInvalidValue;
+  dim3 grid(unsigned(op.k_pad / kSplitColsCrt), unsigned(op.rows_pad / kSplitRowsCrt));
+  if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
+  crt_split_kernel<<<grid, 256, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl,
+                                             reinterpret_cast<const unsigned long long*>(op.maxbits),
+                                             reinterpret_cast<const unsigned long long*>(op.sumsq),
+                                             crt_bits(moduli), moduli, op.residues, op.mu, op.rows_pad, op.k_pad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_crt_gemm(const CrtOperand& a, const CrtOperand& b, const CrtGemmArgs& args, cudaStream_t stream) {
+  if (args.moduli < 1 || args.moduli > a.nmax || args.moduli > b.nmax) return cudaErrorInvalidValue;
+  if (a.k_pad != b.k_pad || a.k_pad % kSliceKBytes != 0) return cudaErrorInvalidValue;
+  if (args.tile_n == kTilePair) return launch_gemm_config<256, 6, true>(a, b, args, stream);
+  if (args.tile_n == 256) return launch_gemm_config<256, 4, false>(a, b, args, stream);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t stream) {
+  if (args.moduli < 1 || args.moduli > kCrtMaxModuli) return cudaErrorInvalidValue;
+  if (args.m == 0 || args.n == 0) return cudaSuccess;
+  const CrtConstants& k = crt_constants(args.moduli);
+  CrtRecParams R;
+  std::memcpy(R.W, k.W, sizeof(R.W));
+  std::memcpy(R.P, k.P, sizeof(R.P));
+  std::memcpy(R.half, k.half, sizeof(R.half));
+  R.P_inv = k.P_inv;
+  R.n = args.moduli;
+  R.b = k.b;
+  R.m = args.m;
+  R.ncols = args.n;
+  R.alpha = args.alpha;
+  R.beta = args.beta;
+  R.C = args.C;
+  R.ldc = args.ldc;
+  R.res = args.cres;
+  R.ld_res = args.ld_res;
+  R.plane = args.plane;
+  R.mu_a = args.mu_a;
+  R.mu_b = args.mu_b;
+  R.err_sq = args.err_sq;
+  R.skip_if_flag = args.skip_if_flag;
+  R.write_c = args.write_c ? 1 : 0;
+  const unsigned gx = unsigned((args.m + 255) / 256);
+  const unsigned gy = unsigned(args.n < 65535 ? args.n : 65535);
+  crt_reconstruct_kernel<<<dim3(gx, gy), 256, 0, stream>>>(R);
+  return cudaGetLastError();
+}
+
+}  // namespace eb2

@@ -69,6 +69,182 @@ int choose_slices(int64_t m, int64_t n, int64_t k) {
   return 8;
 }
 
+int choose_crt_tile(const Context& cx, int64_t m, int64_t n) {
+  const int forced = settings().tile_n.load();
+  if (forced == kTilePair) return kTilePair;
+  if (forced == 128 || forced == 256) return 256;
+  // CTA pairs (256 x 256) unless that leaves most SMs idle
+  const int64_t pair_tiles = ((m + 255) / 256) * ((n + 255) / 256);
+  return 2 * pair_tiles >= cx.num_sms ? kTilePair : 256;
+}
+
+namespace {
+
+// CRT-form emulation (Ozaki scheme II): scan, norm bounds, residue split, one INT8 GEMM
+// per modulus, exact reconstruction.  The a-posteriori check adds two moduli at a time;
+// with beta != 0 the estimate is taken before C is written, so C is read only once.
+int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
+              int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc, cudaStream_t st,
+              const DgemmOptions& opt, eb2_call_info& info) {
+  info.method = EB2_METHOD_CRT;
+  const bool check = opt.check_accuracy;
+  const int forced = opt.moduli ? opt.moduli : settings().dgemm_moduli.load();
+  int nmod = forced ? forced : kCrtDefaultModuli;
+  const int nmax = check ? std::max(nmod, kCrtMaxModuli) : nmod;
+  const int tile = (opt.tile_n == kTilePair || opt.tile_n == 256) ? opt.tile_n : choose_crt_tile(cx, m, n);
+  const int64_t m_pad = round_up(m, crt_tile_rows(tile)), n_pad = round_up(n, crt_tile_cols(tile)),
+                k_pad = round_up(k, kOzakiKBlock);
+  size_t off = 0;
+  const size_t o_mb_a = off;
+  off = align256(off + size_t(m) * 8);
+  const size_t o_mb_b = off;
+  off = align256(off + size_t(n) * 8);
+  const size_t o_ss_a = off;
+  off = align256(off + size_t(m) * 8);
+  const size_t o_ss_b = off;
+  off = align256(off + size_t(n) * 8);
+  const size_t o_mu_a = off;
+  off = align256(off + size_t(m_pad) * 4);
+  const size_t o_mu_b = off;
+  off = align256(off + size_t(n_pad) * 4);
+  const size_t o_res_a = off;
+  off = align256(off + size_t(nmax) * m_pad * k_pad);
+  const size_t o_res_b = off;
+  off = align256(off + size_t(nmax) * n_pad * k_pad);
+  const size_t o_res_c = off;
+  off = align256(off + size_t(nmax) * m_pad * n_pad);
+  if (!cx.ws.ensure(off)) {
+    set_error(EB2_ERR_ALLOC, "could not allocate %zu bytes of emulation workspace", off);
+    return EB2_ERR_ALLOC;
+  }
+  uint8_t* ws = static_cast<uint8_t*>(cx.ws.ptr);
+  const StridedView<double> va = view_a(ta, A, lda, m, k);
+  const StridedView<double> vb = view_bt(tb, B, ldb, n, k);
+  DeviceFlags* df = cx.dflags;
+  CrtOperand oa{reinterpret_cast<int8_t*>(ws + o_res_a), reinterpret_cast<int32_t*>(ws + o_mu_a),
+                reinterpret_cast<uint64_t*>(ws + o_mb_a), reinterpret_cast<uint64_t*>(ws + o_ss_a),
+                m, m_pad, k, k_pad, nmax};
+  CrtOperand ob{reinterpret_cast<int8_t*>(ws + o_res_b), reinterpret_cast<int32_t*>(ws + o_mu_b),
+                reinterpret_cast<uint64_t*>(ws + o_mb_b), reinterpret_cast<uint64_t*>(ws + o_ss_b),
+                n, n_pad, k, k_pad, nmax};
+  // the row-maximum scan is shared with the digit-slice scheme
+  const OzakiOperand sa{nullptr, nullptr, oa.maxbits, nullptr, m, m_pad, k, k_pad, 0};
+  const OzakiOperand sb{nullptr, nullptr, ob.maxbits, nullptr, n, n_pad, k, k_pad, 0};
+
+  bool ok = check_cuda(cudaMemsetAsync(df, 0, sizeof(DeviceFlags), st), "reset flags");
+  ok = ok && check_cuda(launch_ozaki_scan_reset(sa, st), "scan reset A");
+  ok = ok && check_cuda(launch_ozaki_scan_reset(sb, st), "scan reset B");
+  ok = ok && check_cuda(launch_ozaki_scan(va, sa, &df->nonfinite, &df->spread[0], st), "scan A");
+  ok = ok && check_cuda(launch_ozaki_scan(vb, sb, &df->nonfinite, &df->spread[0], st), "scan B");
+  ok = ok && check_cuda(launch_crt_norms(va, oa, st), "norms A");
+  ok = ok && check_cuda(launch_crt_norms(vb, ob, st), "norms B");
+  if (!ok) return EB2_ERR_CUDA;
+  info.launches = 4;
+
+  CrtGemmArgs g{};
+  g.m = m;
+  g.n = n;
+  g.skip_if_flag = &df->nonfinite;
+  g.status = &df->status;
+  g.tile_n = tile;
+  g.num_sms = cx.num_sms;
+  g.cres = ws + o_res_c;
+  g.ld_res = m_pad;
+  CrtReconstructArgs r{};
+  r.m = m;
+  r.n = n;
+  r.alpha = alpha;
+  r.beta = beta;
+  r.C = C;
+  r.ldc = ldc;
+  r.cres = ws + o_res_c;
+  r.ld_res = m_pad;
+  r.plane = m_pad * n_pad;
+  r.mu_a = oa.mu;
+  r.mu_b = ob.mu;
+  r.err_sq = df->err_sq;
+  r.skip_if_flag = &df->nonfinite;
+  // with beta != 0 and the check on, C is written only once the estimate has passed
+  const bool deferred = check && beta != 0.0;
+  auto product = [&](bool first) -> bool {
+    bool good = check_cuda(launch_crt_split(va, oa, nmod, st), "residues A");
+    good = good && check_cuda(launch_crt_split(vb, ob, nmod, st), "residues B");
+    g.moduli = r.moduli = nmod;
+    if (first && opt.timed) cudaEventRecord(cx.ev_gemm0, st);
+    good = good && check_cuda(launch_crt_gemm(oa, ob, g, st), "CRT GEMM");
+    if (first && opt.timed) cudaEventRecord(cx.ev_gemm1, st);
+    r.write_c = !deferred;
+    good = good && check_cuda(launch_crt_reconstruct(r, st), "CRT reconstruction");
+    info.launches += 4;
+    return good;
+  };
+  ok = product(true);
+  // IEEE semantics for NaN/Inf inputs: the FP64 kernel runs only when the scan saw one.
+  ok = ok && check_cuda(launch_dgemm_native(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, &df->nonfinite,
+                                            st),
+                        "non-finite fallback");
+  if (!ok) return EB2_ERR_CUDA;
+  info.launches += 1;
+  info.slices = nmod;
+  info.tile_n = tile;
+  auto finish_timing = [&](bool gemm_timed) {
+    if (opt.timed) {
+      cudaEventRecord(cx.ev_stop, st);
+      set_pending_timing(&cx, gemm_timed);
+    }
+  };
+  if (!opt.sync && !check) {
+    finish_timing(true);
+    return EB2_OK;
+  }
+
+  // ---------------------------------------------------------- a-posteriori check
+  const double tol = opt.tol > 0 ? opt.tol : settings().dgemm_tol.load();
+  for (;;) {
+    if (!check_cuda(cudaMemcpyAsync(cx.hflags, df, sizeof(DeviceFlags), cudaMemcpyDeviceToHost, st), "read flags") ||
+        !check_cuda(cudaStreamSynchronize(st), "DGEMM"))
+      return EB2_ERR_CUDA;
+    const DeviceFlags hf = *cx.hflags;
+    info.spread = hf.spread[1] > 0 ? hf.spread[0] / hf.spread[1] : 0.0;
+    if (hf.status != 0) {
+      set_error(EB2_ERR_TIMEOUT, "a kernel wait timed out (device status 0x%x); C is invalid", hf.status);
+      return EB2_ERR_TIMEOUT;
+    }
+    if (hf.nonfinite) {
+      info.nonfinite = 1;
+      break;
+    }
+    // energies that overflowed (products near the FP64 range) leave the estimate unknown
+    const bool known = std::isfinite(hf.err_sq[0]) && std::isfinite(hf.err_sq[1]);
+    const double est = !known ? -1.0
+                       : hf.err_sq[1] > 0.0 ? std::sqrt(hf.err_sq[0] / hf.err_sq[1])
+                                            : (hf.err_sq[0] > 0.0 ? HUGE_VAL : 0.0);
+    info.err_estimate = est;
+    if (!check || !known || est <= tol || nmod + 2 > nmax) {
+      if (check && est > tol)
+        set_error(EB2_ERR_ACCURACY, "emulated DGEMM estimate %.3g above target %.3g with %d moduli", est, tol, nmod);
+      if (deferred) {
+        r.write_c = true;
+        r.err_sq = nullptr;
+        if (!check_cuda(launch_crt_reconstruct(r, st), "CRT reconstruction")) return EB2_ERR_CUDA;
+        info.launches += 1;
+        if (opt.sync && !check_cuda(cudaStreamSynchronize(st), "DGEMM")) return EB2_ERR_CUDA;
+      }
+      break;
+    }
+    // two more moduli: b grows by 4 bits, so every residue is recomputed
+    nmod += 2;
+    ++info.escalations;
+    info.slices = nmod;
+    if (!check_cuda(cudaMemsetAsync(df->err_sq, 0, sizeof(df->err_sq), st), "reset estimate") || !product(false))
+      return EB2_ERR_CUDA;
+  }
+  finish_timing(info.escalations == 0);
+  return EB2_OK;
+}
+
+}  // namespace
+
 int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
                     int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
                     cudaStream_t st, const DgemmOptions& opt, eb2_call_info& info) {
@@ -121,6 +297,8 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   };
   if (method == EB2_METHOD_NATIVE) return run_native(false);
   if (opt.timed) cudaEventRecord(cx.ev_start, st);
+  if (method == EB2_METHOD_CRT)
+    return dgemm_crt(cx, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, st, opt, info);
 
   // ---------------------------------------------------------- Ozaki emulation
   // Workspace: scan results first (they must survive the stage-2 decision), then the

@@ -11,6 +11,7 @@ namespace eb2 {
 struct DgemmOptions {
   int method = 0;        // EB2_METHOD_*; 0 = settings
   int slices = 0;        // 0 = chosen per call
+  int moduli = 0;        // CRT moduli; 0 = settings (default 16)
   int tile_n = 0;        // 0 = chosen per call
   double tol = 0.0;      // 0 = settings
   bool check_accuracy = true;  // a-posteriori estimate + added slices (needs a host sync)
@@ -28,6 +29,7 @@ struct SgemmOptions {
 
 int choose_tile_n(const Context& cx, int64_t m, int64_t n, bool ozaki);
 int choose_slices(int64_t m, int64_t n, int64_t k);
+int choose_crt_tile(const Context& cx, int64_t m, int64_t n);
 
 // C = alpha*op(A)op(B) + beta*C on device pointers.  Returns EB2_*.
 int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,

@@ -82,6 +82,77 @@ struct OzakiGemmArgs {
 cudaError_t launch_ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, const OzakiGemmArgs& args,
                               cudaStream_t stream);
 
+// ------------------------------------------------------------ CRT / Ozaki-II (emulated FP64)
+// Moduli of the CRT product: pairwise coprime, <= 256, largest first.
+constexpr int kCrtMaxModuli = 20;
+constexpr int kCrtDefaultModuli = 16;
+constexpr int kCrtLimbs = 6;  // 192-bit reconstruction arithmetic (32-bit limbs)
+constexpr int kCrtZeroRow = -(1 << 20);  // mu of a row without a nonzero finite entry
+// (p - 1 packed one byte each, so device code indexes no local array)
+__host__ __device__ constexpr int crt_modulus(int l) {
+  return int((l < 8 ? 0xe8eef0f6fafcfeffull : l < 16 ? 0xc0c4c6d2d8dee2e4ull : 0x00000000acb2b4beull) >>
+                 (8 * (l & 7)) &
+             0xFFu) +
+         1;
+}
+
+// P = p_0 ... p_(n-1), the CRT weights W_l = (P/p_l) ((P/p_l)^-1 mod p_l), P/2 (floor) and
+// b, the largest integer with 2^(2b+1) < P (row norms of the scaled operands <= 2^b).
+struct CrtConstants {
+  int n, b;
+  double P_inv;
+  uint32_t P[kCrtLimbs], half[kCrtLimbs];
+  uint32_t W[kCrtMaxModuli][kCrtLimbs];
+};
+const CrtConstants& crt_constants(int n);
+int crt_bits(int n);
+// Tile rows / columns of the CRT GEMM configurations (256: one CTA, 128 x 256 tiles;
+// kTilePair: a CTA pair, 256 x 256 tiles).
+int64_t crt_tile_rows(int tile_n);
+int64_t crt_tile_cols(int tile_n);
+
+// Per-operand workspace of the residue split.
+struct CrtOperand {
+  int8_t* residues;   // [nmax][rows_pad][k_pad] symmetric residues, row r contiguous along k
+  int32_t* mu;        // [rows_pad] scale exponents: A'_r = trunc(2^mu_r x_r) (kCrtZeroRow: A'_r = 0)
+  uint64_t* maxbits;  // [rows] bit pattern of max |x| (from launch_ozaki_scan)
+  uint64_t* sumsq;    // [rows] integer upper bound of the scaled sum of squares
+  int64_t rows, rows_pad, k, k_pad;
+  int nmax;
+};
+// Zero and accumulate the row norm bounds (needs maxbits).
+cudaError_t launch_crt_norms(const StridedView<double>& x, const CrtOperand& op, cudaStream_t stream);
+// mu and the residues for moduli [0, moduli) (needs maxbits and sumsq).
+cudaError_t launch_crt_split(const StridedView<double>& x, const CrtOperand& op, int moduli, cudaStream_t stream);
+
+struct CrtGemmArgs {
+  int64_t m, n;
+  int moduli;
+  const int* skip_if_flag;
+  uint32_t* status;
+  int tile_n;  // 256 or kTilePair
+  int num_sms;
+  uint8_t* cres;   // [moduli][n_pad][ld_res] residues of C' (uint8 in [0, p))
+  int64_t ld_res;  // = a.rows_pad
+};
+cudaError_t launch_crt_gemm(const CrtOperand& a, const CrtOperand& b, const CrtGemmArgs& args, cudaStream_t stream);
+
+struct CrtReconstructArgs {
+  int64_t m, n;
+  double alpha, beta;
+  double* C;
+  int64_t ldc;
+  const uint8_t* cres;
+  int64_t ld_res, plane;
+  int moduli;
+  const int32_t* mu_a;
+  const int32_t* mu_b;
+  double* err_sq;  // [2]: += estimated squared error, += squared alpha*A*B entries (may be null)
+  const int* skip_if_flag;
+  bool write_c;    // false: only the estimate
+};
+cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t stream);
+
 // ------------------------------------------------------------ split-BF16 (emulated FP32)
 struct Bf16Operand {
   void* pieces;  // [3][rows_pad][k_pad] bf16: hi, mid, lo pieces, row r contiguous along k

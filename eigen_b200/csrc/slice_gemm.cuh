@@ -28,16 +28,19 @@
 #include <cstdint>
 
 #include "device_common.cuh"
+#include "kernels.h"
 
 namespace eb2 {
 
-enum SliceMode : int { kModeOzakiI8 = 0, kModeSplitBF16 = 1 };
+enum SliceMode : int { kModeOzakiI8 = 0, kModeSplitBF16 = 1, kModeCrtI8 = 2 };
 
 constexpr int kSliceBM = 128;      // rows of A per CTA (TMEM lanes)
 constexpr int kSliceKBytes = 128;  // bytes of K per pipeline stage
 // One Ozaki accumulation unit covers at most this many 128-deep digit blocks per
 // output: 4095 * 128 * 64 * 64 < 2^31, so the INT32 accumulator cannot overflow.
 constexpr int kMaxUnitKb = 4095;
+// CRT residues lie in [-128, 127]: 1023 * 128 * 128 * 128 < 2^31.
+constexpr int kMaxUnitKbCrt = 1023;
 
 template <int BN, int STAGES, bool PAIR>
 struct SliceLayout {
@@ -73,10 +76,20 @@ struct SliceGemmParams {
   double* err_sq;        // Ozaki: [0] += energy of diagonal diag_hi, [1] += energy of diagonal 2
   uint32_t* status;
   int group_m;           // row-tiles per raster group (>= tiles_m: column-major tile order)
+  int crt;               // 1: CRT mode (unit t = modulus t, one slice pair (t, t))
+  uint8_t* residues;     // CRT: [moduli][cols][ld_res] residue planes (uint8 in [0, p))
+  int64_t ld_res;        // CRT: rows of one residue plane (padded m)
 };
 
 // Pair range of diagonal t: p = p_lo .. p_lo + total/num_kb - 1 (q = t - p).
-__device__ __forceinline__ bool diag_bounds(int t, int s, int num_kb, int& p_lo, int& total) {
+// In CRT mode "diagonal" t is modulus t with the single pair (t, t): p_lo = t + 1 and
+// the B slice is t (see b_slice()).
+__device__ __forceinline__ bool diag_bounds(int t, int s, int num_kb, int& p_lo, int& total, bool crt = false) {
+  if (crt) {
+    p_lo = t + 1;
+    total = num_kb;
+    return t >= 0 && t < s;
+  }
   p_lo = max(1, t - s);
   const int p_hi = min(s, t - 1);
   if (p_lo > p_hi) return false;
@@ -107,7 +120,7 @@ struct BlockIter {
         f = 0;
         continue;
       }
-      if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total) || f >= total) {
+      if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, P.crt != 0) || f >= total) {
         --t;
         f = 0;
         continue;
@@ -139,11 +152,16 @@ __device__ __forceinline__ double exp2_int(int E) {
 
 template <int MODE, int BN, bool PAIR>
 struct SliceTraits {
-  static constexpr int kKElems = MODE == kModeOzakiI8 ? kSliceKBytes : kSliceKBytes / 2;  // int8 / bf16
-  // instruction descriptor: Ozaki s8 x s8 -> s32, split-BF16 bf16 x bf16 -> f32; M = 128 or 256
-  static constexpr uint32_t kIdesc = MODE == kModeOzakiI8 ? make_idesc(2u, 1u, 1u, PAIR ? 256 : 128, BN)
-                                                          : make_idesc(1u, 1u, 1u, PAIR ? 256 : 128, BN);
+  static constexpr bool kInt8 = MODE != kModeSplitBF16;
+  static constexpr int kKElems = kInt8 ? kSliceKBytes : kSliceKBytes / 2;  // int8 / bf16
+  // instruction descriptor: s8 x s8 -> s32 (Ozaki, CRT), bf16 x bf16 -> f32 (split-BF16); M = 128 or 256
+  static constexpr uint32_t kIdesc = kInt8 ? make_idesc(2u, 1u, 1u, PAIR ? 256 : 128, BN)
+                                           : make_idesc(1u, 1u, 1u, PAIR ? 256 : 128, BN);
+  static constexpr int kUnitKb = MODE == kModeCrtI8 ? kMaxUnitKbCrt : kMaxUnitKb;
 };
+
+// B slice of a block: q - 1 = t - p - 1 for Ozaki/split-BF16 diagonals, t for CRT moduli.
+__device__ __forceinline__ int b_slice(int t, int p, bool crt) { return crt ? t : t - p - 1; }
 
 // Tile loop bounds of this CTA (the two CTAs of a pair walk one tile sequence).
 template <bool PAIR>
@@ -187,11 +205,12 @@ __device__ __forceinline__ void slice_producer(const CUtensorMap* tmA, const CUt
       const uint32_t leader_full = mapa_shared(smem_u32(&full[stage]), 0);
       if (rank == 0) mbar_arrive_expect_tx(&full[stage], kTx);
       tma_load_3d_pair(smem + L::kAOff + stage * L::kABytes, tmA, leader_full, kb * ke, a_row, p - 1);
-      tma_load_3d_pair(smem + L::kBOff + stage * L::kBBytes, tmB, leader_full, kb * ke, b_row, it.t - p - 1);
+      tma_load_3d_pair(smem + L::kBOff + stage * L::kBBytes, tmB, leader_full, kb * ke, b_row,
+                       b_slice(it.t, p, P.crt != 0));
     } else {
       mbar_arrive_expect_tx(&full[stage], kTx);
       tma_load_3d(smem + L::kAOff + stage * L::kABytes, tmA, &full[stage], kb * ke, a_row, p - 1);
-      tma_load_3d(smem + L::kBOff + stage * L::kBBytes, tmB, &full[stage], kb * ke, b_row, it.t - p - 1);
+      tma_load_3d(smem + L::kBOff + stage * L::kBBytes, tmB, &full[stage], kb * ke, b_row, b_slice(it.t, p, P.crt != 0));
     }
     ++issued;
     it.next(P, num_tiles);
@@ -239,9 +258,10 @@ __device__ __forceinline__ void slice_mma(uint8_t* smem, uint64_t* full, uint64_
     }
     for (int t = P.diag_hi; t >= P.diag_lo && ok; --t) {
       int p_lo, total;
-      if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total)) continue;
+      if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, MODE == kModeCrtI8)) continue;
+      constexpr int kUnit = SliceTraits<MODE, BN, PAIR>::kUnitKb;
       for (int u0 = 0; u0 < total && ok;) {
-        const int u1 = (kTileUnit || total - u0 <= kMaxUnitKb) ? total : u0 + kMaxUnitKb;
+        const int u1 = (kTileUnit || total - u0 <= kUnit) ? total : u0 + kUnit;
         if (!kTileUnit) {
           if (!mbar_wait(&tempty[buf], ((tphase >> buf) & 1u) ^ 1u, abort_flag, P.status)) {
             ok = false;
@@ -265,12 +285,12 @@ __device__ __forceinline__ void slice_mma(uint8_t* smem, uint64_t* full, uint64_
             const uint32_t acc = (fresh && kk == 0) ? 0u : 1u;
             const uint64_t ad = adesc + uint64_t(2 * kk), bd = bdesc + uint64_t(2 * kk);
             if (PAIR) {
-              if (MODE == kModeOzakiI8)
+              if (MODE != kModeSplitBF16)
                 mma_i8_pair(d_tmem, ad, bd, idesc, acc);
               else
                 mma_f16_pair(d_tmem, ad, bd, idesc, acc);
             } else {
-              if (MODE == kModeOzakiI8)
+              if (MODE != kModeSplitBF16)
                 mma_i8(d_tmem, ad, bd, idesc, acc);
               else
                 mma_f16(d_tmem, ad, bd, idesc, acc);
@@ -412,6 +432,81 @@ __device__ __forceinline__ void ozaki_epilogue(uint32_t tmem_base, uint64_t* tfu
   }
 }
 
+// x mod p for a 32-bit x and p <= 256, with m = floor((2^32 - 1) / p): the estimate
+// q = umulhi(x, m) is at most 2 short of floor(x / p).
+__device__ __forceinline__ uint32_t mod_small(uint32_t x, uint32_t p, uint32_t m) {
+  uint32_t r = x - __umulhi(x, m) * p;
+  if (r >= p) r -= p;
+  if (r >= p) r -= p;
+  return r;
+}
+
+// CRT: unit t is modulus p_t; every INT32 product entry is reduced to [0, p_t) and stored
+// as one byte of residue plane t (column-major, ld_res).  K beyond one unit comes in
+// further chunks whose residues are added mod p_t.
+template <int BN, int NW, bool PAIR>
+__device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull, uint64_t* tempty,
+                                             volatile int* abort_flag, const SliceGemmParams& P) {
+  constexpr int kCols = BN * 4 / NW;
+  static_assert(kCols % 32 == 0, "column slice");
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int quad = warp & 3;
+  const int col_base = ((warp - 2) >> 2) * kCols;
+  const int row = quad * 32 + lane;
+  const int num_tiles = P.tiles_m * P.tiles_n;
+  const int row_base = PAIR ? int(cluster_ctarank()) * kSliceBM : 0;
+  const int64_t plane = P.ld_res * int64_t(P.tiles_n) * BN;
+  int buf = 0;
+  uint32_t ephase = 0u;
+  bool ok = true;
+  for (int tile = first_tile<PAIR>(); tile < num_tiles && ok; tile += tile_step<PAIR>()) {
+    int tm, tn;
+    tile_coords(tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
+    const int64_t m0 = int64_t(tm) * (PAIR ? 2 * kSliceBM : kSliceBM) + row_base;
+    const int64_t n0 = int64_t(tn) * BN + col_base;
+    const int64_t grow = m0 + row;
+    for (int t = P.diag_hi; t >= P.diag_lo && ok; --t) {
+      int p_lo, total;
+      if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, true)) continue;
+      const uint32_t pm = uint32_t(crt_modulus(t));
+      const uint32_t magic = 0xFFFFFFFFu / pm;
+      uint8_t* rp = P.residues + int64_t(t) * plane + grow;
+      for (int u0 = 0; u0 < total && ok; u0 += kMaxUnitKbCrt) {
+        if (!mbar_wait(&tfull[buf], (ephase >> buf) & 1u, abort_flag, P.status)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t taddr = tmem_base + uint32_t(buf * BN + col_base) + (uint32_t(quad * 32) << 16);
+#pragma unroll 1
+        for (int c = 0; c < kCols / 32; ++c) {
+          uint32_t r[32];
+          tmem_ld_32x32b_x32(taddr + uint32_t(c * 32), r);
+          tmem_ld_wait();
+          if (grow < P.ld_res) {
+#pragma unroll
+            for (int jj = 0; jj < 32; ++jj) {
+              const int32_t v = static_cast<int32_t>(r[jj]);
+              uint32_t res = mod_small(v < 0 ? 0u - uint32_t(v) : uint32_t(v), pm, magic);
+              if (v < 0 && res) res = pm - res;
+              uint8_t* dst = rp + (n0 + c * 32 + jj) * P.ld_res;
+              if (u0 > 0) {
+                res += *dst;
+                if (res >= pm) res -= pm;
+              }
+              *dst = uint8_t(res);
+            }
+          }
+        }
+        tc_fence_before();
+        acc_release<PAIR>(&tempty[buf]);
+        ephase ^= 1u << buf;
+        buf ^= 1;
+      }
+    }
+  }
+}
+
 // Split-BF16: C = alpha * acc + beta * C in FP32, one unit per tile.
 template <int BN, int NW, bool PAIR>
 __device__ __forceinline__ void bf16_epilogue(uint32_t tmem_base, uint64_t* tfull, uint64_t* tempty,
@@ -526,6 +621,8 @@ __global__ void __launch_bounds__(64 + 32 * NW, 1)
   } else {
     if constexpr (MODE == kModeOzakiI8)
       ozaki_epilogue<BN, NW, PAIR>(tmem_base, tfull, tempty, col_exp, abort_flag, P);
+    else if constexpr (MODE == kModeCrtI8)
+      crt_epilogue<BN, NW, PAIR>(tmem_base, tfull, tempty, abort_flag, P);
     else
       bf16_epilogue<BN, NW, PAIR>(tmem_base, tfull, tempty, abort_flag, P);
   }

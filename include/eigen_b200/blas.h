@@ -71,13 +71,19 @@ enum {
 enum {
   EB2_METHOD_AUTO = 0,     /* DGEMM: Ozaki INT8 emulation; SGEMM: split-BF16 on tcgen05 */
   EB2_METHOD_NATIVE = 1,   /* DGEMM: FP64 DMMA kernel; SGEMM: FP32 FFMA kernel */
-  EB2_METHOD_EMULATED = 2  /* force the emulated method */
+  EB2_METHOD_EMULATED = 2, /* DGEMM: Ozaki digit slices (scheme I); SGEMM: split-BF16 */
+  EB2_METHOD_CRT = 3       /* DGEMM: Ozaki scheme II, INT8 products modulo coprime moduli
+                              recombined by the Chinese remainder theorem */
 };
 
 int eb2_set_dgemm_method(int method);
 int eb2_set_sgemm_method(int method);
 /* Digit slices per operand for the emulated DGEMM (2..12); 0 = chosen per call. */
 int eb2_set_dgemm_slices(int slices);
+/* Moduli of the CRT-form emulated DGEMM (8..20; 0 = default 16).  With N moduli every
+ * row of op(A) and column of op(B) keeps about b bits relative to its 2-norm, b = 62 for
+ * 16, 69 for 18, 77 for 20; the a-posteriori check adds two moduli at a time. */
+int eb2_set_dgemm_moduli(int moduli);
 /* Accuracy target of the emulated DGEMM: the a-posteriori estimate of
  * ||C - C_exact||_F / ||alpha*op(A)op(B)||_F must not exceed it (default 2^-53);
  * slices are added one at a time until it holds or 12 are used. */
@@ -102,10 +108,10 @@ void eb2_clear_error(void);
 /* Details of the last product computed by this thread. */
 typedef struct eb2_call_info {
   int dtype;          /* 'd' or 's' */
-  int method;         /* EB2_METHOD_NATIVE or EB2_METHOD_EMULATED */
-  int slices;         /* digit slices (DGEMM emulated) or BF16 products (SGEMM emulated) */
-  int tile_n;         /* tcgen05 tile width, 0 for native kernels */
-  int escalations;    /* slices added by the a-posteriori check */
+  int method;         /* EB2_METHOD_NATIVE, EB2_METHOD_EMULATED or EB2_METHOD_CRT */
+  int slices;         /* digit slices or moduli (DGEMM emulated), BF16 products (SGEMM emulated) */
+  int tile_n;         /* tcgen05 tile configuration, 0 for native kernels */
+  int escalations;    /* slices (or pairs of moduli) added by the a-posteriori check */
   int nonfinite;      /* 1 if NaN/Inf inputs sent the call to the native kernel */
   int staged;         /* 1 if host buffers were staged through device memory */
   double err_estimate; /* a-posteriori relative error estimate (emulated DGEMM), else -1 */

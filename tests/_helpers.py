@@ -61,6 +61,17 @@ def oracle():
     return lib
 
 
+@lru_cache(maxsize=1)
+def crt_model():
+    """The exact CPU model of the CRT-form emulated DGEMM (oracle/ozaki2.py)."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("oracle_ozaki2", ORACLE_DIR / "ozaki2.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def P(a: np.ndarray | None):
     return None if a is None else a.ctypes.data_as(_vp)
 
