@@ -260,14 +260,20 @@ __device__ __forceinline__ uint32_t residue_of(const Chunks21& c, const CrtModCo
 constexpr int kSplitRowsCrt = 32;
 constexpr int kSplitColsCrt = 128;
 
+constexpr int kSplitThreadsCrt = 512;  // 16 threads per row, 8 entries each
+
+// |t| mod p for |t| < 2^63 (at most 16 moduli: |t| <= 2^62) without the 2^63 chunk
+__device__ __forceinline__ uint32_t residue_of3(const Chunks21& c, const CrtModConst& k) {
+  return mod_small(c.a0 + c.a1 * k.c21 + c.a2 * k.c42, k.p, k.magic);
+}
+
 // Residues of A' = trunc(2^mu_r x) for moduli [0, n): plane l at residues + l*rows_pad*k_pad,
 // row r contiguous along k; symmetric int8 representatives.  Blocks of column 0 write mu_r.
-__global__ void __launch_bounds__(256) crt_split_kernel(const double* __restrict__ X, int64_t rows, int64_t cols,
-                                                        int64_t sr, int64_t sl,
-                                                        const unsigned long long* __restrict__ maxbits,
-                                                        const unsigned long long* __restrict__ sumsq, int b, int n,
-                                                        int8_t* __restrict__ residues, int32_t* __restrict__ mu,
-                                                        int64_t rows_pad, int64_t k_pad) {
+template <bool kWide>  // kWide: |t| may reach 2^63 (more than 16 moduli)
+__global__ void __launch_bounds__(kSplitThreadsCrt) crt_split_kernel(
+    const double* __restrict__ X, int64_t rows, int64_t cols, int64_t sr, int64_t sl,
+    const unsigned long long* __restrict__ maxbits, const unsigned long long* __restrict__ sumsq, int b, int n,
+    int8_t* __restrict__ residues, int32_t* __restrict__ mu, int64_t rows_pad, int64_t k_pad) {
   __shared__ double tile[kSplitRowsCrt][kSplitColsCrt + 1];
   __shared__ int row_mu_s[kSplitRowsCrt];
   const int64_t r0 = int64_t(blockIdx.y) * kSplitRowsCrt;
@@ -292,36 +298,32 @@ __global__ void __launch_bounds__(256) crt_split_kernel(const double* __restrict
     tile[rr][ll] = (r < rows && l < cols) ? X[r * sr + l * sl] : 0.0;
   }
   __syncthreads();
-  const int rr = threadIdx.x >> 3;
-  const int cb = (threadIdx.x & 7) * 16;
+  const int rr = threadIdx.x >> 4;
+  const int cb = (threadIdx.x & 15) * 8;
   const int m = row_mu_s[rr];
-  double at[16];
+  Chunks21 ch[8];
   uint32_t neg = 0;
 #pragma unroll
-  for (int j = 0; j < 16; ++j) {
+  for (int j = 0; j < 8; ++j) {
     // |v| <= 2^b, an exact integer (0 in zero rows: 2^kCrtZeroRow underflows to 0)
     const double v = trunc(scale2(tile[rr][cb + j], m));
-    at[j] = fabs(v);
+    ch[j] = chunks21(fabs(v));
     neg |= (v < 0.0 ? 1u : 0u) << j;
   }
-  const int64_t row = r0 + rr;
-  Chunks21 ch[16];
-#pragma unroll
-  for (int j = 0; j < 16; ++j) ch[j] = chunks21(at[j]);
+  int8_t* dst = residues + (size_t(r0 + rr)) * size_t(k_pad) + size_t(l0 + cb);
+  const size_t plane = size_t(rows_pad) * size_t(k_pad);
   for (int l = 0; l < n; ++l) {
     const CrtModConst k = kModConst[l];
     const int hi = int(k.p >> 1) - ((k.p & 1u) ? 0 : 1);  // largest representative kept as is
-    uint32_t w[4] = {0u, 0u, 0u, 0u};
+    uint32_t w[2] = {0u, 0u};
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      uint32_t res = residue_of(ch[j], k);
+    for (int j = 0; j < 8; ++j) {
+      uint32_t res = kWide ? residue_of(ch[j], k) : residue_of3(ch[j], k);
       if (((neg >> j) & 1u) && res) res = k.p - res;  // residue of the negative value
       const int sres = int(res) > hi ? int(res) - int(k.p) : int(res);  // [-(p/2), (p-1)/2]
       w[j >> 2] |= (uint32_t(sres) & 0xFFu) << (8 * (j & 3));
     }
-    uint4* dst = reinterpret_cast<uint4*>(residues + (size_t(l) * size_t(rows_pad) + size_t(row)) * size_t(k_pad) +
-                                          size_t(l0 + cb));
-    *dst = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint2*>(dst + size_t(l) * plane) = make_uint2(w[0], w[1]);
   }
 }
 
@@ -372,108 +374,190 @@ __device__ __forceinline__ double scale_exp(double d, int e) {
   return scale2(d, e);
 }
 
-// One thread per element (i, j): C'_ij from its residues, then C_ij.
+// C_ij from RN(C'_ij) = d 2^shift (signed d): scale by 2^-(mu_i + nu_j), apply alpha and
+// beta, and add the estimate terms: e += 2^(2(b - mu_i - nu_j)) (the squared truncation
+// error bound, up to the factor 2/3 alpha^2 applied per block), v += (alpha C')^2.
+__device__ __forceinline__ void crt_store(const CrtRecParams& R, int64_t i, int64_t j, double d, int shift,
+                                          double& e_acc, double& v_acc) {
+  const int mu_i = R.mu_a[i], nu_j = R.mu_b[j];
+  const double val = d != 0.0 ? scale_exp(d, shift - mu_i - nu_j) : 0.0;  // d = 0 in zero rows
+  const double v = __dmul_rn(R.alpha, val);
+  if (R.write_c) {
+    double* c = R.C + j * R.ldc + i;
+    *c = R.beta == 0.0 ? v : __fma_rn(R.beta, *c, v);
+  }
+  if (R.err_sq) {
+    // truncation errors need a nonzero row on both sides
+    if (mu_i != kCrtZeroRow && nu_j != kCrtZeroRow) e_acc += exp2_int(2 * (R.b - mu_i - nu_j));
+    v_acc += v * v;
+  }
+}
+
+// One pair of atomics per block (same-address atomics serialise in L2).
+__device__ __forceinline__ void crt_reduce_energies(const CrtRecParams& R, double e_acc, double v_acc) {
+  __shared__ double red[2][8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    e_acc += __shfl_xor_sync(0xffffffffu, e_acc, o);
+    v_acc += __shfl_xor_sync(0xffffffffu, v_acc, o);
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][w] = e_acc;
+    red[1][w] = v_acc;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double e = 0.0, v = 0.0;
+    for (int q = 0; q < 8; ++q) {
+      e += red[0][q];
+      v += red[1][q];
+    }
+    e *= (2.0 / 3.0) * R.alpha * R.alpha;  // rms of a truncation error in (-1, 1): 1/sqrt(3)
+    if (e != 0.0) atomicAdd(&R.err_sq[0], e);
+    if (v != 0.0) atomicAdd(&R.err_sq[1], v);
+  }
+}
+
+constexpr int kRecCols = 8;  // columns per block and pass
+
+// One thread per row i, kRecCols columns per pass: C'_ij from its residues, then C_ij.
 __global__ void __launch_bounds__(256) crt_reconstruct_kernel(const __grid_constant__ CrtRecParams R) {
   if (R.skip_if_flag && *R.skip_if_flag) return;
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double e_acc = 0.0, v_acc = 0.0;
-  const double e_scale = 0.816496580927726;  // sqrt(2/3): rms of the truncation error
-  for (int64_t j = blockIdx.y; j < R.ncols; j += gridDim.y) {
-    if (i >= R.m) break;
-    const uint8_t* rp = R.res + j * R.ld_res + i;
-    unsigned long long acc[kCrtLimbs] = {0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
-    // unrolled over the largest modulus count: the weights are immediate constant-bank operands
+  // blockIdx.y walks groups of kRecCols columns
+  const int64_t jstep = int64_t(gridDim.y) * kRecCols;
+  for (int64_t j0 = int64_t(blockIdx.y) * kRecCols; i < R.m && j0 < R.ncols; j0 += jstep) {
+    const int64_t j1 = j0 + kRecCols < R.ncols ? j0 + kRecCols : R.ncols;
+    for (int64_t j = j0; j < j1; ++j) {
+      const uint8_t* rp = R.res + j * R.ld_res + i;
+      unsigned long long acc[kCrtLimbs] = {0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
+      // unrolled over the largest modulus count: the weights are immediate constant-bank operands
 #pragma unroll
-    for (int l = 0; l < kCrtMaxModuli; ++l) {
-      if (l < R.n) {
-        const uint32_t r = rp[int64_t(l) * R.plane];
+      for (int l = 0; l < kCrtMaxModuli; ++l) {
+        if (l < R.n) {
+          const uint32_t r = rp[int64_t(l) * R.plane];
 #pragma unroll
-        for (int q = 0; q < kCrtLimbs; ++q) acc[q] += static_cast<unsigned long long>(r) * R.W[l][q];
+          for (int q = 0; q < kCrtLimbs; ++q) acc[q] += static_cast<unsigned long long>(r) * R.W[l][q];
+        }
       }
-    }
-    // S = sum r_l W_l < n * 256 * P < 2^192 as six 32-bit limbs
-    uint32_t s[kCrtLimbs];
-    unsigned long long carry = 0;
-#pragma unroll
-    for (int q = 0; q < kCrtLimbs; ++q) {
-      const unsigned long long v = acc[q] + carry;
-      s[q] = uint32_t(v);
-      carry = v >> 32;
-    }
-    // R = S - q P with q = rint(S / P); then R is C' or C' +- P
-    double sd = 0.0;
-#pragma unroll
-    for (int q = kCrtLimbs - 1; q >= 0; --q) sd = fma(sd, 4294967296.0, double(s[q]));
-    const uint32_t qq = uint32_t(rint(sd * R.P_inv));
-    long long borrow = 0;
-    unsigned long long mcarry = 0;
-#pragma unroll
-    for (int q = 0; q < kCrtLimbs; ++q) {
-      const unsigned long long qp = static_cast<unsigned long long>(qq) * R.P[q] + mcarry;
-      mcarry = qp >> 32;
-      const long long d = static_cast<long long>(s[q]) - static_cast<long long>(uint32_t(qp)) + borrow;
-      s[q] = uint32_t(d);
-      borrow = d >> 32;  // 0 or -1
-    }
-    bool negative = (s[kCrtLimbs - 1] >> 31) != 0;
-    if (negative) {  // two's complement negate
-      unsigned long long c = 1;
+      // S = sum r_l W_l < n * 256 * P < 2^192 as six 32-bit limbs
+      uint32_t s[kCrtLimbs];
+      unsigned long long carry = 0;
 #pragma unroll
       for (int q = 0; q < kCrtLimbs; ++q) {
-        const unsigned long long v = static_cast<unsigned long long>(~s[q]) + c;
+        const unsigned long long v = acc[q] + carry;
         s[q] = uint32_t(v);
-        c = v >> 32;
+        carry = v >> 32;
       }
-    }
-    // |R| > P/2: the representative is P - |R| with the opposite sign
-    bool above = false;
+      // R = S - q P with q = rint(S / P); then R is C' or C' +- P
+      double sd = 0.0;
 #pragma unroll
-    for (int q = kCrtLimbs - 1; q >= 0; --q) {
-      if (s[q] != R.half[q]) {
-        above = s[q] > R.half[q];
-        break;
-      }
-    }
-    if (above) {
-      long long bw = 0;
+      for (int q = kCrtLimbs - 1; q >= 0; --q) sd = fma(sd, 4294967296.0, double(s[q]));
+      const uint32_t qq = uint32_t(rint(sd * R.P_inv));
+      long long borrow = 0;
+      unsigned long long mcarry = 0;
 #pragma unroll
       for (int q = 0; q < kCrtLimbs; ++q) {
-        const long long d = static_cast<long long>(R.P[q]) - static_cast<long long>(s[q]) + bw;
+        const unsigned long long qp = static_cast<unsigned long long>(qq) * R.P[q] + mcarry;
+        mcarry = qp >> 32;
+        const long long d = static_cast<long long>(s[q]) - static_cast<long long>(uint32_t(qp)) + borrow;
         s[q] = uint32_t(d);
-        bw = d >> 32;
+        borrow = d >> 32;  // 0 or -1
       }
-      negative = !negative;
-    }
-    int shift;
-    double d = limbs_to_double(s, shift);
-    if (negative) d = -d;
-    const int mu_i = R.mu_a[i], nu_j = R.mu_b[j];
-    const double val = d != 0.0 ? scale_exp(d, shift - mu_i - nu_j) : 0.0;  // d = 0 in zero rows
-    const double v = __dmul_rn(R.alpha, val);
-    if (R.write_c) {
-      double* c = R.C + j * R.ldc + i;
-      *c = R.beta == 0.0 ? v : __fma_rn(R.beta, *c, v);
-    }
-    if (R.err_sq) {
-      // truncation errors need a nonzero row on both sides
-      if (mu_i != kCrtZeroRow && nu_j != kCrtZeroRow) {
-        const double eij = ldexp(e_scale * fabs(R.alpha), R.b - mu_i - nu_j);
-        e_acc += eij * eij;
-      }
-      v_acc += v * v;
-    }
-  }
-  if (R.err_sq) {
+      bool negative = (s[kCrtLimbs - 1] >> 31) != 0;
+      if (negative) {  // two's complement negate
+        unsigned long long c = 1;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      e_acc += __shfl_xor_sync(0xffffffffu, e_acc, o);
-      v_acc += __shfl_xor_sync(0xffffffffu, v_acc, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-      if (e_acc != 0.0) atomicAdd(&R.err_sq[0], e_acc);
-      if (v_acc != 0.0) atomicAdd(&R.err_sq[1], v_acc);
+        for (int q = 0; q < kCrtLimbs; ++q) {
+          const unsigned long long v = static_cast<unsigned long long>(~s[q]) + c;
+          s[q] = uint32_t(v);
+          c = v >> 32;
+        }
+      }
+      // |R| > P/2: the representative is P - |R| with the opposite sign
+      bool above = false;
+#pragma unroll
+      for (int q = kCrtLimbs - 1; q >= 0; --q) {
+        if (s[q] != R.half[q]) {
+          above = s[q] > R.half[q];
+          break;
+        }
+      }
+      if (above) {
+        long long bw = 0;
+#pragma unroll
+        for (int q = 0; q < kCrtLimbs; ++q) {
+          const long long d = static_cast<long long>(R.P[q]) - static_cast<long long>(s[q]) + bw;
+          s[q] = uint32_t(d);
+          bw = d >> 32;
+        }
+        negative = !negative;
+      }
+      int shift;
+      double d = limbs_to_double(s, shift);
+      crt_store(R, i, j, negative ? -d : d, shift, e_acc, v_acc);
     }
   }
+  if (R.err_sq) crt_reduce_energies(R, e_acc, v_acc);
+}
+
+// The same for at most 16 moduli: P < 2^126, so W_l fits four limbs, S = sum r_l W_l is
+// known modulo 2^128, and R = S - q P (|R| < 1.5 P < 2^127) is exact in 128-bit two's
+// complement.  Bit for bit the result of the kernel above (both round C' once).
+__global__ void __launch_bounds__(256) crt_reconstruct128_kernel(const __grid_constant__ CrtRecParams R) {
+  using u128 = unsigned __int128;
+  using s128 = __int128;
+  if (R.skip_if_flag && *R.skip_if_flag) return;
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  double e_acc = 0.0, v_acc = 0.0;
+  const u128 P = (u128(R.P[3]) << 96) | (u128(R.P[2]) << 64) | (u128(R.P[1]) << 32) | u128(R.P[0]);
+  const s128 half = s128(P >> 1);
+  const int64_t jstep = int64_t(gridDim.y) * kRecCols;
+  for (int64_t j0 = int64_t(blockIdx.y) * kRecCols; i < R.m && j0 < R.ncols; j0 += jstep) {
+    const int64_t j1 = j0 + kRecCols < R.ncols ? j0 + kRecCols : R.ncols;
+    for (int64_t j = j0; j < j1; ++j) {
+      const uint8_t* rp = R.res + j * R.ld_res + i;
+      unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
+#pragma unroll
+      for (int l = 0; l < 16; ++l) {
+        if (l < R.n) {
+          const uint32_t r = rp[int64_t(l) * R.plane];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[q] += static_cast<unsigned long long>(r) * R.W[l][q];
+        }
+      }
+      // q = rint(S / P) from the partial sums in FP64; it may be off by one near a
+      // half-integer, which the range fix below absorbs
+      const double sd =
+          fma(double(acc[3]), 0x1p96, fma(double(acc[2]), 0x1p64, fma(double(acc[1]), 0x1p32, double(acc[0]))));
+      const u128 q = u128(static_cast<unsigned long long>(rint(sd * R.P_inv)));
+      const u128 S = u128(acc[0]) + (u128(acc[1]) << 32) + (u128(acc[2]) << 64) + (u128(acc[3]) << 96);
+      s128 r = s128(S - q * P);
+      if (r > half)
+        r -= s128(P);
+      else if (r < -half)
+        r += s128(P);
+      const bool negative = r < 0;
+      const u128 mag = negative ? u128(-r) : u128(r);
+      const unsigned long long hi = static_cast<unsigned long long>(mag >> 64);
+      const unsigned long long lo = static_cast<unsigned long long>(mag);
+      double d;
+      int shift = 0;
+      if (hi == 0) {
+        d = __ull2double_rn(lo);
+      } else {  // top 64 bits and a sticky bit: one correct rounding
+        const int lz = __clzll(static_cast<long long>(hi));
+        const unsigned long long u = lz ? (hi << lz) | (lo >> (64 - lz)) : hi;
+        const unsigned long long sticky = (lo << lz) != 0ull ? 1ull : 0ull;
+        d = __ull2double_rn(u | sticky);
+        shift = 64 - lz;
+      }
+      crt_store(R, i, j, negative ? -d : d, shift, e_acc, v_acc);
+    }
+  }
+  if (R.err_sq) crt_reduce_energies(R, e_acc, v_acc);
 }
 
 template <int BN, int STAGES, bool PAIR>
@@ -528,10 +612,15 @@ cudaError_t launch_crt_split(const StridedView<double>& x, const CrtOperand& op,
   if (op.k_pad % kSplitColsCrt != 0 || op.rows_pad % kSplitRowsCrt != 0) return cudaErrorInvalidValue;
   dim3 grid(unsigned(op.k_pad / kSplitColsCrt), unsigned(op.rows_pad / kSplitRowsCrt));
   if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
-  crt_split_kernel<<<grid, 256, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl,
-                                             reinterpret_cast<const unsigned long long*>(op.maxbits),
-                                             reinterpret_cast<const unsigned long long*>(op.sumsq),
-                                             crt_bits(moduli), moduli, op.residues, op.mu, op.rows_pad, op.k_pad);
+  const unsigned long long* mb = reinterpret_cast<const unsigned long long*>(op.maxbits);
+  const unsigned long long* ss = reinterpret_cast<const unsigned long long*>(op.sumsq);
+  const int b = crt_bits(moduli);
+  if (b <= 62)
+    crt_split_kernel<false><<<grid, kSplitThreadsCrt, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl, mb, ss, b,
+                                                                  moduli, op.residues, op.mu, op.rows_pad, op.k_pad);
+  else
+    crt_split_kernel<true><<<grid, kSplitThreadsCrt, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl, mb, ss, b,
+                                                                 moduli, op.residues, op.mu, op.rows_pad, op.k_pad);
   return cudaGetLastError();
 }
 
@@ -569,8 +658,12 @@ cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t 
   R.skip_if_flag = args.skip_if_flag;
   R.write_c = args.write_c ? 1 : 0;
   const unsigned gx = unsigned((args.m + 255) / 256);
-  const unsigned gy = unsigned(args.n < 65535 ? args.n : 65535);
-  crt_reconstruct_kernel<<<dim3(gx, gy), 256, 0, stream>>>(R);
+  const int64_t groups = (args.n + kRecCols - 1) / kRecCols;
+  const unsigned gy = unsigned(groups < 65535 ? groups : 65535);
+  if (args.moduli <= 16)
+    crt_reconstruct128_kernel<<<dim3(gx, gy), 256, 0, stream>>>(R);
+  else
+    crt_reconstruct_kernel<<<dim3(gx, gy), 256, 0, stream>>>(R);
   return cudaGetLastError();
 }
 
