@@ -114,6 +114,9 @@ def load(path: str | os.PathLike | None = None, mode: int = ctypes.RTLD_GLOBAL) 
     lib.eb2_sgemm_device.argtypes = [ctypes.c_char, ctypes.c_char, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                      ctypes.c_float, vp, ctypes.c_int64, vp, ctypes.c_int64, ctypes.c_float, vp,
                                      ctypes.c_int64, vp]
+    lib.eb2_dgemm_device_noalloc.argtypes = [ctypes.c_char, ctypes.c_char, ctypes.c_int64, ctypes.c_int64,
+                                             ctypes.c_int64, ctypes.c_double, vp, ctypes.c_int64, vp, ctypes.c_int64,
+                                             ctypes.c_double, vp, ctypes.c_int64, vp]
     pp = ctypes.POINTER(GemmProblem)
     lib.eb2_grouped_plan_create.argtypes = [ctypes.c_char, ctypes.c_int64, pp, ctypes.POINTER(ctypes.c_void_p)]
     lib.eb2_grouped_plan_execute.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
@@ -182,6 +185,13 @@ def dgemm_device(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, s
 def sgemm_device(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream=0) -> int:
     return load().eb2_sgemm_device(transa.encode(), transb.encode(), m, n, k, alpha, _ptr(a), lda, _ptr(b), ldb, beta,
                                    _ptr(c), ldc, stream or None)
+
+
+def dgemm_device_noalloc(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream=0) -> int:
+    """eb2_dgemm_device_noalloc: the CRT-form DGEMM with its scratch in a fixed device array
+    (no device allocation; for callers whose memory is owned by another allocator)."""
+    return load().eb2_dgemm_device_noalloc(transa.encode(), transb.encode(), m, n, k, alpha, _ptr(a), lda, _ptr(b),
+                                           ldb, beta, _ptr(c), ldc, stream or None)
 
 
 def set_dgemm_method(method: int) -> int:

@@ -137,6 +137,23 @@ int eb2_dgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, 
 int eb2_sgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, float alpha, const float* a,
                      int64_t lda, const float* b, int64_t ldb, float beta, float* c, int64_t ldc, void* stream);
 
+/* DGEMM on device pointers that allocates nothing.  No counterpart in the reference: it
+ * serves callers that cannot let a library call cudaMalloc -- a process whose GPU memory
+ * is already reserved by another allocator (a framework's caching allocator, a pool sized
+ * at start-up), or a code path that must not allocate or free (cudaMalloc and cudaFree may
+ * synchronise the device or fail).  It computes the CRT-form emulated product (16 moduli,
+ * no a-posteriori check, NaN/Inf inputs on the native kernel) with all scratch in one
+ * fixed 64 MiB device array that the library holds on every GPU where it is loaded, until
+ * the process exits.  Square products up to 1024 x 1024 x 1024 fit; a product that
+ * needs more returns EB2_ERR_ARG, with the size in eb2_last_error_string, before any launch.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress,
+ * with that device current); make that first call before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU (other streams, other host threads)
+ * race and corrupt each other's results.  Waits for `stream` before returning. */
+int eb2_dgemm_device_noalloc(char transa, char transb, int64_t m, int64_t n, int64_t k, double alpha,
+                             const double* a, int64_t lda, const double* b, int64_t ldb, double beta, double* c,
+                             int64_t ldc, void* stream);
+
 /* ---------------------------------------------------------------- grouped products
  * Thousands of independent products C_i = alpha_i*op(A_i)op(B_i) + beta_i*C_i (device
  * pointers, column-major) in ONE persistent launch.  Eigen has no batch entry point;
