@@ -344,6 +344,7 @@ struct CrtRecParams {
   double* err_sq;  // [0] += estimated squared error, [1] += squared alpha*A*B entries
   const int* skip_if_flag;
   int write_c;
+  int cols_per_block;  // columns one block handles per pass (fewer when the grid would be small)
 };
 
 // RN(|R|) of a 192-bit magnitude as d * 2^shift, d an integer-valued double < 2^64:
@@ -419,17 +420,18 @@ __device__ __forceinline__ void crt_reduce_energies(const CrtRecParams& R, doubl
   }
 }
 
-constexpr int kRecCols = 8;  // columns per block and pass
+constexpr int kRecCols = 8;  // most columns per block and pass
 
-// One thread per row i, kRecCols columns per pass: C'_ij from its residues, then C_ij.
+// One thread per row i, cols_per_block columns per pass: C'_ij from its residues, then C_ij.
 __global__ void __launch_bounds__(256) crt_reconstruct_kernel(const __grid_constant__ CrtRecParams R) {
   if (R.skip_if_flag && *R.skip_if_flag) return;
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double e_acc = 0.0, v_acc = 0.0;
-  // blockIdx.y walks groups of kRecCols columns
-  const int64_t jstep = int64_t(gridDim.y) * kRecCols;
-  for (int64_t j0 = int64_t(blockIdx.y) * kRecCols; i < R.m && j0 < R.ncols; j0 += jstep) {
-    const int64_t j1 = j0 + kRecCols < R.ncols ? j0 + kRecCols : R.ncols;
+  // blockIdx.y walks groups of cols_per_block columns
+  const int cpb = R.cols_per_block;
+  const int64_t jstep = int64_t(gridDim.y) * cpb;
+  for (int64_t j0 = int64_t(blockIdx.y) * cpb; i < R.m && j0 < R.ncols; j0 += jstep) {
+    const int64_t j1 = j0 + cpb < R.ncols ? j0 + cpb : R.ncols;
     for (int64_t j = j0; j < j1; ++j) {
       const uint8_t* rp = R.res + j * R.ld_res + i;
       unsigned long long acc[kCrtLimbs] = {0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
@@ -514,9 +516,10 @@ __global__ void __launch_bounds__(256) crt_reconstruct128_kernel(const __grid_co
   double e_acc = 0.0, v_acc = 0.0;
   const u128 P = (u128(R.P[3]) << 96) | (u128(R.P[2]) << 64) | (u128(R.P[1]) << 32) | u128(R.P[0]);
   const s128 half = s128(P >> 1);
-  const int64_t jstep = int64_t(gridDim.y) * kRecCols;
-  for (int64_t j0 = int64_t(blockIdx.y) * kRecCols; i < R.m && j0 < R.ncols; j0 += jstep) {
-    const int64_t j1 = j0 + kRecCols < R.ncols ? j0 + kRecCols : R.ncols;
+  const int cpb = R.cols_per_block;
+  const int64_t jstep = int64_t(gridDim.y) * cpb;
+  for (int64_t j0 = int64_t(blockIdx.y) * cpb; i < R.m && j0 < R.ncols; j0 += jstep) {
+    const int64_t j1 = j0 + cpb < R.ncols ? j0 + cpb : R.ncols;
     for (int64_t j = j0; j < j1; ++j) {
       const uint8_t* rp = R.res + j * R.ld_res + i;
       unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
@@ -658,7 +661,11 @@ cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t 
   R.skip_if_flag = args.skip_if_flag;
   R.write_c = args.write_c ? 1 : 0;
   const unsigned gx = unsigned((args.m + 255) / 256);
-  const int64_t groups = (args.n + kRecCols - 1) / kRecCols;
+  // up to kRecCols columns per block, fewer while the grid is under ~4 blocks per SM
+  int64_t cpb = int64_t(gx) * args.n / (4 * 148);
+  cpb = cpb < 1 ? 1 : (cpb > kRecCols ? kRecCols : cpb);
+  R.cols_per_block = int(cpb);
+  const int64_t groups = (args.n + cpb - 1) / cpb;
   const unsigned gy = unsigned(groups < 65535 ? groups : 65535);
   if (args.moduli <= 16)
     crt_reconstruct128_kernel<<<dim3(gx, gy), 256, 0, stream>>>(R);

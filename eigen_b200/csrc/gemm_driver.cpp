@@ -276,7 +276,7 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   int pick_cfg = -1, pick_s = 0;
   if (use_picker && picker_predict(m, n, k, 'd', 0.0, 1, &pick_cfg, &pick_s) && auto_method && pick_cfg == 0)
     method = EB2_METHOD_NATIVE;
-  if (method == EB2_METHOD_AUTO) method = EB2_METHOD_EMULATED;
+  if (method == EB2_METHOD_AUTO) method = EB2_METHOD_CRT;
   info.method = method;
 
   auto run_native = [&](bool from_auto) -> int {

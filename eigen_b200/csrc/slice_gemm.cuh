@@ -107,17 +107,40 @@ __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, 
   tn = r / gm;
 }
 
-// Walks the (tile, diagonal, pair, k-block) schedule in issue order.
+// Work items: one per output tile, or in CRT mode one per (tile, modulus): the moduli are
+// independent products, so small outputs still spread over the SMs, and the items in
+// flight at any time share one modulus (its residue planes stay in L2).
+__host__ __device__ __forceinline__ int num_work(const SliceGemmParams& P) {
+  return P.tiles_m * P.tiles_n * (P.crt ? P.slices : 1);
+}
+__device__ __forceinline__ void work_item(const SliceGemmParams& P, int w, int& tile, int& t_hi, int& t_lo) {
+  if (P.crt) {
+    const int nt = P.tiles_m * P.tiles_n;
+    tile = w % nt;
+    t_hi = t_lo = w / nt;
+  } else {
+    tile = w;
+    t_hi = P.diag_hi;
+    t_lo = P.diag_lo;
+  }
+}
+
+// Walks the (work item, diagonal, pair, k-block) schedule in issue order.
 struct BlockIter {
-  int tile, t, f, p_lo, total, stride;
+  int work, tile, t, t_lo, f, p_lo, total, stride;
   bool valid;
-  __device__ __forceinline__ void settle(const SliceGemmParams& P, int num_tiles) {
+  __device__ __forceinline__ void load(const SliceGemmParams& P) {
+    int t_hi;
+    work_item(P, work, tile, t_hi, t_lo);
+    t = t_hi;
+    f = 0;
+  }
+  __device__ __forceinline__ void settle(const SliceGemmParams& P, int nwork) {
     valid = false;
-    while (tile < num_tiles) {
-      if (t < P.diag_lo) {
-        tile += stride;
-        t = P.diag_hi;
-        f = 0;
+    while (work < nwork) {
+      if (t < t_lo) {
+        work += stride;
+        if (work < nwork) load(P);
         continue;
       }
       if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, P.crt != 0) || f >= total) {
@@ -129,16 +152,15 @@ struct BlockIter {
       return;
     }
   }
-  __device__ __forceinline__ void start(const SliceGemmParams& P, int num_tiles, int first, int step) {
-    tile = first;
+  __device__ __forceinline__ void start(const SliceGemmParams& P, int nwork, int first, int step) {
+    work = first;
     stride = step;
-    t = P.diag_hi;
-    f = 0;
-    settle(P, num_tiles);
+    if (work < nwork) load(P);
+    settle(P, nwork);
   }
-  __device__ __forceinline__ void next(const SliceGemmParams& P, int num_tiles) {
+  __device__ __forceinline__ void next(const SliceGemmParams& P, int nwork) {
     ++f;
-    settle(P, num_tiles);
+    settle(P, nwork);
   }
 };
 
@@ -182,11 +204,11 @@ __device__ __forceinline__ void slice_producer(const CUtensorMap* tmA, const CUt
   using L = SliceLayout<BN, STAGES, PAIR>;
   constexpr int ke = SliceTraits<MODE, BN, PAIR>::kKElems;  // innermost coordinate step (elements)
   constexpr uint32_t kTx = (PAIR ? 2u : 1u) * uint32_t(L::kABytes + L::kBBytes);
-  const int num_tiles = P.tiles_m * P.tiles_n;
+  const int nwork = num_work(P);
   const int a_row_off = PAIR ? int(rank) * kSliceBM : 0;
   const int b_row_off = PAIR ? int(rank) * L::kBRows : 0;
   BlockIter it;
-  it.start(P, num_tiles, first_tile<PAIR>(), tile_step<PAIR>());
+  it.start(P, nwork, first_tile<PAIR>(), tile_step<PAIR>());
   uint32_t issued = 0;  // stage = issued % STAGES, phase = (issued / STAGES) & 1
   bool ok = true;
   while (it.valid) {
@@ -213,7 +235,7 @@ __device__ __forceinline__ void slice_producer(const CUtensorMap* tmA, const CUt
       tma_load_3d(smem + L::kBOff + stage * L::kBBytes, tmB, &full[stage], kb * ke, b_row, b_slice(it.t, p, P.crt != 0));
     }
     ++issued;
-    it.next(P, num_tiles);
+    it.next(P, nwork);
   }
   if (!ok && !PAIR) {
     // let the copies still in flight land before the CTA can exit (bounded); a pair's
@@ -245,18 +267,20 @@ __device__ __forceinline__ void slice_mma(uint8_t* smem, uint64_t* full, uint64_
   using L = SliceLayout<BN, STAGES, PAIR>;
   constexpr uint32_t idesc = SliceTraits<MODE, BN, PAIR>::kIdesc;
   constexpr bool kTileUnit = (MODE == kModeSplitBF16);
-  const int num_tiles = P.tiles_m * P.tiles_n;
+  const int nwork = num_work(P);
   uint32_t consumed = 0;  // stage = consumed % STAGES, phase = (consumed / STAGES) & 1
   int buf = 0;
   uint32_t tphase = 0u;  // bit b: phase of accumulator buffer b
   bool ok = true;
-  for (int tile = first_tile<PAIR>(); tile < num_tiles && ok; tile += tile_step<PAIR>()) {
+  for (int w = first_tile<PAIR>(); w < nwork && ok; w += tile_step<PAIR>()) {
+    int tile, t_hi, t_lo;
+    work_item(P, w, tile, t_hi, t_lo);
     bool fresh = true;  // the next MMA overwrites the accumulator
     if (kTileUnit) {
       if (!mbar_wait(&tempty[buf], ((tphase >> buf) & 1u) ^ 1u, abort_flag, P.status)) break;
       tc_fence_after();
     }
-    for (int t = P.diag_hi; t >= P.diag_lo && ok; --t) {
+    for (int t = t_hi; t >= t_lo && ok; --t) {
       int p_lo, total;
       if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, MODE == kModeCrtI8)) continue;
       constexpr int kUnit = SliceTraits<MODE, BN, PAIR>::kUnitKb;
@@ -453,19 +477,20 @@ __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull
   const int quad = warp & 3;
   const int col_base = ((warp - 2) >> 2) * kCols;
   const int row = quad * 32 + lane;
-  const int num_tiles = P.tiles_m * P.tiles_n;
+  const int nwork = num_work(P);
   const int row_base = PAIR ? int(cluster_ctarank()) * kSliceBM : 0;
   const int64_t plane = P.ld_res * int64_t(P.tiles_n) * BN;
   int buf = 0;
   uint32_t ephase = 0u;
   bool ok = true;
-  for (int tile = first_tile<PAIR>(); tile < num_tiles && ok; tile += tile_step<PAIR>()) {
-    int tm, tn;
+  for (int w = first_tile<PAIR>(); w < nwork && ok; w += tile_step<PAIR>()) {
+    int tile, t_hi, t_lo, tm, tn;
+    work_item(P, w, tile, t_hi, t_lo);
     tile_coords(tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
     const int64_t m0 = int64_t(tm) * (PAIR ? 2 * kSliceBM : kSliceBM) + row_base;
     const int64_t n0 = int64_t(tn) * BN + col_base;
     const int64_t grow = m0 + row;
-    for (int t = P.diag_hi; t >= P.diag_lo && ok; --t) {
+    for (int t = t_hi; t >= t_lo && ok; --t) {
       int p_lo, total;
       if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, true)) continue;
       const uint32_t pm = uint32_t(crt_modulus(t));
@@ -649,7 +674,7 @@ inline cudaError_t launch_slice_gemm(const CUtensorMap& tmA, const CUtensorMap& 
   auto kern = slice_gemm_kernel<MODE, BN, STAGES, NW, PAIR>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kAlloc);
   if (e != cudaSuccess) return e;
-  const int tiles = P.tiles_m * P.tiles_n;
+  const int tiles = num_work(P);
   const int ctas = PAIR ? 2 * (tiles < num_sms / 2 ? tiles : num_sms / 2) : (tiles < num_sms ? tiles : num_sms);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(unsigned(ctas), 1, 1);
