@@ -7,6 +7,7 @@
 // here "blocking" is the tcgen05 tile width and the number of digit slices.
 #include "gemm_driver.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -90,9 +91,14 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   const bool check = opt.check_accuracy;
   const int forced = opt.moduli ? opt.moduli : settings().dgemm_moduli.load();
   int nmod = forced ? forced : kCrtDefaultModuli;
-  const int nmax = check ? std::max(nmod, kCrtMaxModuli) : nmod;
-  const int tile = (opt.tile_n == kTilePair || opt.tile_n == 256) ? opt.tile_n : choose_crt_tile(cx, m, n);
-  const int64_t m_pad = round_up(m, crt_tile_rows(tile)), n_pad = round_up(n, crt_tile_cols(tile)),
+  const bool auto_tile = opt.tile_n != kTilePair && opt.tile_n != 256 && settings().tile_n.load() == 0;
+  // Stage 2 of the learned picker: tile configuration and modulus count, once the scan
+  // has measured the inputs' exponent spread.
+  const bool stage2 = picker_weights() != nullptr && (auto_tile || forced == 0);
+  const int nmax = (check || stage2) ? std::max(nmod, kCrtMaxModuli) : nmod;
+  int tile = (opt.tile_n == kTilePair || opt.tile_n == 256) ? opt.tile_n : choose_crt_tile(cx, m, n);
+  // rows padded for the pair tile whenever the picker may still choose it
+  const int64_t m_pad = round_up(m, stage2 ? 256 : crt_tile_rows(tile)), n_pad = round_up(n, crt_tile_cols(tile)),
                 k_pad = round_up(k, kOzakiKBlock);
   size_t off = 0;
   const size_t o_mb_a = off;
@@ -140,6 +146,19 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   ok = ok && check_cuda(launch_crt_norms(vb, ob, st), "norms B");
   if (!ok) return EB2_ERR_CUDA;
   info.launches = 4;
+  if (stage2) {
+    if (!check_cuda(cudaMemcpyAsync(cx.hflags, df, sizeof(DeviceFlags), cudaMemcpyDeviceToHost, st), "read scan") ||
+        !check_cuda(cudaStreamSynchronize(st), "scan"))
+      return EB2_ERR_CUDA;
+    const double spread = cx.hflags->spread[1] > 0 ? cx.hflags->spread[0] / cx.hflags->spread[1] : 0.0;
+    int cfg = -1, cls = 0;
+    if (picker_predict(m, n, k, 'd', spread, 1, &cfg, &cls)) {
+      // DGEMM configurations: 1 = one CTA per 128 x 256 tile, 2 = CTA pair per 256 x 256 tile;
+      // precision class c -> 8 + 2c moduli
+      if (auto_tile && (cfg == 1 || cfg == 2)) tile = cfg == 1 ? 256 : kTilePair;
+      if (forced == 0) nmod = std::min(kCrtMaxModuli, std::max(8, 8 + 2 * (cls - kMlpSliceBase)));
+    }
+  }
 
   CrtGemmArgs g{};
   g.m = m;
@@ -276,7 +295,13 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   int pick_cfg = -1, pick_s = 0;
   if (use_picker && picker_predict(m, n, k, 'd', 0.0, 1, &pick_cfg, &pick_s) && auto_method && pick_cfg == 0)
     method = EB2_METHOD_NATIVE;
-  if (method == EB2_METHOD_AUTO) method = EB2_METHOD_CRT;
+  if (method == EB2_METHOD_AUTO) {
+    // without picker weights: the CRT emulation where its fixed costs (scans, residues,
+    // reconstruction, about 0.1 ms) and the O(mn + (m+n)k) passes are amortised
+    const double mnk = double(m) * double(n) * double(k);
+    method = (use_picker || (mnk >= 4294967296.0 && k >= 1024 && std::min(m, n) >= 256)) ? EB2_METHOD_CRT
+                                                                                          : EB2_METHOD_NATIVE;
+  }
   info.method = method;
 
   auto run_native = [&](bool from_auto) -> int {

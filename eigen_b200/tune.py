@@ -1,23 +1,26 @@
-"""Autotuner and learned configuration picker for the emulated products.
+"""Autotuner and learned configuration picker for the DGEMM path.
 
 The counterpart of Eigen's blocking-size heuristic
 (Eigen/src/Core/products/GeneralBlockPanelKernel.h:202-452, computeProductBlockingSizes):
 instead of a cache model, an exhaustive autotuner times every kernel configuration on
-random shapes and a small MLP learns to predict the best one, plus the digit-slice count
-the emulated DGEMM needs to meet its accuracy target.
+random shapes and a small MLP learns to predict the best one, plus the number of CRT
+moduli the emulated DGEMM needs to meet its accuracy target.
 
     python -m eigen_b200.tune all [--train 2000] [--holdout 500] [--out eigen_b200/data]
 
-* collect : for each shape (m, n, k log-uniform in [3, 16384]; dtype f64 or f32; entries
-            u*2^e with e in [-r, r], r uniform in 0..32) the slice count the a-posteriori
-            check settles on (f64), then the device time of every configuration
-            (native; emulated 128x128, 128x256, CTA pair) at that slice count.
+* collect : for each shape (m, n, k log-uniform in [3, max-dim]; entries u*2^e with e in
+            [-r, r], r uniform in 0..32) the modulus count the a-posteriori check settles
+            on (starting from 8, two at a time), then the device time of every
+            configuration at that count: native FP64 kernel; CRT emulation with one CTA
+            per 128 x 256 tile; CRT emulation with a CTA pair per 256 x 256 tile.
 * train   : the MLP (eb2_mlp_param_count() weights) is trained on the GPU by the
             library's own CUDA kernels (eb2_mlp_backward / eb2_mlp_adam), full batch,
-            cross-entropy on the best configuration and on the needed slice count.
+            cross-entropy on the best configuration and on the precision class
+            c = (moduli - 8) / 2.
 * evaluate: on held-out shapes, regret of the picked configuration against the
-            exhaustive best, how often the picked slice count meets the target without
-            escalation, and the same call timed with and without the picker.
+            exhaustive best, next to the regret of the library's rule without a picker
+            (native below ~2^32 multiply-adds, else CRT, pair tiles when they fill the
+            SMs, 16 moduli plus escalation).
 Outputs: <out>/tune_db.json, <out>/picker_weights.bin (+ .json metadata), <out>/tune_report.json.
 The library reads picker_weights.bin next to itself (eigen_b200/data) when the GPU matches.
 """
@@ -37,8 +40,9 @@ import numpy as np
 
 import eigen_b200 as eb
 
-CONFIGS = [0, 128, 256, 512]  # 0 = native; tile configurations of the emulated products
-SLICE_BASE, NUM_SLICES = 6, 7
+CONFIGS = [0, 256, 512]  # 0 = native; CRT with one CTA per 128 x 256 tile; CRT with CTA pairs (256 x 256)
+SLICE_BASE, NUM_SLICES = 6, 7  # the picker's precision head: class c -> 8 + 2c moduli
+MODULI_MIN, MODULI_MAX = 8, 20
 PICKER_MAGIC = b"EB2PICK1"
 
 
@@ -47,9 +51,8 @@ def shapes(count, seed, lo=3, hi=16384):
     out = []
     for _ in range(count):
         m, n, k = (int(round(math.exp(rng.uniform(math.log(lo), math.log(hi))))) for _ in range(3))
-        dtype = "d" if rng.random() < 0.6 else "s"
         r = int(rng.integers(0, 33))
-        out.append(dict(m=m, n=n, k=k, dtype=dtype, r=r))
+        out.append(dict(m=m, n=n, k=k, dtype="d", r=r))
     return out
 
 
@@ -93,6 +96,13 @@ def time_call(torch, fn, reps=3):
     return best
 
 
+def _reset():
+    eb.set_dgemm_method(eb.METHOD_AUTO)
+    eb.set_tile_n(0)
+    eb.set_dgemm_moduli(0)
+    eb.set_dgemm_tolerance(2.0 ** -53)
+
+
 def measure_shape(torch, pool, sh, gen, reps=3):
     m, n, k, dt, r = sh["m"], sh["n"], sh["k"], sh["dtype"], sh["r"]
     A, B, C = pool.get(dt)
@@ -101,46 +111,29 @@ def measure_shape(torch, pool, sh, gen, reps=3):
     c = C[: m * n]
     rec = dict(sh, spread=0.0)
     eb.set_picker(None)
-    if dt == "d":
-        # slice count the a-posteriori check settles on for this data
-        eb.set_dgemm_method(eb.METHOD_EMULATED)
-        eb.set_tile_n(128)
-        eb.set_dgemm_slices(SLICE_BASE)
-        eb.set_dgemm_tolerance(2.0 ** -53)
-        rc = eb.dgemm_device("N", "N", m, n, k, 1.0, a, m, b, k, 0.0, c, m, check_accuracy=True)
-        info = eb.last_call_info()
-        rec["spread"] = float(info["spread"])
-        need = info["slices"] if rc == eb.EB2_OK else SLICE_BASE + NUM_SLICES - 1
-        rec["slices"] = int(min(max(need, SLICE_BASE), SLICE_BASE + NUM_SLICES - 1))
-        eb.set_dgemm_slices(rec["slices"])
-        eb.set_dgemm_tolerance(1.0)  # time exactly that many slices
+    # modulus count the a-posteriori check settles on for this data (from 8, two at a time)
+    eb.set_dgemm_method(eb.METHOD_CRT)
+    eb.set_dgemm_moduli(MODULI_MIN)
+    eb.set_dgemm_tolerance(2.0 ** -53)
+    rc = eb.dgemm_device("N", "N", m, n, k, 1.0, a, m, b, k, 0.0, c, m, check_accuracy=True)
+    info = eb.last_call_info()
+    rec["spread"] = float(info["spread"])
+    need = info["slices"] if rc == eb.EB2_OK else MODULI_MAX
+    rec["moduli"] = int(min(max(need, MODULI_MIN), MODULI_MAX))
+    eb.set_dgemm_moduli(rec["moduli"])
+    eb.set_dgemm_tolerance(1.0)  # time exactly that many moduli
     times = {}
     for cfg in CONFIGS:
-        if dt == "d" and cfg == 256:
-            continue  # the Ozaki GEMM has no 128x256 single-CTA tile (256 selects the pair)
         if cfg == 0:
-            if dt == "d":
-                eb.set_dgemm_method(eb.METHOD_NATIVE)
-            else:
-                eb.set_sgemm_method(eb.METHOD_NATIVE)
+            eb.set_dgemm_method(eb.METHOD_NATIVE)
         else:
+            eb.set_dgemm_method(eb.METHOD_CRT)
             eb.set_tile_n(cfg)
-            if dt == "d":
-                eb.set_dgemm_method(eb.METHOD_EMULATED)
-            else:
-                eb.set_sgemm_method(eb.METHOD_EMULATED)
-        if dt == "d":
-            fn = lambda: eb.dgemm_device("N", "N", m, n, k, 1.0, a, m, b, k, 0.0, c, m, check_accuracy=True)
-        else:
-            fn = lambda: eb.sgemm_device("N", "N", m, n, k, 1.0, a, m, b, k, 0.0, c, m)
+        fn = lambda: eb.dgemm_device("N", "N", m, n, k, 1.0, a, m, b, k, 0.0, c, m, check_accuracy=True)
         times[str(cfg)] = time_call(torch, fn, reps)
     rec["times_ms"] = times
     rec["best"] = int(min(times, key=lambda c: times[c]))
-    eb.set_dgemm_method(eb.METHOD_AUTO)
-    eb.set_sgemm_method(eb.METHOD_AUTO)
-    eb.set_tile_n(0)
-    eb.set_dgemm_slices(0)
-    eb.set_dgemm_tolerance(2.0 ** -53)
+    _reset()
     return rec
 
 
@@ -154,9 +147,8 @@ def features(sh, spread=None):
 
 
 def labels(rec):
-    cfg_index = {0: 0, 128: 1, 256: 2, 512: 3}[rec["best"]]
-    sl = rec["slices"] - SLICE_BASE if rec["dtype"] == "d" else -1
-    return cfg_index, sl
+    cfg_index = {0: 0, 256: 1, 512: 2}[rec["best"]]
+    return cfg_index, (rec["moduli"] - MODULI_MIN) // 2
 
 
 def train(torch, db, steps=4000, lr=3e-3, seed=0):
@@ -196,6 +188,8 @@ def train(torch, db, steps=4000, lr=3e-3, seed=0):
 
 
 def predict(w, sh, spread=None):
+    """(configuration, moduli) the library picks with weights w; configuration 3 (the
+    digit-slice scheme) and a native pick are both reported as 0 / native."""
     lib = eb.load()
     x = (ctypes.c_float * 8)(*features(sh, spread))
     lg = (ctypes.c_float * 11)()
@@ -203,8 +197,32 @@ def predict(w, sh, spread=None):
     lib.eb2_picker_forward_host(wa, x, lg)
     lg = list(lg)
     cfg = int(np.argmax(lg[:4]))
-    s = SLICE_BASE + int(np.argmax(lg[4:]))
-    return [0, 128, 256, 512][cfg], s
+    moduli = MODULI_MIN + 2 * int(np.argmax(lg[4:]))
+    return {1: 256, 2: 512}.get(cfg, 0), moduli
+
+
+def default_choice(sh, num_sms):
+    """What the library does without a picker (gemm_driver.cpp): native below ~2^32
+    multiply-adds, thin k or thin m/n; else CRT, CTA pairs when they fill the SMs, 16 moduli."""
+    m, n, k = sh["m"], sh["n"], sh["k"]
+    if not (m * n * k >= 2 ** 32 and k >= 1024 and min(m, n) >= 256):
+        return 0, 16
+    pair_tiles = ((m + 255) // 256) * ((n + 255) // 256)
+    return (512 if 2 * pair_tiles >= num_sms else 256), 16
+
+
+def charged_time(rec, cfg, moduli):
+    """Device time of configuration `cfg` run with `moduli` moduli, from the measured time
+    at the needed count: fewer than needed costs one more full pass per escalation (two
+    moduli each), more than needed scales with the modulus count."""
+    t = rec["times_ms"][str(cfg)]
+    if cfg == 0:
+        return t
+    need = rec["moduli"]
+    if moduli >= need:
+        return t * moduli / need
+    passes = (need - moduli + 1) // 2
+    return t * (1.0 + sum((moduli + 2 * i) / need for i in range(passes)))
 
 
 def device_key(torch):
@@ -224,27 +242,36 @@ def write_weights(path: Path, w: np.ndarray, key: dict):
     path.with_suffix(".json").write_text(json.dumps(meta, indent=1))
 
 
-def evaluate(torch, pool, w, held, gen):
-    rows = []
-    for sh in held:
-        rec = measure_shape(torch, pool, sh, gen, reps=2)
-        cfg, s = predict(w, rec)
-        t_best = rec["times_ms"][str(rec["best"])]
-        key = str(cfg if not (sh["dtype"] == "d" and cfg == 256) else 512)
-        t_pick = rec["times_ms"].get(key, float("nan"))
-        ok_slices = (sh["dtype"] == "s") or (s >= rec["slices"])
-        # a slice count below the need costs an escalation pass: charge the exhaustive
-        # time of the chosen configuration scaled by the extra diagonal's work
-        if sh["dtype"] == "d" and cfg != 0 and s < rec["slices"]:
-            t_pick *= 1.0 + (rec["slices"] - s) * (rec["slices"] + 1) / (rec["slices"] * (rec["slices"] + 1) / 2)
-        rows.append(dict(rec, pick_cfg=cfg, pick_slices=s, regret=t_pick / t_best - 1.0, slices_ok=ok_slices))
-    reg = np.array([r["regret"] for r in rows])
-    return dict(n=len(rows), regret_mean=float(np.nanmean(reg)), regret_p50=float(np.nanmedian(reg)),
-                regret_p95=float(np.nanpercentile(reg, 95)),
-                exact_best=float(np.mean([r["pick_cfg"] == r["best"] or
-                                          (r["dtype"] == "d" and r["pick_cfg"] == 256 and r["best"] == 512)
-                                          for r in rows])),
-                slice_pass_rate=float(np.mean([r["slices_ok"] for r in rows if r["dtype"] == "d"] or [1.0]))), rows
+def compare(rows, w, num_sms):
+    """Regret (time / exhaustive best - 1) of the picker and of the no-picker rule on
+    measured rows; pure host computation on recorded times."""
+    out = []
+    for rec in rows:
+        best = rec["times_ms"][str(rec["best"])]
+        pc, pm = predict(w, rec)
+        dc, dm = default_choice(rec, num_sms)
+        out.append(dict(m=rec["m"], n=rec["n"], k=rec["k"], r=rec["r"], best=rec["best"], moduli=rec["moduli"],
+                        pick_cfg=pc, pick_moduli=pm, default_cfg=dc,
+                        regret_picker=charged_time(rec, pc, pm) / best - 1.0,
+                        regret_default=charged_time(rec, dc, dm) / best - 1.0,
+                        t_best=best, t_picker=charged_time(rec, pc, pm), t_default=charged_time(rec, dc, dm)))
+    rp = np.array([o["regret_picker"] for o in out])
+    rd = np.array([o["regret_default"] for o in out])
+    summary = dict(n=len(out), regret_mean=float(rp.mean()), regret_p50=float(np.median(rp)),
+                   regret_p95=float(np.percentile(rp, 95)), default_regret_mean=float(rd.mean()),
+                   default_regret_p95=float(np.percentile(rd, 95)),
+                   total_ms_best=float(sum(o["t_best"] for o in out)),
+                   total_ms_picker=float(sum(o["t_picker"] for o in out)),
+                   total_ms_default=float(sum(o["t_default"] for o in out)),
+                   exact_best=float(np.mean([o["pick_cfg"] == o["best"] for o in out])),
+                   moduli_pass_rate=float(np.mean([o["pick_moduli"] >= o["moduli"] for o in out])))
+    return summary, out
+
+
+def evaluate(torch, pool, w, held, gen, num_sms):
+    rows = [measure_shape(torch, pool, sh, gen, reps=2) for sh in held]
+    summary, _ = compare(rows, w, num_sms)
+    return summary, rows
 
 
 def main(argv=None):
@@ -277,10 +304,10 @@ def main(argv=None):
     w, hist = train(torch, db, steps=a.steps)
     write_weights(out / "picker_weights.bin", w, key)
     held = shapes(a.holdout, seed=2, hi=md)
-    summary, rows = evaluate(torch, pool, w, held, gen)
-    report = dict(device=key, train=len(db), holdout=len(held), loss_history=hist, **summary,
+    summary, rows = evaluate(torch, pool, w, held, gen, key["sms"])
+    report = dict(device=key, train=len(db), holdout=len(held), max_dim=md, loss_history=hist, **summary,
                   seconds=round(time.time() - t0, 1))
-    (out / "tune_report.json").write_text(json.dumps(dict(report, rows=rows)))
+    (out / "tune_report.json").write_text(json.dumps(dict(report, holdout_rows=rows)))
     print(json.dumps(report))
     return 0
 

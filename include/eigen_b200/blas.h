@@ -194,14 +194,19 @@ int eb2_gemm_each(char dtype, int64_t count, const eb2_gemm_problem* problems, v
  * A 3-layer MLP (8 features -> 64 -> 64 -> 11, ReLU, FP32) that plays the role of Eigen's
  * computeProductBlockingSizes (Eigen/src/Core/products/GeneralBlockPanelKernel.h:202-452):
  * from log2 m, n, k, the dtype, the inputs' exponent spread and the batch size it scores
- * 4 kernel configurations (0 native, 1 emulated 128x128, 2 emulated 128x256, 3 emulated
- * CTA pair 256x256) and 7 digit-slice counts (6..12) of the emulated DGEMM.  Weights are a
- * flat float array of eb2_mlp_param_count() entries:
+ * 4 DGEMM configurations (0 native FP64 kernel, 1 CRT emulation with one CTA per 128x256
+ * tile, 2 CRT emulation with a CTA pair per 256x256 tile, 3 digit-slice emulation) and 7
+ * precision classes c (eb2_picker_predict reports 6 + c; the CRT path uses 8 + 2c moduli).
+ * DGEMM with an automatic method consults it twice: on the shape (native or emulated) and,
+ * once the scan has measured the exponent spread, for the tile and modulus count.  The
+ * library loads eigen_b200/data/picker_weights.bin (trained by python -m eigen_b200.tune)
+ * when its SM count matches the device.  Weights are a flat float array of
+ * eb2_mlp_param_count() entries:
  *   W1[64][8] b1[64] W2[64][64] b2[64] W3[11][64] b3[11]. */
 int eb2_mlp_param_count(void);
-/* Installs the weights the product path consults when method/tile/slices are automatic
+/* Installs the weights the product path consults when method/tile/moduli are automatic
  * (copied; NULL or count 0 removes the picker).  The a-posteriori accuracy check still
- * adds slices when a prediction falls short. */
+ * adds moduli when a prediction falls short. */
 int eb2_picker_set_weights(const float* weights, int count);
 int eb2_picker_features(int64_t m, int64_t n, int64_t k, char dtype, double spread, int64_t batch, float* out8);
 int eb2_picker_forward_host(const float* weights, const float* features8, float* logits11);

@@ -201,3 +201,29 @@ def test_training_kernels_fit_a_separable_problem():
     out = np_forward(dw.cpu().numpy().astype(np.float64), X.astype(np.float64))[2]
     assert np.mean(np.argmax(out[:, :NC], 1) == yc) > 0.95
     assert np.mean(np.argmax(out[:, NC:], 1) == ys) > 0.8
+
+
+# ------------------------------------------------------------------ the trained picker
+DATA = eb.LIB_PATH.parent.parent / "data"
+
+
+def test_trained_picker_beats_the_rule_without_it():
+    """On the held-out shapes the tuner measured on a B200 (recorded device times of every
+    configuration), the committed weights pick configurations whose total time is well
+    below the library's fixed rule, and close to the exhaustive best."""
+    import json
+
+    from eigen_b200 import tune
+
+    rep = json.loads((DATA / "tune_report.json").read_text())
+    raw = (DATA / "picker_weights.bin").read_bytes()
+    assert raw[:8] == b"EB2PICK1"
+    count = int.from_bytes(raw[8:12], "little")
+    w = np.frombuffer(raw[16:16 + 4 * count], dtype="<f4").astype(np.float32)
+    assert count == eb.load().eb2_mlp_param_count()
+    summary, rows = tune.compare(rep["holdout_rows"], w, rep["device"]["sms"])
+    assert summary["n"] >= 400
+    assert summary["total_ms_picker"] < 0.8 * summary["total_ms_default"]
+    assert summary["regret_mean"] < 0.05 < summary["default_regret_mean"]
+    assert summary["total_ms_picker"] < 1.05 * summary["total_ms_best"]
+    assert summary["moduli_pass_rate"] >= 0.98
