@@ -1,19 +1,20 @@
 #!/usr/bin/env python
-"""FP64-accurate GEMM throughput on B200: emulated DGEMM (Ozaki INT8 slices on tcgen05)
-next to the native FP64 DMMA kernel, at M = N = K = 8192.
+"""FP64-accurate GEMM throughput on B200: the emulated DGEMM (Ozaki scheme II: INT8
+residue products modulo 16 coprime moduli on tcgen05, exact CRT reconstruction) next to
+the native FP64 DMMA kernel, at M = N = K = 8192.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--r R]
 
 One step = one C = A*B product (NN, column-major, alpha = 1, beta = 0) of 8192^3 with
 entries u*2^e, u ~ U[-1,1], e ~ U{-r..r} (r = 0 by default), through the library's
 public entry points:
-  * value: eb2_dgemm_device on device-resident inputs (the product path with its
+  * value: eb2_dgemm_device on device-resident inputs (automatic method, with the
     a-posteriori accuracy check), device time from CUDA events on the launching stream,
     max over ranks;
   * e2e:   dgemm_ (the Fortran BLAS ABI Eigen binds) on pinned host buffers: the H2D copy
     of A and B, the product and the D2H copy of C are inside the timed region;
   * roofline: the main tcgen05 GEMM kernel, timed by CUDA events recorded around it on
-    its own stream;
+    its own stream; its DRAM traffic comes from the committed ncu summary;
   * cpu_baseline: Eigen's own multithreaded CPU GEMM (operator*, OpenMP) built from the
     reference sources (oracle/_ref), on a bounded sample, rank 0 only.
 Multi-GPU: replicas only (every rank computes its own product; no collective on the data
@@ -185,8 +186,8 @@ def peaks():
 
 def profiled_traffic(size: int):
     """DRAM bytes per launch of the main GEMM kernel from the committed ncu summary
-    (profiles/ozaki_gemm_i8.md: 'dram_bytes_per_launch: <bytes> at <size>')."""
-    f = ROOT / "profiles" / "ozaki_gemm_i8.md"
+    (profiles/crt_gemm_i8_8192.md: 'dram_bytes_per_launch: <bytes> at <size>')."""
+    f = ROOT / "profiles" / "crt_gemm_i8_8192.md"
     try:
         m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)\s*at\s*(\d+)", f.read_text())
     except OSError:
@@ -194,7 +195,7 @@ def profiled_traffic(size: int):
     if not m:
         return None
     b, at = float(m.group(1)), int(m.group(2))
-    return b * (size / at) ** 3 if at != size else b
+    return b if at == size else None
 
 
 # ------------------------------------------------------------------------ grouped batch
@@ -436,26 +437,31 @@ def our_arm(a, world, rank, local):
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": err}
 
     bf16, bf16_sus, hbm, basis = peaks()
-    products = slices * (slices + 1) // 2
+    method = infos[-1]["method"]
+    tile = infos[-1]["tile_n"]
+    # INT8 products of 2*M*N*K each: one per modulus (CRT) or one per digit pair (slices)
+    products = slices if method == eb.METHOD_CRT else slices * (slices + 1) // 2
     roof = None
-    if gemm_ms_avg:
+    if gemm_ms_avg and method != eb.METHOD_NATIVE:
         achieved = flops / (gemm_ms_avg * 1e-3) / 1e12  # FP64-equivalent TFLOP/s of the GEMM kernel
         int8_peak = 2.0 * bf16  # dense int8 rate is twice the dense bf16 rate on sm_100
         peak = int8_peak / products  # the FP64-equivalent ceiling of an int8 kernel doing `products` GEMMs
+        shape = "CTA pair, 256x256 tiles, cta_group::2" if tile == 512 else "one CTA, 128x256 tiles"
+        kname = "slice_gemm_kernel<CRT>" if method == eb.METHOD_CRT else "slice_gemm_kernel<Ozaki>"
         roof = {"bound": "tensor", "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": UNIT,
                 "frac": round(achieved / peak, 4), "traffic": profiled_traffic(S),
-                "kernel": f"ozaki_gemm_kernel<256,4> (tcgen05.mma kind::i8), {gemm_ms_avg:.3f} ms/launch",
+                "kernel": f"{kname} (tcgen05.mma kind::i8, {shape}), {gemm_ms_avg:.3f} ms/launch",
                 "pipe": {"achieved_tops": round(achieved * products, 1), "peak_tops": round(int8_peak, 1),
                          "basis": f"peak = 2 x {basis} dense bf16 ({bf16} TFLOP/s burst), of {basis}; "
-                                  f"{products} int8 slice products of 2*M*N*K each"}}
+                                  f"{products} int8 products of 2*M*N*K each"}}
 
     value = world * flops / (ms_emu_max * 1e-3) / 1e12
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(ms_emu_max, 3), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int8 slices (s32 accumulate) -> f64", "data": "synthetic",
-            "config": dict(workload_config(a), slices=slices, tile_n=infos[-1]["tile_n"],
+            "vs_baseline": None, "dtype": "int8 residues (s32 accumulate) -> f64", "data": "synthetic",
+            "config": dict(workload_config(a), method=method, moduli_or_slices=slices, tile_n=infos[-1]["tile_n"],
                            err_estimate=infos[-1]["err_estimate"], escalations=infos[-1]["escalations"]),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "native_fp64": native, "grouped_batch": grouped,
