@@ -327,6 +327,70 @@ __global__ void __launch_bounds__(kSplitThreadsCrt) crt_split_kernel(
   }
 }
 
+// CRT constants for every modulus count, computed at compile time (192-bit arithmetic in
+// 32-bit limbs) and placed in constant memory: the reconstruction reads W_l, P and P/2 as
+// immediate constant-bank operands, with no per-device set-up.
+struct CrtTable {
+  uint32_t W[kCrtMaxModuli + 1][kCrtMaxModuli][kCrtLimbs];
+  uint32_t P[kCrtMaxModuli + 1][kCrtLimbs];
+  uint32_t half[kCrtMaxModuli + 1][kCrtLimbs];
+};
+
+__host__ __device__ constexpr void ct_mul_small(uint32_t (&a)[kCrtLimbs], uint32_t s) {
+  uint64_t carry = 0;
+  for (int i = 0; i < kCrtLimbs; ++i) {
+    const uint64_t v = uint64_t(a[i]) * s + carry;
+    a[i] = uint32_t(v);
+    carry = v >> 32;
+  }
+}
+__host__ __device__ constexpr uint32_t ct_div_small(uint32_t (&a)[kCrtLimbs], uint32_t s) {
+  uint64_t rem = 0;
+  for (int i = kCrtLimbs - 1; i >= 0; --i) {
+    const uint64_t cur = (rem << 32) | a[i];
+    a[i] = uint32_t(cur / s);
+    rem = cur % s;
+  }
+  return uint32_t(rem);
+}
+__host__ __device__ constexpr uint32_t ct_inverse_mod(uint32_t a, uint32_t p) {
+  int64_t t = 0, nt = 1, r = p, nr = a % p;
+  while (nr) {
+    const int64_t q = r / nr;
+    const int64_t t2 = t - q * nt;
+    t = nt;
+    nt = t2;
+    const int64_t r2 = r - q * nr;
+    r = nr;
+    nr = r2;
+  }
+  return uint32_t(t < 0 ? t + p : t);
+}
+__host__ __device__ constexpr CrtTable make_crt_table() {
+  CrtTable t{};
+  for (int n = 1; n <= kCrtMaxModuli; ++n) {
+    uint32_t P[kCrtLimbs] = {1, 0, 0, 0, 0, 0};
+    for (int l = 0; l < n; ++l) ct_mul_small(P, uint32_t(crt_modulus(l)));
+    for (int l = 0; l < n; ++l) {
+      const uint32_t p = uint32_t(crt_modulus(l));
+      uint32_t M[kCrtLimbs] = {P[0], P[1], P[2], P[3], P[4], P[5]};
+      (void)ct_div_small(M, p);
+      uint32_t Mm[kCrtLimbs] = {M[0], M[1], M[2], M[3], M[4], M[5]};
+      const uint32_t m_mod = ct_div_small(Mm, p);
+      ct_mul_small(M, ct_inverse_mod(m_mod, p));
+      for (int i = 0; i < kCrtLimbs; ++i) t.W[n][l][i] = M[i];
+    }
+    uint32_t H[kCrtLimbs] = {P[0], P[1], P[2], P[3], P[4], P[5]};
+    (void)ct_div_small(H, 2);
+    for (int i = 0; i < kCrtLimbs; ++i) {
+      t.P[n][i] = P[i];
+      t.half[n][i] = H[i];
+    }
+  }
+  return t;
+}
+__constant__ CrtTable kCrtTable = make_crt_table();
+
 struct CrtRecParams {
   uint32_t W[kCrtMaxModuli][kCrtLimbs];
   uint32_t P[kCrtLimbs];
@@ -375,21 +439,41 @@ __device__ __forceinline__ double scale_exp(double d, int e) {
   return scale2(d, e);
 }
 
+// The fields the per-entry store needs, copied into registers at kernel entry: reading them
+// through a reference to the __grid_constant__ parameter block would cost a load from
+// parameter space per entry.
+struct CrtStoreCtx {
+  double alpha, beta;
+  double* C;
+  int64_t ldc;
+  const int32_t* mu_a;
+  const int32_t* mu_b;
+  int b;
+  bool write_c, estimate;
+};
+
+__device__ __forceinline__ CrtStoreCtx store_ctx(const CrtRecParams& R) {
+  return CrtStoreCtx{R.alpha, R.beta, R.C, R.ldc, R.mu_a, R.mu_b, R.b, R.write_c != 0, R.err_sq != nullptr};
+}
+
 // C_ij from RN(C'_ij) = d 2^shift (signed d): scale by 2^-(mu_i + nu_j), apply alpha and
 // beta, and add the estimate terms: e += 2^(2(b - mu_i - nu_j)) (the squared truncation
 // error bound, up to the factor 2/3 alpha^2 applied per block), v += (alpha C')^2.
-__device__ __forceinline__ void crt_store(const CrtRecParams& R, int64_t i, int64_t j, double d, int shift,
+__device__ __forceinline__ void crt_store(const CrtStoreCtx& S, int64_t i, int64_t j, double d, int shift,
                                           double& e_acc, double& v_acc) {
-  const int mu_i = R.mu_a[i], nu_j = R.mu_b[j];
+  const int mu_i = S.mu_a[i], nu_j = S.mu_b[j];
   const double val = d != 0.0 ? scale_exp(d, shift - mu_i - nu_j) : 0.0;  // d = 0 in zero rows
-  const double v = __dmul_rn(R.alpha, val);
-  if (R.write_c) {
-    double* c = R.C + j * R.ldc + i;
-    *c = R.beta == 0.0 ? v : __fma_rn(R.beta, *c, v);
+  const double v = __dmul_rn(S.alpha, val);
+  if (S.write_c) {
+    double* c = S.C + j * S.ldc + i;
+    if (S.beta == 0.0)
+      *c = v;
+    else
+      *c = __fma_rn(S.beta, *c, v);
   }
-  if (R.err_sq) {
+  if (S.estimate) {
     // truncation errors need a nonzero row on both sides
-    if (mu_i != kCrtZeroRow && nu_j != kCrtZeroRow) e_acc += exp2_int(2 * (R.b - mu_i - nu_j));
+    if (mu_i != kCrtZeroRow && nu_j != kCrtZeroRow) e_acc += exp2_int(2 * (S.b - mu_i - nu_j));
     v_acc += v * v;
   }
 }
@@ -425,6 +509,7 @@ constexpr int kRecCols = 8;  // most columns per block and pass
 // One thread per row i, cols_per_block columns per pass: C'_ij from its residues, then C_ij.
 __global__ void __launch_bounds__(256) crt_reconstruct_kernel(const __grid_constant__ CrtRecParams R) {
   if (R.skip_if_flag && *R.skip_if_flag) return;
+  const CrtStoreCtx sc = store_ctx(R);
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double e_acc = 0.0, v_acc = 0.0;
   // blockIdx.y walks groups of cols_per_block columns
@@ -499,43 +584,59 @@ __global__ void __launch_bounds__(256) crt_reconstruct_kernel(const __grid_const
       }
       int shift;
       double d = limbs_to_double(s, shift);
-      crt_store(R, i, j, negative ? -d : d, shift, e_acc, v_acc);
+      crt_store(sc, i, j, negative ? -d : d, shift, e_acc, v_acc);
     }
   }
   if (R.err_sq) crt_reduce_energies(R, e_acc, v_acc);
 }
 
-// The same for at most 16 moduli: P < 2^126, so W_l fits four limbs, S = sum r_l W_l is
-// known modulo 2^128, and R = S - q P (|R| < 1.5 P < 2^127) is exact in 128-bit two's
-// complement.  Bit for bit the result of the kernel above (both round C' once).
+// The same for N <= 16 moduli, N a template parameter: P < 2^126, so W_l fits four limbs,
+// S = sum r_l W_l is known modulo 2^128, and R = S - q P (|R| < 1.5 P < 2^127) is exact in
+// 128-bit two's complement.  W_l, P and P/2 come from the compile-time table.  Bit for bit
+// the result of the kernel above (both round C' once).
+template <int N, bool EST>
 __global__ void __launch_bounds__(256) crt_reconstruct128_kernel(const __grid_constant__ CrtRecParams R) {
+  static_assert(N >= 1 && N <= 16, "128-bit path");
   using u128 = unsigned __int128;
   using s128 = __int128;
   if (R.skip_if_flag && *R.skip_if_flag) return;
+  CrtStoreCtx sc = store_ctx(R);
+  sc.estimate = EST;  // compiled separately with and without the estimate
+  const uint8_t* const res = R.res;
+  const int64_t ld_res = R.ld_res, plane = R.plane, m = R.m, ncols = R.ncols;
+  const double P_inv = R.P_inv;
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double e_acc = 0.0, v_acc = 0.0;
-  const u128 P = (u128(R.P[3]) << 96) | (u128(R.P[2]) << 64) | (u128(R.P[1]) << 32) | u128(R.P[0]);
+  const u128 P = (u128(kCrtTable.P[N][3]) << 96) | (u128(kCrtTable.P[N][2]) << 64) | (u128(kCrtTable.P[N][1]) << 32) |
+                 u128(kCrtTable.P[N][0]);
   const s128 half = s128(P >> 1);
   const int cpb = R.cols_per_block;
   const int64_t jstep = int64_t(gridDim.y) * cpb;
-  for (int64_t j0 = int64_t(blockIdx.y) * cpb; i < R.m && j0 < R.ncols; j0 += jstep) {
-    const int64_t j1 = j0 + cpb < R.ncols ? j0 + cpb : R.ncols;
+  for (int64_t j0 = int64_t(blockIdx.y) * cpb; i < m && j0 < ncols; j0 += jstep) {
+    const int64_t j1 = j0 + cpb < ncols ? j0 + cpb : ncols;
+    // software pipeline: the residues of column j+1 are loaded while column j is reduced
+    uint32_t rn[N];
+#pragma unroll
+    for (int l = 0; l < N; ++l) rn[l] = res[j0 * ld_res + i + l * plane];
     for (int64_t j = j0; j < j1; ++j) {
-      const uint8_t* rp = R.res + j * R.ld_res + i;
+      uint32_t rc[N];
+#pragma unroll
+      for (int l = 0; l < N; ++l) rc[l] = rn[l];
+      if (j + 1 < j1) {
+#pragma unroll
+        for (int l = 0; l < N; ++l) rn[l] = res[(j + 1) * ld_res + i + l * plane];
+      }
       unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
 #pragma unroll
-      for (int l = 0; l < 16; ++l) {
-        if (l < R.n) {
-          const uint32_t r = rp[int64_t(l) * R.plane];
+      for (int l = 0; l < N; ++l) {
 #pragma unroll
-          for (int q = 0; q < 4; ++q) acc[q] += static_cast<unsigned long long>(r) * R.W[l][q];
-        }
+        for (int q = 0; q < 4; ++q) acc[q] += static_cast<unsigned long long>(rc[l]) * kCrtTable.W[N][l][q];
       }
       // q = rint(S / P) from the partial sums in FP64; it may be off by one near a
       // half-integer, which the range fix below absorbs
       const double sd =
           fma(double(acc[3]), 0x1p96, fma(double(acc[2]), 0x1p64, fma(double(acc[1]), 0x1p32, double(acc[0]))));
-      const u128 q = u128(static_cast<unsigned long long>(rint(sd * R.P_inv)));
+      const u128 q = u128(static_cast<unsigned long long>(rint(sd * P_inv)));
       const u128 S = u128(acc[0]) + (u128(acc[1]) << 32) + (u128(acc[2]) << 64) + (u128(acc[3]) << 96);
       s128 r = s128(S - q * P);
       if (r > half)
@@ -557,10 +658,18 @@ __global__ void __launch_bounds__(256) crt_reconstruct128_kernel(const __grid_co
         d = __ull2double_rn(u | sticky);
         shift = 64 - lz;
       }
-      crt_store(R, i, j, negative ? -d : d, shift, e_acc, v_acc);
+      crt_store(sc, i, j, negative ? -d : d, shift, e_acc, v_acc);
     }
   }
-  if (R.err_sq) crt_reduce_energies(R, e_acc, v_acc);
+  if (EST) crt_reduce_energies(R, e_acc, v_acc);
+}
+
+template <int N>
+void launch_rec128(bool est, dim3 grid, cudaStream_t stream, const CrtRecParams& R) {
+  if (est)
+    crt_reconstruct128_kernel<N, true><<<grid, 256, 0, stream>>>(R);
+  else
+    crt_reconstruct128_kernel<N, false><<<grid, 256, 0, stream>>>(R);
 }
 
 template <int BN, int STAGES, bool PAIR>
@@ -667,10 +776,20 @@ cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t 
   R.cols_per_block = int(cpb);
   const int64_t groups = (args.n + cpb - 1) / cpb;
   const unsigned gy = unsigned(groups < 65535 ? groups : 65535);
-  if (args.moduli <= 16)
-    crt_reconstruct128_kernel<<<dim3(gx, gy), 256, 0, stream>>>(R);
-  else
-    crt_reconstruct_kernel<<<dim3(gx, gy), 256, 0, stream>>>(R);
+  const dim3 grid(gx, gy);
+  const bool est = args.err_sq != nullptr;
+  switch (args.moduli) {
+    case 8: launch_rec128<8>(est, grid, stream, R); break;
+    case 9: launch_rec128<9>(est, grid, stream, R); break;
+    case 10: launch_rec128<10>(est, grid, stream, R); break;
+    case 11: launch_rec128<11>(est, grid, stream, R); break;
+    case 12: launch_rec128<12>(est, grid, stream, R); break;
+    case 13: launch_rec128<13>(est, grid, stream, R); break;
+    case 14: launch_rec128<14>(est, grid, stream, R); break;
+    case 15: launch_rec128<15>(est, grid, stream, R); break;
+    case 16: launch_rec128<16>(est, grid, stream, R); break;
+    default: crt_reconstruct_kernel<<<grid, 256, 0, stream>>>(R); break;  // other counts: 192-bit path
+  }
   return cudaGetLastError();
 }
 
