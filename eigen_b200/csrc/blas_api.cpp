@@ -125,6 +125,18 @@ void blas_gemm(char transa, char transb, int64_t m, int64_t n, int64_t k, T alph
   const bool a_dev = !need_ab || device_usable(a);
   const bool b_dev = !need_ab || device_usable(b);
   const bool c_dev = device_usable(c);
+  if constexpr (sizeof(T) == 8) {
+    // all three in host memory: copies overlapped with the product, block by block
+    if (need_ab && !a_dev && !b_dev && !c_dev &&
+        crt_pipeline_applies(*cx, m, n, k, resolve_dgemm_method(m, n, k))) {
+      const int rc = dgemm_crt_pipelined(*cx, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, ci);
+      if (rc != EB2_OK && rc != EB2_ERR_ACCURACY) {
+        std::fprintf(stderr, "eigen_b200: %s\n", eb2_last_error_string());
+        (void)cudaDeviceSynchronize();
+      }
+      return;
+    }
+  }
   const T* da = a;
   const T* db = b;
   T* dc = c;

@@ -120,6 +120,15 @@ Context* current_context() {
   ok = ok && cudaEventCreate(&c->ev_gemm1) == cudaSuccess;
   ok = ok && cudaMalloc(&c->dflags, sizeof(DeviceFlags)) == cudaSuccess;
   ok = ok && cudaHostAlloc(&c->hflags, sizeof(DeviceFlags), cudaHostAllocDefault) == cudaSuccess;
+  ok = ok && cudaStreamCreateWithFlags(&c->copy_in, cudaStreamNonBlocking) == cudaSuccess;
+  ok = ok && cudaStreamCreateWithFlags(&c->copy_out, cudaStreamNonBlocking) == cudaSuccess;
+  ok = ok && cudaEventCreateWithFlags(&c->ev_a, cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; i < Context::kPipeChunks && ok; ++i) {
+    ok = cudaEventCreateWithFlags(&c->ev_in[i], cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&c->ev_done[i], cudaEventDisableTiming) == cudaSuccess;
+  }
+  ok = ok && cudaHostAlloc(&c->hchunk, sizeof(double) * 2 * Context::kPipeChunks, cudaHostAllocDefault) ==
+                 cudaSuccess;
   if (!ok) {
     set_error(EB2_ERR_CUDA, "creating the device context failed: %s", cudaGetErrorString(cudaGetLastError()));
     delete c;  // the few handles that were created are reclaimed at process exit

@@ -41,6 +41,14 @@ struct Context {
   DeviceBuffer stage_a, stage_b, stage_c;  // device copies of host operands
   DeviceFlags* dflags = nullptr;  // device
   DeviceFlags* hflags = nullptr;  // pinned host mirror
+  // Host-buffer pipeline of the BLAS entry (copies overlapped with the product by column
+  // blocks): one stream per copy direction, events without timing, pinned estimate slots.
+  static constexpr int kPipeChunks = 16;
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  cudaEvent_t ev_a = nullptr;
+  cudaEvent_t ev_in[kPipeChunks] = {};
+  cudaEvent_t ev_done[kPipeChunks] = {};
+  double* hchunk = nullptr;  // pinned [kPipeChunks][2]: per-block error-estimate energies
 };
 
 // Context of the calling thread's current device, created on first use.

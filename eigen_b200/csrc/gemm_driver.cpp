@@ -70,6 +70,22 @@ int choose_slices(int64_t m, int64_t n, int64_t k) {
   return 8;
 }
 
+int auto_method_rule(int64_t m, int64_t n, int64_t k) {
+  // without picker weights: the CRT emulation where its fixed costs (scans, residues,
+  // reconstruction, about 0.1 ms) and the O(mn + (m+n)k) passes are amortised
+  const double mnk = double(m) * double(n) * double(k);
+  return (mnk >= 4294967296.0 && k >= 1024 && std::min(m, n) >= 256) ? EB2_METHOD_CRT : EB2_METHOD_NATIVE;
+}
+
+int resolve_dgemm_method(int64_t m, int64_t n, int64_t k) {
+  const int method = settings().dgemm_method.load();
+  if (method != EB2_METHOD_AUTO) return method;
+  int cfg = -1, cls = 0;
+  if (picker_weights() != nullptr && picker_predict(m, n, k, 'd', 0.0, 1, &cfg, &cls))
+    return cfg == 0 ? EB2_METHOD_NATIVE : EB2_METHOD_CRT;
+  return auto_method_rule(m, n, k);
+}
+
 int choose_crt_tile(const Context& cx, int64_t m, int64_t n) {
   const int forced = settings().tile_n.load();
   if (forced == kTilePair) return kTilePair;
@@ -295,13 +311,7 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   int pick_cfg = -1, pick_s = 0;
   if (use_picker && picker_predict(m, n, k, 'd', 0.0, 1, &pick_cfg, &pick_s) && auto_method && pick_cfg == 0)
     method = EB2_METHOD_NATIVE;
-  if (method == EB2_METHOD_AUTO) {
-    // without picker weights: the CRT emulation where its fixed costs (scans, residues,
-    // reconstruction, about 0.1 ms) and the O(mn + (m+n)k) passes are amortised
-    const double mnk = double(m) * double(n) * double(k);
-    method = (use_picker || (mnk >= 4294967296.0 && k >= 1024 && std::min(m, n) >= 256)) ? EB2_METHOD_CRT
-                                                                                          : EB2_METHOD_NATIVE;
-  }
+  if (method == EB2_METHOD_AUTO) method = use_picker ? EB2_METHOD_CRT : auto_method_rule(m, n, k);
   info.method = method;
 
   auto run_native = [&](bool from_auto) -> int {

@@ -30,6 +30,17 @@ struct SgemmOptions {
 int choose_tile_n(const Context& cx, int64_t m, int64_t n, bool ozaki);
 int choose_slices(int64_t m, int64_t n, int64_t k);
 int choose_crt_tile(const Context& cx, int64_t m, int64_t n);
+// DGEMM method without a per-call override: the settings, else the learned picker on the
+// shape, else the size rule (auto_method_rule).
+int resolve_dgemm_method(int64_t m, int64_t n, int64_t k);
+int auto_method_rule(int64_t m, int64_t n, int64_t k);
+
+// The BLAS entry's DGEMM with A, B and C in host memory, as a pipeline of column blocks
+// (copies overlapped with the product).  crt_pipeline_applies() tells whether it is used.
+bool crt_pipeline_applies(const Context& cx, int64_t m, int64_t n, int64_t k, int method);
+int dgemm_crt_pipelined(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
+                        const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
+                        int64_t ldc, eb2_call_info& info);
 
 // C = alpha*op(A)op(B) + beta*C on device pointers.  Returns EB2_*.
 int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
