@@ -267,9 +267,38 @@ __device__ __forceinline__ uint32_t residue_of3(const Chunks21& c, const CrtModC
   return mod_small(c.a0 + c.a1 * k.c21 + c.a2 * k.c42, k.p, k.magic);
 }
 
+// The 8 symmetric residues of one thread's entries for one modulus, packed into 8 bytes.
+template <bool kWide>
+__device__ __forceinline__ void store_residues(const CrtModConst& k, const Chunks21 (&ch)[8], uint32_t neg,
+                                               int8_t* dst) {
+  const int hi = int(k.p >> 1) - ((k.p & 1u) ? 0 : 1);  // largest representative kept as is
+  uint32_t w[2] = {0u, 0u};
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int res = int(kWide ? residue_of(ch[j], k) : residue_of3(ch[j], k));
+    int sres = res > hi ? res - int(k.p) : res;  // symmetric residue of |t|: [-(p/2), (p-1)/2]
+    // of -|t|: its negation (for p = 256, 128 packs to the same byte as -128)
+    if ((neg >> j) & 1u) sres = -sres;
+    w[j >> 2] |= (uint32_t(sres) & 0xFFu) << (8 * (j & 3));
+  }
+  *reinterpret_cast<uint2*>(dst) = make_uint2(w[0], w[1]);
+}
+
+// Moduli L .. NT-1 with their constants as compile-time immediates.
+template <int L, int NT, bool kWide>
+__device__ __forceinline__ void store_residues_static(const Chunks21 (&ch)[8], uint32_t neg, int8_t* dst,
+                                                      size_t plane) {
+  if constexpr (L < NT) {
+    constexpr CrtModConst k = crt_mod_const(L);
+    store_residues<kWide>(k, ch, neg, dst + size_t(L) * plane);
+    store_residues_static<L + 1, NT, kWide>(ch, neg, dst, plane);
+  }
+}
+
 // Residues of A' = trunc(2^mu_r x) for moduli [0, n): plane l at residues + l*rows_pad*k_pad,
 // row r contiguous along k; symmetric int8 representatives.  Blocks of column 0 write mu_r.
-template <bool kWide>  // kWide: |t| may reach 2^63 (more than 16 moduli)
+// NT > 0: the modulus count is NT (constants as immediates); NT = 0: n, read at run time.
+template <bool kWide, int NT>  // kWide: |t| may reach 2^63 (more than 16 moduli)
 __global__ void __launch_bounds__(kSplitThreadsCrt) crt_split_kernel(
     const double* __restrict__ X, int64_t rows, int64_t cols, int64_t sr, int64_t sl,
     const unsigned long long* __restrict__ maxbits, const unsigned long long* __restrict__ sumsq, int b, int n,
@@ -312,18 +341,10 @@ __global__ void __launch_bounds__(kSplitThreadsCrt) crt_split_kernel(
   }
   int8_t* dst = residues + (size_t(r0 + rr)) * size_t(k_pad) + size_t(l0 + cb);
   const size_t plane = size_t(rows_pad) * size_t(k_pad);
-  for (int l = 0; l < n; ++l) {
-    const CrtModConst k = kModConst[l];
-    const int hi = int(k.p >> 1) - ((k.p & 1u) ? 0 : 1);  // largest representative kept as is
-    uint32_t w[2] = {0u, 0u};
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      uint32_t res = kWide ? residue_of(ch[j], k) : residue_of3(ch[j], k);
-      if (((neg >> j) & 1u) && res) res = k.p - res;  // residue of the negative value
-      const int sres = int(res) > hi ? int(res) - int(k.p) : int(res);  // [-(p/2), (p-1)/2]
-      w[j >> 2] |= (uint32_t(sres) & 0xFFu) << (8 * (j & 3));
-    }
-    *reinterpret_cast<uint2*>(dst + size_t(l) * plane) = make_uint2(w[0], w[1]);
+  if constexpr (NT > 0) {
+    store_residues_static<0, NT, kWide>(ch, neg, dst, plane);
+  } else {
+    for (int l = 0; l < n; ++l) store_residues<kWide>(kModConst[l], ch, neg, dst + size_t(l) * plane);
   }
 }
 
@@ -727,12 +748,17 @@ cudaError_t launch_crt_split(const StridedView<double>& x, const CrtOperand& op,
   const unsigned long long* mb = reinterpret_cast<const unsigned long long*>(op.maxbits);
   const unsigned long long* ss = reinterpret_cast<const unsigned long long*>(op.sumsq);
   const int b = crt_bits(moduli);
-  if (b <= 62)
-    crt_split_kernel<false><<<grid, kSplitThreadsCrt, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl, mb, ss, b,
-                                                                  moduli, op.residues, op.mu, op.rows_pad, op.k_pad);
+  if (moduli == kCrtDefaultModuli && b <= 62)
+    crt_split_kernel<false, kCrtDefaultModuli><<<grid, kSplitThreadsCrt, 0, stream>>>(
+        x.ptr, x.rows, x.cols, x.sr, x.sl, mb, ss, b, moduli, op.residues, op.mu, op.rows_pad, op.k_pad);
+  else if (b <= 62)
+    crt_split_kernel<false, 0><<<grid, kSplitThreadsCrt, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl, mb, ss, b,
+                                                                     moduli, op.residues, op.mu, op.rows_pad,
+                                                                     op.k_pad);
   else
-    crt_split_kernel<true><<<grid, kSplitThreadsCrt, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl, mb, ss, b,
-                                                                 moduli, op.residues, op.mu, op.rows_pad, op.k_pad);
+    crt_split_kernel<true, 0><<<grid, kSplitThreadsCrt, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl, mb, ss, b,
+                                                                    moduli, op.residues, op.mu, op.rows_pad,
+                                                                    op.k_pad);
   return cudaGetLastError();
 }
 

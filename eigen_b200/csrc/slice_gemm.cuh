@@ -456,13 +456,12 @@ __device__ __forceinline__ void ozaki_epilogue(uint32_t tmem_base, uint64_t* tfu
   }
 }
 
-// x mod p for a 32-bit x and p <= 256, with m = floor((2^32 - 1) / p): the estimate
-// q = umulhi(x, m) is at most 2 short of floor(x / p).
+// x mod p for a 32-bit x and p <= 256, with m = floor((2^32 - 1) / p): p m >= 2^32 - p, so
+// x/p - x m / 2^32 <= x / 2^32 < 1 and the estimate q = umulhi(x, m) is at most one short
+// of floor(x / p): one conditional subtraction finishes it.
 __device__ __forceinline__ uint32_t mod_small(uint32_t x, uint32_t p, uint32_t m) {
-  uint32_t r = x - __umulhi(x, m) * p;
-  if (r >= p) r -= p;
-  if (r >= p) r -= p;
-  return r;
+  const uint32_t r = x - __umulhi(x, m) * p;
+  return r >= p ? r - p : r;
 }
 
 // CRT: unit t is modulus p_t; every INT32 product entry is reduced to [0, p_t) and stored
