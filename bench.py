@@ -57,6 +57,7 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-native", action="store_true")
     ap.add_argument("--no-grouped", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     a.steps = max(a.steps, 1)
@@ -271,6 +272,72 @@ def grouped_bench(eb, torch, dev, stream, steps, warmup, count=10000, seed=7):
     return res
 
 
+# ------------------------------------------------------------------------ accuracy
+def _exact_block(Ar, Bc):
+    """alpha*A*B on a sampled block, rounded once from the exact sum: every product a*b is
+    split exactly into hi + lo (Dekker), and math.fsum adds them without intermediate error."""
+    import math
+
+    import numpy as np
+
+    split = 134217729.0  # 2^27 + 1
+
+    def halves(x):
+        t = x * split
+        hi = t - (t - x)
+        return hi, x - hi
+
+    out = np.empty((Ar.shape[0], Bc.shape[1]))
+    for i in range(Ar.shape[0]):
+        a = Ar[i][:, None]
+        p = a * Bc
+        ah, al = halves(np.broadcast_to(a, Bc.shape))
+        bh, bl = halves(Bc)
+        e = ((ah * bh - p) + ah * bl + al * bh) + al * bl  # exact error of each product
+        for j in range(Bc.shape[1]):
+            out[i, j] = math.fsum(np.concatenate([p[:, j], e[:, j]]))
+    return out
+
+
+def accuracy_leg(eb, torch, dev, S, r_values, seed=99, sample=24):
+    """Normwise error of the automatic (emulated) and the native DGEMM against an exactly
+    rounded reference on a sampled sub-block, for entries u*2^e with e in [-r, r]."""
+    import numpy as np
+
+    out = {}
+    g = torch.Generator(device=dev)
+    rng = np.random.default_rng(seed)
+    for r in r_values:
+        g.manual_seed(seed + r)
+        A = torch.rand((S, S), dtype=torch.float64, device=dev, generator=g) * 2 - 1
+        B = torch.rand((S, S), dtype=torch.float64, device=dev, generator=g) * 2 - 1
+        if r:
+            A = torch.ldexp(A, torch.randint(-r, r + 1, (S, S), device=dev, generator=g).to(torch.float64))
+            B = torch.ldexp(B, torch.randint(-r, r + 1, (S, S), device=dev, generator=g).to(torch.float64))
+        rows = np.sort(rng.choice(S, sample, replace=False))
+        cols = np.sort(rng.choice(S, sample, replace=False))
+        # column-major: A(i, l) is A_t[l, i]
+        Ar = A[:, rows].T.cpu().numpy().astype(np.float64)
+        Bc = B[cols, :].T.cpu().numpy().astype(np.float64)
+        ref = _exact_block(Ar, Bc)
+        res = {}
+        for name, method in (("emulated", eb.METHOD_AUTO), ("native", eb.METHOD_NATIVE)):
+            eb.set_dgemm_method(method)
+            C = torch.zeros((S, S), dtype=torch.float64, device=dev)
+            rc = eb.dgemm_device("N", "N", S, S, S, 1.0, A, S, B, S, 0.0, C, S, check_accuracy=True)
+            torch.cuda.synchronize()
+            info = eb.last_call_info()
+            got = C[cols][:, rows].T.cpu().numpy()
+            err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+            res[name] = {"rel_error": err, "rc": rc, "method": info["method"], "moduli_or_slices": info["slices"],
+                         "escalations": info["escalations"], "err_estimate": info["err_estimate"]}
+        eb.set_dgemm_method(eb.METHOD_AUTO)
+        res["sample"] = f"{sample}x{sample} block of C, exactly rounded reference"
+        out[f"r{r}"] = res
+        del A, B, C
+    return out
+
+
 # ------------------------------------------------------------------------ arms
 def reference_arm(a, world, rank):
     cfg = workload_config(a)
@@ -421,6 +488,10 @@ def our_arm(a, world, rank, local):
                "ms_per_step": round(t_step * 1e3, 3), "steps": e2e_steps,
                "api": "dgemm_ (Fortran BLAS ABI) on pinned host buffers; synchronous call timed on the host"}
 
+    accuracy = None
+    if not a.no_accuracy:
+        accuracy = accuracy_leg(eb, torch, dev, S, (0, 8, 32))
+
     grouped = None
     if not a.no_grouped:
         grouped = grouped_bench(eb, torch, dev, stream, a.steps, a.warmup)
@@ -464,7 +535,7 @@ def our_arm(a, world, rank, local):
             "config": dict(workload_config(a), method=method, moduli_or_slices=slices, tile_n=infos[-1]["tile_n"],
                            err_estimate=infos[-1]["err_estimate"], escalations=infos[-1]["escalations"]),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk, "native_fp64": native, "grouped_batch": grouped,
+            "clocks": clk, "native_fp64": native, "accuracy": accuracy, "grouped_batch": grouped,
             "emulated_over_native": round(value / native["tflops"], 3) if native else None,
         }
         print(json.dumps(line))
