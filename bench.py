@@ -82,6 +82,23 @@ def dist_setup(a):
     return world, rank, local
 
 
+def max_over_ranks(dist, x: float, world: int, device) -> float:
+    """The slowest rank's time (every rank takes part, in the same order)."""
+    if world == 1:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_tflops(world: int, flops_per_rank: float, ms_max: float) -> float:
+    """Replicas: every rank computes its own product; the job's throughput is all ranks'
+    flops over the slowest rank's time."""
+    return world * flops_per_rank / (ms_max * 1e-3) / 1e12
+
+
 def host_cpu_info():
     model, flags = "unknown", ""
     try:
@@ -410,12 +427,8 @@ def our_arm(a, world, rank, local):
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def rank_max(x: float) -> float:
+        return max_over_ranks(dist, x, world, dev)
 
     def run_device(method, steps):
         eb.set_dgemm_method(method)
@@ -448,10 +461,10 @@ def our_arm(a, world, rank, local):
     time.sleep(0.3)
     ms_emu, infos = run_device(eb.METHOD_AUTO, a.steps)
     clk = clocks.stop()
-    ms_emu_max = max_over_ranks(ms_emu)
+    ms_emu_max = rank_max(ms_emu)
     C_emu = C.clone()
     gemm_ms = [i["gemm_kernel_ms"] for i in infos if i["gemm_kernel_ms"] > 0]
-    gemm_ms_avg = max_over_ranks(sum(gemm_ms) / len(gemm_ms)) if gemm_ms else None
+    gemm_ms_avg = rank_max(sum(gemm_ms) / len(gemm_ms)) if gemm_ms else None
     slices = infos[-1]["slices"]
     launches = sum(i["launches"] for i in infos)
 
@@ -459,9 +472,9 @@ def our_arm(a, world, rank, local):
     if not a.no_native:
         nsteps = min(a.steps, 5)
         ms_nat, _ = run_device(eb.METHOD_NATIVE, nsteps)
-        ms_nat = max_over_ranks(ms_nat)
+        ms_nat = rank_max(ms_nat)
         diff = float(torch.linalg.norm(C_emu - C) / torch.linalg.norm(C))
-        native = {"tflops": round(world * flops / (ms_nat * 1e-3) / 1e12, 3), "ms_per_step": round(ms_nat, 3),
+        native = {"tflops": round(whole_job_tflops(world, flops, ms_nat), 3), "ms_per_step": round(ms_nat, 3),
                   "steps": nsteps, "kernel": "dgemm_dmma (mma.sync f64)", "rel_diff_emulated_vs_native": diff}
         eb.set_dgemm_method(eb.METHOD_AUTO)
 
@@ -482,8 +495,8 @@ def our_arm(a, world, rank, local):
             eb.dgemm("N", "N", S, S, S, 1.0, hA, S, hB, S, 0.0, hC, S)
             times.append(time.perf_counter() - t0)
         barrier()
-        t_step = max_over_ranks(sum(times) / len(times))
-        e2e = {"value": round(world * flops / t_step / 1e12, 3), "unit": UNIT,
+        t_step = rank_max(sum(times) / len(times))
+        e2e = {"value": round(whole_job_tflops(world, flops, t_step * 1e3), 3), "unit": UNIT,
                "h2d_bytes_per_step": 2 * S * S * 8, "d2h_bytes_per_step": S * S * 8,
                "ms_per_step": round(t_step * 1e3, 3), "steps": e2e_steps,
                "api": "dgemm_ (Fortran BLAS ABI) on pinned host buffers; synchronous call timed on the host"}
@@ -529,7 +542,7 @@ def our_arm(a, world, rank, local):
                                   f"of {basis}; {products} int8 products of 2*M*N*K each",
                          "burst_frac": round(achieved * products / (2.0 * bf16), 4)}}
 
-    value = world * flops / (ms_emu_max * 1e-3) / 1e12
+    value = whole_job_tflops(world, flops, ms_emu_max)
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
