@@ -160,13 +160,20 @@ __device__ __forceinline__ double scale2(double x, int e) {
   return __dmul_rn(__dmul_rn(x, exp2_int(e1)), exp2_int(e - e1));
 }
 
-// Deterministic upper bound of sum_l (x_l 2^-e)^2 in units of 2^-32, e the exponent of
-// the row maximum: every nonzero x adds ceil(rn(x'^2) 2^32) + 1, x' = x 2^-e (|x'| < 1);
-// the +1 covers the rounding of x'^2 (and a product that underflows).
-__global__ void __launch_bounds__(256) crt_norm_kernel(const double* __restrict__ X, int64_t rows, int64_t cols,
-                                                       int64_t sr, int64_t sl,
-                                                       const unsigned long long* __restrict__ maxbits,
-                                                       unsigned long long* __restrict__ sumsq) {
+// One read of the operand for everything the scale exponents need.  Per row r and 128-column
+// chunk c (columns 128c .. 128c+127 of op(X)^T's row, i.e. along K):
+//   * the chunk maximum: row maxima (atomicMax), the NaN/Inf flag, and the exponent-spread
+//     statistic of the configuration picker (the first 64 columns of every 512, as the
+//     digit-slice scan computes it);
+//   * e_c, the exponent of the chunk maximum, and the deterministic integer bound
+//     S_c = sum over nonzero x of ceil(rn(x'^2) 2^32) + 1, x' = x 2^-e_c (|x'| < 1); the +1
+//     covers the rounding of x'^2 and a product that underflows.
+// Every (row, chunk) record is written by exactly one thread group.
+__global__ void __launch_bounds__(256) crt_scan_norm_kernel(const double* __restrict__ X, int64_t rows, int64_t cols,
+                                                            int64_t sr, int64_t sl, unsigned long long* maxbits,
+                                                            int32_t* __restrict__ chunk_e,
+                                                            unsigned long long* __restrict__ chunk_s,
+                                                            int64_t nchunks, int* nonfinite, double* spread) {
   __shared__ double tile[kNormRows][kNormCols + 1];
   const int64_t r0 = int64_t(blockIdx.y) * kNormRows;
   const int64_t l0 = int64_t(blockIdx.x) * kNormCols;
@@ -184,14 +191,36 @@ __global__ void __launch_bounds__(256) crt_norm_kernel(const double* __restrict_
     tile[rr][ll] = (r < rows && l < cols) ? X[r * sr + l * sl] : 0.0;
   }
   __syncthreads();
-  // 8 threads per row, 16 columns each; the 8 partial sums meet in a shuffle reduction
+  // 8 threads per row, 16 columns each, reduced with shuffles inside each 8-lane group
   const int rr = threadIdx.x >> 3;
-  const int cb = (threadIdx.x & 7) * 16;
+  const int sub = threadIdx.x & 7;
+  const int cb = sub * 16;
   const int64_t r = r0 + rr;
+  unsigned long long mb = 0;
+  int esum = 0, ecnt = 0;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(fabs(tile[rr][cb + j])));
+    mb = bits > mb ? bits : mb;
+    if (bits && sub < 4) {  // the first 64 columns, for the spread statistic
+      esum += int(bits >> 52);
+      ++ecnt;
+    }
+  }
+  unsigned long long mb64 = sub < 4 ? mb : 0ull;
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) {
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, mb, o);
+    mb = other > mb ? other : mb;
+    const unsigned long long other64 = __shfl_xor_sync(0xffffffffu, mb64, o);
+    mb64 = other64 > mb64 ? other64 : mb64;
+    esum += __shfl_xor_sync(0xffffffffu, esum, o);
+    ecnt += __shfl_xor_sync(0xffffffffu, ecnt, o);
+  }
   unsigned long long s = 0;
-  const unsigned long long mb = r < rows ? maxbits[r] : 0ull;
+  int e = 0;
   if (mb != 0 && mb < kInfBitsCrt) {
-    const int e = frexp_exp(mb);
+    e = frexp_exp(mb);
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const double x = tile[rr][cb + j];
@@ -203,16 +232,57 @@ __global__ void __launch_bounds__(256) crt_norm_kernel(const double* __restrict_
   }
 #pragma unroll
   for (int o = 4; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 7) == 0 && s != 0) atomicAdd(&sumsq[r], s);
+  if (sub == 0 && r < rows) {
+    const int64_t c = int64_t(blockIdx.x);
+    chunk_e[r * nchunks + c] = e;
+    chunk_s[r * nchunks + c] = mb < kInfBitsCrt ? s : 0ull;
+    if (mb >= kInfBitsCrt) *nonfinite = 1;
+    if (mb) atomicMax(&maxbits[r], mb);
+  }
+  if (spread != nullptr && (l0 & 511) == 0) {
+    double chunk_spread = 0.0, chunk_count = 0.0;
+    if (sub == 0 && r < rows && ecnt > 0 && mb64 < kInfBitsCrt) {
+      chunk_spread = double(int(mb64 >> 52)) - double(esum) / double(ecnt);
+      chunk_count = 1.0;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      chunk_spread += __shfl_xor_sync(0xffffffffu, chunk_spread, o);
+      chunk_count += __shfl_xor_sync(0xffffffffu, chunk_count, o);
+    }
+    if ((threadIdx.x & 31) == 0 && chunk_count > 0.0) {
+      atomicAdd(&spread[0], chunk_spread);
+      atomicAdd(&spread[1], chunk_count);
+    }
+  }
 }
 
-// Scale exponent of one row: mu = b - c with 2^c >= ||x|| from the bound above:
-// ||x||^2 <= S 2^(2e-32), S <= 2^L (L = bit length of S-1), so c = e - 16 + ceil(L/2).
-__device__ __forceinline__ int row_mu(unsigned long long mb, unsigned long long S, int b) {
-  if (mb == 0 || mb >= kInfBitsCrt || S == 0) return kCrtZeroRow;
-  const int e = frexp_exp(mb);
-  const int L = S > 1 ? 64 - __clzll(static_cast<long long>(S - 1)) : 0;
-  return b - (e - 16 + (L + 1) / 2);
+// Scale exponent of each row: with e the row maximum's exponent, the chunk bounds fold into
+// S = sum_c ceil(S_c 4^(e_c - e)) (exact shifts), ||x||^2 <= S 2^(2e-32), S <= 2^L (L = bit
+// length of S-1), so 2^c >= ||x|| for c = e - 16 + ceil(L/2) and mu = b - c.
+__global__ void __launch_bounds__(256) crt_mu_kernel(const unsigned long long* __restrict__ maxbits,
+                                                     const int32_t* __restrict__ chunk_e,
+                                                     const unsigned long long* __restrict__ chunk_s, int64_t nchunks,
+                                                     int64_t rows, int64_t rows_pad, int b, int32_t* __restrict__ mu) {
+  const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= rows_pad) return;
+  int m = kCrtZeroRow;
+  const unsigned long long mb = r < rows ? maxbits[r] : 0ull;
+  if (mb != 0 && mb < kInfBitsCrt) {
+    const int e = frexp_exp(mb);
+    unsigned long long S = 0;
+    for (int64_t c = 0; c < nchunks; ++c) {
+      const unsigned long long sc = chunk_s[r * nchunks + c];
+      if (sc == 0) continue;
+      const int sh = 2 * (e - chunk_e[r * nchunks + c]);
+      S += sh >= 64 ? 1ull : ((sc - 1) >> sh) + 1;  // ceil(sc / 2^sh), sc >= 1
+    }
+    if (S != 0) {
+      const int L = S > 1 ? 64 - __clzll(static_cast<long long>(S - 1)) : 0;
+      m = b - (e - 16 + (L + 1) / 2);
+    }
+  }
+  mu[r] = m;
 }
 
 // Per-modulus constants: p, floor((2^32 - 1) / p) for mod_small, and 2^21, 2^42, 2^63 mod p.
@@ -296,13 +366,12 @@ __device__ __forceinline__ void store_residues_static(const Chunks21 (&ch)[8], u
 }
 
 // Residues of A' = trunc(2^mu_r x) for moduli [0, n): plane l at residues + l*rows_pad*k_pad,
-// row r contiguous along k; symmetric int8 representatives.  Blocks of column 0 write mu_r.
+// row r contiguous along k; symmetric int8 representatives (mu from crt_mu_kernel).
 // NT > 0: the modulus count is NT (constants as immediates); NT = 0: n, read at run time.
 template <bool kWide, int NT>  // kWide: |t| may reach 2^63 (more than 16 moduli)
 __global__ void __launch_bounds__(kSplitThreadsCrt) crt_split_kernel(
     const double* __restrict__ X, int64_t rows, int64_t cols, int64_t sr, int64_t sl,
-    const unsigned long long* __restrict__ maxbits, const unsigned long long* __restrict__ sumsq, int b, int n,
-    int8_t* __restrict__ residues, int32_t* __restrict__ mu, int64_t rows_pad, int64_t k_pad) {
+    const int32_t* __restrict__ mu, int n, int8_t* __restrict__ residues, int64_t rows_pad, int64_t k_pad) {
   __shared__ double tile[kSplitRowsCrt][kSplitColsCrt + 1];
   __shared__ int row_mu_s[kSplitRowsCrt];
   const int64_t r0 = int64_t(blockIdx.y) * kSplitRowsCrt;
@@ -310,9 +379,7 @@ __global__ void __launch_bounds__(kSplitThreadsCrt) crt_split_kernel(
   const bool rows_contig = (sr == 1);
   if (threadIdx.x < kSplitRowsCrt) {
     const int64_t r = r0 + threadIdx.x;
-    const int m = (r < rows) ? row_mu(maxbits[r], sumsq[r], b) : kCrtZeroRow;
-    row_mu_s[threadIdx.x] = m;
-    if (blockIdx.x == 0) mu[r] = m;
+    row_mu_s[threadIdx.x] = mu[r];
   }
   for (int idx = threadIdx.x; idx < kSplitRowsCrt * kSplitColsCrt; idx += blockDim.x) {
     int rr, ll;
@@ -729,14 +796,17 @@ cudaError_t launch_gemm_config(const CrtOperand& a, const CrtOperand& b, const C
 int64_t crt_tile_rows(int tile_n) { return tile_n == kTilePair ? 256 : 128; }
 int64_t crt_tile_cols(int tile_n) { return tile_n == 128 ? 128 : 256; }
 
-cudaError_t launch_crt_norms(const StridedView<double>& x, const CrtOperand& op, cudaStream_t stream) {
-  cudaError_t e = cudaMemsetAsync(op.sumsq, 0, size_t(op.rows) * sizeof(uint64_t), stream);
+cudaError_t launch_crt_scan_norms(const StridedView<double>& x, const CrtOperand& op, int* nonfinite, double* spread,
+                                  cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(op.maxbits, 0, size_t(op.rows) * sizeof(uint64_t), stream);
   if (e != cudaSuccess || x.rows == 0 || x.cols == 0) return e;
+  if (op.k_pad % kNormCols != 0) return cudaErrorInvalidValue;
   dim3 grid(unsigned((x.cols + kNormCols - 1) / kNormCols), unsigned((x.rows + kNormRows - 1) / kNormRows));
   if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
-  crt_norm_kernel<<<grid, 256, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl,
-                                            reinterpret_cast<const unsigned long long*>(op.maxbits),
-                                            reinterpret_cast<unsigned long long*>(op.sumsq));
+  crt_scan_norm_kernel<<<grid, 256, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl,
+                                                 reinterpret_cast<unsigned long long*>(op.maxbits), op.chunk_e,
+                                                 reinterpret_cast<unsigned long long*>(op.chunk_s),
+                                                 op.k_pad / kNormCols, nonfinite, spread);
   return cudaGetLastError();
 }
 
@@ -745,20 +815,19 @@ cudaError_t launch_crt_split(const StridedView<double>& x, const CrtOperand& op,
   if (op.k_pad % kSplitColsCrt != 0 || op.rows_pad % kSplitRowsCrt != 0) return cudaErrorInvalidValue;
   dim3 grid(unsigned(op.k_pad / kSplitColsCrt), unsigned(op.rows_pad / kSplitRowsCrt));
   if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
-  const unsigned long long* mb = reinterpret_cast<const unsigned long long*>(op.maxbits);
-  const unsigned long long* ss = reinterpret_cast<const unsigned long long*>(op.sumsq);
   const int b = crt_bits(moduli);
+  crt_mu_kernel<<<unsigned((op.rows_pad + 255) / 256), 256, 0, stream>>>(
+      reinterpret_cast<const unsigned long long*>(op.maxbits), op.chunk_e,
+      reinterpret_cast<const unsigned long long*>(op.chunk_s), op.k_pad / kNormCols, op.rows, op.rows_pad, b, op.mu);
   if (moduli == kCrtDefaultModuli && b <= 62)
     crt_split_kernel<false, kCrtDefaultModuli><<<grid, kSplitThreadsCrt, 0, stream>>>(
-        x.ptr, x.rows, x.cols, x.sr, x.sl, mb, ss, b, moduli, op.residues, op.mu, op.rows_pad, op.k_pad);
+        x.ptr, x.rows, x.cols, x.sr, x.sl, op.mu, moduli, op.residues, op.rows_pad, op.k_pad);
   else if (b <= 62)
-    crt_split_kernel<false, 0><<<grid, kSplitThreadsCrt, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl, mb, ss, b,
-                                                                     moduli, op.residues, op.mu, op.rows_pad,
-                                                                     op.k_pad);
+    crt_split_kernel<false, 0><<<grid, kSplitThreadsCrt, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl, op.mu, moduli,
+                                                                     op.residues, op.rows_pad, op.k_pad);
   else
-    crt_split_kernel<true, 0><<<grid, kSplitThreadsCrt, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl, mb, ss, b,
-                                                                    moduli, op.residues, op.mu, op.rows_pad,
-                                                                    op.k_pad);
+    crt_split_kernel<true, 0><<<grid, kSplitThreadsCrt, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl, op.mu, moduli,
+                                                                    op.residues, op.rows_pad, op.k_pad);
   return cudaGetLastError();
 }
 

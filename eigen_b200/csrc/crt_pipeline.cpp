@@ -74,9 +74,12 @@ int dgemm_crt_pipelined(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int
     off = align256(off + bytes);
     return o;
   };
-  const size_t o_mb_a = take(size_t(m) * 8), o_ss_a = take(size_t(m) * 8), o_mu_a = take(size_t(m_pad) * 4);
+  const int64_t nchunks = k_pad / kOzakiKBlock;  // 128-column chunks of the norm bounds
+  const size_t o_mb_a = take(size_t(m) * 8), o_ss_a = take(size_t(m) * nchunks * 8),
+               o_ce_a = take(size_t(m) * nchunks * 4), o_mu_a = take(size_t(m_pad) * 4);
   const size_t o_res_a = take(size_t(nmod) * m_pad * k_pad);
-  const size_t o_mb_b = take(size_t(nc) * 8), o_ss_b = take(size_t(nc) * 8), o_mu_b = take(size_t(nc_pad) * 4);
+  const size_t o_mb_b = take(size_t(nc) * 8), o_ss_b = take(size_t(nc) * nchunks * 8),
+               o_ce_b = take(size_t(nc) * nchunks * 4), o_mu_b = take(size_t(nc_pad) * 4);
   const size_t o_res_b = take(size_t(nmod) * nc_pad * k_pad);
   const size_t o_res_c = take(size_t(nmod) * m_pad * nc_pad);
   const size_t o_est = take(sizeof(double) * 2 * Context::kPipeChunks);
@@ -120,22 +123,19 @@ int dgemm_crt_pipelined(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int
   const StridedView<double> va = ta ? StridedView<double>{dA, m, k, a_rows, 1} : StridedView<double>{dA, m, k, 1, a_rows};
   CrtOperand oa{reinterpret_cast<int8_t*>(ws + o_res_a), reinterpret_cast<int32_t*>(ws + o_mu_a),
                 reinterpret_cast<uint64_t*>(ws + o_mb_a), reinterpret_cast<uint64_t*>(ws + o_ss_a),
-                m, m_pad, k, k_pad, nmod};
-  const OzakiOperand sa{nullptr, nullptr, oa.maxbits, nullptr, m, m_pad, k, k_pad, 0};
+                reinterpret_cast<int32_t*>(ws + o_ce_a), m, m_pad, k, k_pad, nmod};
   bool ok = check_cuda(cudaMemsetAsync(df, 0, sizeof(DeviceFlags), st), "reset flags");
   ok = ok && check_cuda(cudaMemsetAsync(d_est, 0, sizeof(double) * 2 * Context::kPipeChunks, st), "reset estimates");
   ok = ok && check_cuda(cudaStreamWaitEvent(st, cx.ev_a, 0), "wait A");
   cudaEventRecord(cx.ev_start, st);
-  ok = ok && check_cuda(launch_ozaki_scan_reset(sa, st), "scan reset A");
-  ok = ok && check_cuda(launch_ozaki_scan(va, sa, &df->nonfinite, &df->spread[0], st), "scan A");
-  ok = ok && check_cuda(launch_crt_norms(va, oa, st), "norms A");
+  ok = ok && check_cuda(launch_crt_scan_norms(va, oa, &df->nonfinite, &df->spread[0], st), "scan A");
   ok = ok && check_cuda(launch_crt_split(va, oa, nmod, st), "residues A");
   if (!ok) return EB2_ERR_CUDA;
   info.launches += 3;
 
   CrtOperand ob{reinterpret_cast<int8_t*>(ws + o_res_b), reinterpret_cast<int32_t*>(ws + o_mu_b),
                 reinterpret_cast<uint64_t*>(ws + o_mb_b), reinterpret_cast<uint64_t*>(ws + o_ss_b),
-                nc, nc_pad, k, k_pad, nmod};
+                reinterpret_cast<int32_t*>(ws + o_ce_b), nc, nc_pad, k, k_pad, nmod};
   bool degraded = false;  // a block missed the target: the rest takes the ordinary path
 
   // the ordinary device path for block c (adds moduli as needed), C block restored first
@@ -214,12 +214,9 @@ int dgemm_crt_pipelined(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int
     const StridedView<double> vb =
         tb ? StridedView<double>{bblk, w, k, 1, b_rows} : StridedView<double>{bblk, w, k, b_rows, 1};
     ob.rows = w;
-    const OzakiOperand sb{nullptr, nullptr, ob.maxbits, nullptr, w, nc_pad, k, k_pad, 0};
     const int tile = choose_crt_tile(cx, m, w);
     ok = check_cuda(cudaStreamWaitEvent(st, cx.ev_in[c], 0), "wait B block");
-    ok = ok && check_cuda(launch_ozaki_scan_reset(sb, st), "scan reset B");
-    ok = ok && check_cuda(launch_ozaki_scan(vb, sb, &df->nonfinite, &df->spread[0], st), "scan B");
-    ok = ok && check_cuda(launch_crt_norms(vb, ob, st), "norms B");
+    ok = ok && check_cuda(launch_crt_scan_norms(vb, ob, &df->nonfinite, &df->spread[0], st), "scan B");
     ok = ok && check_cuda(launch_crt_split(vb, ob, nmod, st), "residues B");
     CrtGemmArgs g{};
     g.m = m;
@@ -258,7 +255,7 @@ int dgemm_crt_pipelined(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int
     ok = ok && check_cuda(cudaMemcpyAsync(cx.hflags, df, sizeof(DeviceFlags), cudaMemcpyDeviceToHost, st), "read flags");
     ok = ok && check_cuda(cudaEventRecord(cx.ev_done[c], st), "event");
     if (!ok) return EB2_ERR_CUDA;
-    info.launches += 9;
+    info.launches += 8;
     if (pending >= 0) {  // check the previous block while this one runs
       const int rc = finish_block(pending);
       if (rc != EB2_OK) return rc;

@@ -121,10 +121,15 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   off = align256(off + size_t(m) * 8);
   const size_t o_mb_b = off;
   off = align256(off + size_t(n) * 8);
+  const int64_t nchunks = k_pad / kOzakiKBlock;  // 128-column chunks of the norm bounds
   const size_t o_ss_a = off;
-  off = align256(off + size_t(m) * 8);
+  off = align256(off + size_t(m) * nchunks * 8);
   const size_t o_ss_b = off;
-  off = align256(off + size_t(n) * 8);
+  off = align256(off + size_t(n) * nchunks * 8);
+  const size_t o_ce_a = off;
+  off = align256(off + size_t(m) * nchunks * 4);
+  const size_t o_ce_b = off;
+  off = align256(off + size_t(n) * nchunks * 4);
   const size_t o_mu_a = off;
   off = align256(off + size_t(m_pad) * 4);
   const size_t o_mu_b = off;
@@ -145,23 +150,16 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   DeviceFlags* df = cx.dflags;
   CrtOperand oa{reinterpret_cast<int8_t*>(ws + o_res_a), reinterpret_cast<int32_t*>(ws + o_mu_a),
                 reinterpret_cast<uint64_t*>(ws + o_mb_a), reinterpret_cast<uint64_t*>(ws + o_ss_a),
-                m, m_pad, k, k_pad, nmax};
+                reinterpret_cast<int32_t*>(ws + o_ce_a), m, m_pad, k, k_pad, nmax};
   CrtOperand ob{reinterpret_cast<int8_t*>(ws + o_res_b), reinterpret_cast<int32_t*>(ws + o_mu_b),
                 reinterpret_cast<uint64_t*>(ws + o_mb_b), reinterpret_cast<uint64_t*>(ws + o_ss_b),
-                n, n_pad, k, k_pad, nmax};
-  // the row-maximum scan is shared with the digit-slice scheme
-  const OzakiOperand sa{nullptr, nullptr, oa.maxbits, nullptr, m, m_pad, k, k_pad, 0};
-  const OzakiOperand sb{nullptr, nullptr, ob.maxbits, nullptr, n, n_pad, k, k_pad, 0};
+                reinterpret_cast<int32_t*>(ws + o_ce_b), n, n_pad, k, k_pad, nmax};
 
   bool ok = check_cuda(cudaMemsetAsync(df, 0, sizeof(DeviceFlags), st), "reset flags");
-  ok = ok && check_cuda(launch_ozaki_scan_reset(sa, st), "scan reset A");
-  ok = ok && check_cuda(launch_ozaki_scan_reset(sb, st), "scan reset B");
-  ok = ok && check_cuda(launch_ozaki_scan(va, sa, &df->nonfinite, &df->spread[0], st), "scan A");
-  ok = ok && check_cuda(launch_ozaki_scan(vb, sb, &df->nonfinite, &df->spread[0], st), "scan B");
-  ok = ok && check_cuda(launch_crt_norms(va, oa, st), "norms A");
-  ok = ok && check_cuda(launch_crt_norms(vb, ob, st), "norms B");
+  ok = ok && check_cuda(launch_crt_scan_norms(va, oa, &df->nonfinite, &df->spread[0], st), "scan A");
+  ok = ok && check_cuda(launch_crt_scan_norms(vb, ob, &df->nonfinite, &df->spread[0], st), "scan B");
   if (!ok) return EB2_ERR_CUDA;
-  info.launches = 4;
+  info.launches = 2;
   if (stage2) {
     if (!check_cuda(cudaMemcpyAsync(cx.hflags, df, sizeof(DeviceFlags), cudaMemcpyDeviceToHost, st), "read scan") ||
         !check_cuda(cudaStreamSynchronize(st), "scan"))
@@ -210,7 +208,7 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
     if (first && opt.timed) cudaEventRecord(cx.ev_gemm1, st);
     r.write_c = !deferred;
     good = good && check_cuda(launch_crt_reconstruct(r, st), "CRT reconstruction");
-    info.launches += 4;
+    info.launches += 6;
     return good;
   };
   ok = product(true);

@@ -115,14 +115,17 @@ int64_t crt_tile_cols(int tile_n);
 struct CrtOperand {
   int8_t* residues;   // [nmax][rows_pad][k_pad] symmetric residues, row r contiguous along k
   int32_t* mu;        // [rows_pad] scale exponents: A'_r = trunc(2^mu_r x_r) (kCrtZeroRow: A'_r = 0)
-  uint64_t* maxbits;  // [rows] bit pattern of max |x| (from launch_ozaki_scan)
-  uint64_t* sumsq;    // [rows] integer upper bound of the scaled sum of squares
+  uint64_t* maxbits;  // [rows] bit pattern of max |x|
+  uint64_t* chunk_s;  // [rows][k_pad/128] integer norm bound of each 128-column chunk, relative to
+  int32_t* chunk_e;   // [rows][k_pad/128]   the exponent of the chunk's maximum
   int64_t rows, rows_pad, k, k_pad;
   int nmax;
 };
-// Zero and accumulate the row norm bounds (needs maxbits).
-cudaError_t launch_crt_norms(const StridedView<double>& x, const CrtOperand& op, cudaStream_t stream);
-// mu and the residues for moduli [0, moduli) (needs maxbits and sumsq).
+// One read of op(X): row maxima, chunk norm bounds, the NaN/Inf flag (*nonfinite = 1) and
+// the exponent-spread statistic (spread[0..1] += sum, count; may be null).
+cudaError_t launch_crt_scan_norms(const StridedView<double>& x, const CrtOperand& op, int* nonfinite, double* spread,
+                                  cudaStream_t stream);
+// mu for `moduli` moduli, then the residues for moduli [0, moduli) (needs the scan).
 cudaError_t launch_crt_split(const StridedView<double>& x, const CrtOperand& op, int moduli, cudaStream_t stream);
 
 struct CrtGemmArgs {

@@ -131,10 +131,15 @@ extern "C" int eb2_dgemm_device_noalloc(char transa, char transb, int64_t m, int
   off = align256(off + size_t(m) * 8);
   const size_t o_mb_b = off;
   off = align256(off + size_t(n) * 8);
+  const int64_t nchunks = k_pad / kOzakiKBlock;  // 128-column chunks of the norm bounds
   const size_t o_ss_a = off;
-  off = align256(off + size_t(m) * 8);
+  off = align256(off + size_t(m) * nchunks * 8);
   const size_t o_ss_b = off;
-  off = align256(off + size_t(n) * 8);
+  off = align256(off + size_t(n) * nchunks * 8);
+  const size_t o_ce_a = off;
+  off = align256(off + size_t(m) * nchunks * 4);
+  const size_t o_ce_b = off;
+  off = align256(off + size_t(n) * nchunks * 4);
   const size_t o_mu_a = off;
   off = align256(off + size_t(m_pad) * 4);
   const size_t o_mu_b = off;
@@ -162,22 +167,17 @@ extern "C" int eb2_dgemm_device_noalloc(char transa, char transb, int64_t m, int
       tb ? StridedView<double>{b, n, k, 1, ldb} : StridedView<double>{b, n, k, ldb, 1};  // op(B)^T, n x k
   CrtOperand oa{reinterpret_cast<int8_t*>(ws + o_res_a), reinterpret_cast<int32_t*>(ws + o_mu_a),
                 reinterpret_cast<uint64_t*>(ws + o_mb_a), reinterpret_cast<uint64_t*>(ws + o_ss_a),
-                m, m_pad, k, k_pad, kNoAllocModuli};
+                reinterpret_cast<int32_t*>(ws + o_ce_a), m, m_pad, k, k_pad, kNoAllocModuli};
   CrtOperand ob{reinterpret_cast<int8_t*>(ws + o_res_b), reinterpret_cast<int32_t*>(ws + o_mu_b),
                 reinterpret_cast<uint64_t*>(ws + o_mb_b), reinterpret_cast<uint64_t*>(ws + o_ss_b),
-                n, n_pad, k, k_pad, kNoAllocModuli};
-  const OzakiOperand sa{nullptr, nullptr, oa.maxbits, nullptr, m, m_pad, k, k_pad, 0};
-  const OzakiOperand sb{nullptr, nullptr, ob.maxbits, nullptr, n, n_pad, k, k_pad, 0};
+                reinterpret_cast<int32_t*>(ws + o_ce_b), n, n_pad, k, k_pad, kNoAllocModuli};
 
-  // The scratch keeps whatever the previous call left: the flags, the row maxima
-  // (atomicMax) and the norm bounds (atomicAdd) start from zero; residues are overwritten.
+  // The scratch keeps whatever the previous call left: the flags and the row maxima
+  // (atomicMax, zeroed by the scan launcher) start from zero; the chunk norm bounds, scale
+  // exponents and residues are overwritten.
   bool good = ok(cudaMemsetAsync(flags, 0, sizeof(NoAllocFlags), st), "reset flags");
-  good = good && ok(launch_ozaki_scan_reset(sa, st), "reset row maxima A");
-  good = good && ok(launch_ozaki_scan_reset(sb, st), "reset row maxima B");
-  good = good && ok(launch_ozaki_scan(va, sa, &flags->nonfinite, nullptr, st), "scan A");
-  good = good && ok(launch_ozaki_scan(vb, sb, &flags->nonfinite, nullptr, st), "scan B");
-  good = good && ok(launch_crt_norms(va, oa, st), "norms A");  // zeroes its sums first
-  good = good && ok(launch_crt_norms(vb, ob, st), "norms B");
+  good = good && ok(launch_crt_scan_norms(va, oa, &flags->nonfinite, nullptr, st), "scan A");
+  good = good && ok(launch_crt_scan_norms(vb, ob, &flags->nonfinite, nullptr, st), "scan B");
   good = good && ok(launch_crt_split(va, oa, kNoAllocModuli, st), "residues A");
   good = good && ok(launch_crt_split(vb, ob, kNoAllocModuli, st), "residues B");
   CrtGemmArgs g{};

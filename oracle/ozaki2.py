@@ -8,8 +8,10 @@ directly.  What the model does restate exactly is every floating-point step that
 the result:
 
   * e_r: exponent of the row maximum (max |x| in [2^(e-1), 2^e));
-  * S_r = sum over nonzero x of ceil(rn(x'^2) 2^32) + 1, x' = x 2^-e computed as two exact
-    power-of-two products (``scale2``), an integer upper bound of ||x||^2 2^(32-2e);
+  * per 128-column chunk c: S_c = sum over nonzero x of ceil(rn(x'^2) 2^32) + 1, with
+    x' = x 2^-e_c (e_c: exponent of the chunk maximum) computed as two exact power-of-two
+    products (``scale2``); folded into S_r = sum_c ceil(S_c 4^(e_c - e)), an integer upper
+    bound of ||x||^2 2^(32-2e);
   * mu_r = b - (e - 16 + ceil(L/2)), L = bit length of S_r - 1 (0 for a zero row);
   * A'_rl = trunc(scale2(x_rl, mu_r)) as an exact integer;
   * C_ij = alpha * RN(RN(C'_ij) 2^-(mu_i + nu_j))  [+ beta C_ij as one fused multiply-add].
@@ -57,21 +59,35 @@ def scale2(x: float, e: int) -> float:
     return float(np.float64(np.float64(x) * np.float64(math.ldexp(1.0, e1))) * np.float64(math.ldexp(1.0, e - e1)))
 
 
+CHUNK = 128  # columns (along K) per norm-bound chunk
+
+
 def row_mu(row: np.ndarray, b: int) -> int:
+    """Scale exponent of one row from chunked integer norm bounds: per 128-column chunk c,
+    S_c = sum over nonzero x of ceil(rn(x'^2) 2^32) + 1 with x' = x 2^-e_c (e_c: exponent of
+    the chunk maximum); S = sum_c ceil(S_c 4^(e_c - e)) with e the row maximum's exponent;
+    mu = b - (e - 16 + ceil(L/2)), L the bit length of S - 1."""
     row = np.asarray(row, dtype=np.float64)
     mx = float(np.max(np.abs(row))) if row.size else 0.0
     if mx == 0.0 or not math.isfinite(mx):
         return 0
     e = math.frexp(mx)[1]
     S = 0
-    for x in row:
-        x = float(x)
-        if x != 0.0:
-            xs = scale2(x, -e)
-            sq = float(np.float64(xs) * np.float64(xs))
-            S += int(math.ceil(sq * 4294967296.0)) + 1
-    if S == 0:
-        return 0
+    for c0 in range(0, row.size, CHUNK):
+        chunk = row[c0:c0 + CHUNK]
+        cmx = float(np.max(np.abs(chunk)))
+        if cmx == 0.0:
+            continue
+        ec = math.frexp(cmx)[1]
+        Sc = 0
+        for x in chunk:
+            x = float(x)
+            if x != 0.0:
+                xs = scale2(x, -ec)
+                sq = float(np.float64(xs) * np.float64(xs))
+                Sc += int(math.ceil(sq * 4294967296.0)) + 1
+        sh = 2 * (e - ec)
+        S += 1 if sh >= 64 else ((Sc - 1) >> sh) + 1
     L = (S - 1).bit_length() if S > 1 else 0
     return b - (e - 16 + (L + 1) // 2)
 
