@@ -176,6 +176,46 @@ def sgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, ilp64=Fa
     _gemm("sgemm", ctypes.c_float, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, ilp64)
 
 
+# Argument kinds of the other exported level-3 routines, in the order of their Fortran
+# signatures: c = character, i = dimension, s = scalar, a = array.
+LEVEL3_SIGNATURES = {
+    "gemmtr": "cccii" "s" "ai" "ai" "s" "ai",  # uplo transa transb n k alpha a lda b ldb beta c ldc
+    "syrk": "ccii" "s" "ai" "s" "ai",          # uplo trans n k alpha a lda beta c ldc
+    "syr2k": "ccii" "s" "ai" "ai" "s" "ai",    # uplo trans n k alpha a lda b ldb beta c ldc
+    "symm": "ccii" "s" "ai" "ai" "s" "ai",     # side uplo m n alpha a lda b ldb beta c ldc
+    "trmm": "ccccii" "s" "ai" "ai",            # side uplo transa diag m n alpha a lda b ldb
+    "trsm": "ccccii" "s" "ai" "ai",            # side uplo transa diag m n alpha a lda b ldb
+}
+
+
+def level3(name: str, *args, ilp64: bool = False) -> None:
+    """Call an exported level-3 routine by its BLAS name (``dsyrk``, ``strsm``, ``dgemmtr`` ...)
+    with its Fortran argument list in order (see ``LEVEL3_SIGNATURES``): characters as str,
+    dimensions and scalars as Python numbers, matrices as numpy arrays / torch tensors (host or
+    CUDA) or raw addresses.  ``ilp64`` calls the ``_64_`` symbol."""
+    lib = load()
+    dtype, routine = name[0], name[1:]
+    kinds = LEVEL3_SIGNATURES[routine]
+    if dtype not in "ds" or len(args) != len(kinds):
+        raise ValueError(f"{name}: expected {len(kinds)} arguments")
+    ctype = ctypes.c_double if dtype == "d" else ctypes.c_float
+    itype = ctypes.c_int64 if ilp64 else ctypes.c_int
+    out, keep = [], []
+    for kind, v in zip(kinds, args):
+        if kind == "c":
+            out.append(ctypes.c_char_p(v.encode() if isinstance(v, str) else bytes(v)))
+            continue
+        if kind == "a":
+            out.append(ctypes.c_void_p(_ptr(v)))
+            continue
+        x = itype(v) if kind == "i" else ctype(v)
+        keep.append(x)
+        out.append(ctypes.cast(ctypes.byref(x), ctypes.c_void_p))
+    f = getattr(lib, name + ("_64_" if ilp64 else "_"))
+    f.restype = None
+    f(*out)
+
+
 def dgemm_device(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, stream=0, check_accuracy=True) -> int:
     """Stream-ordered DGEMM on device pointers (``eb2_dgemm_device``); returns an EB2_* status."""
     return load().eb2_dgemm_device(transa.encode(), transb.encode(), m, n, k, alpha, _ptr(a), lda, _ptr(b), ldb, beta,

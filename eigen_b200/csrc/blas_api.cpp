@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 
+#include "blas_common.h"
 #include "context.h"
 #include "eigen_b200/blas.h"
 #include "gemm_driver.h"
@@ -22,16 +23,30 @@ extern "C" __attribute__((weak)) void xerbla_(const char* name, int* info, size_
 }
 
 namespace eb2 {
-namespace {
 
-enum { kNoTr = 0, kTr = 1, kAdj = 2, kInvalid = 0xff };
-
-int op_code(char c) {
-  if (c == 'N' || c == 'n') return kNoTr;
-  if (c == 'T' || c == 't') return kTr;
-  if (c == 'C' || c == 'c') return kAdj;
-  return kInvalid;
+bool device_usable(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
+
+bool copy_block(void* dst, size_t dpitch, const void* src, size_t spitch, size_t row_bytes, int64_t cols,
+                cudaMemcpyKind kind, cudaStream_t st) {
+  if (cols <= 0 || row_bytes == 0) return true;
+  cudaError_t e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, row_bytes, size_t(cols), kind, st);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    set_error(EB2_ERR_CUDA, "staging copy failed: %s", cudaGetErrorString(e));
+    return false;
+  }
+  return true;
+}
+
+namespace {
 
 // blas/level3_impl.h:61-78
 int gemm_info(char ta, char tb, int64_t m, int64_t n, int64_t k, int64_t lda, int64_t ldb, int64_t ldc) {
@@ -45,30 +60,6 @@ int gemm_info(char ta, char tb, int64_t m, int64_t n, int64_t k, int64_t lda, in
   if (ldb < std::max<int64_t>(1, ob == kNoTr ? k : n)) return 10;
   if (ldc < std::max<int64_t>(1, m)) return 13;
   return 0;
-}
-
-// True when the device can use the pointer in place (device or managed memory).
-bool device_usable(const void* p) {
-  if (!p) return false;
-  cudaPointerAttributes a;
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    (void)cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
-
-// Copy a rows x cols column-major block (leading dimension ld) host<->device.
-bool copy_block(void* dst, size_t dpitch, const void* src, size_t spitch, size_t row_bytes, int64_t cols,
-                cudaMemcpyKind kind, cudaStream_t st) {
-  if (cols <= 0 || row_bytes == 0) return true;
-  cudaError_t e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, row_bytes, size_t(cols), kind, st);
-  if (e != cudaSuccess) {
-    (void)cudaGetLastError();
-    set_error(EB2_ERR_CUDA, "staging copy failed: %s", cudaGetErrorString(e));
-    return false;
-  }
-  return true;
 }
 
 template <typename T>

@@ -39,6 +39,7 @@ struct Context {
   std::mutex mu;                  // one product at a time per device
   DeviceBuffer ws;                // emulation workspace (digits, exponents, scan results)
   DeviceBuffer stage_a, stage_b, stage_c;  // device copies of host operands
+  DeviceBuffer tmp;               // level-3 routines: expanded operands, diagonal-block products
   DeviceFlags* dflags = nullptr;  // device
   DeviceFlags* hflags = nullptr;  // pinned host mirror
   // Host-buffer pipeline of the BLAS entry (copies overlapped with the product by column

@@ -179,4 +179,26 @@ struct SgemmSplitArgs {
 cudaError_t launch_sgemm_split_bf16(const Bf16Operand& a, const Bf16Operand& b, const SgemmSplitArgs& args,
                                     cudaStream_t stream);
 
+// ------------------------------------------------------------ triangles (level-3 routines)
+constexpr int kTriBlock = 64;  // largest diagonal block launch_tri_block takes
+constexpr int kTriVecs = 64;   // vectors per CTA of launch_tri_block
+// out (n x n) = the symmetric matrix whose triangle `upper` (else lower) is stored in A.
+template <typename T>
+cudaError_t launch_expand_symmetric(const T* A, int64_t lda, int64_t n, bool upper, T* out, int64_t ldo,
+                                    cudaStream_t stream);
+// On the triangle `upper` of the n x n C only: C = P + beta C (beta == 0 does not read C;
+// P == null: C = beta C, beta == 0 writing zeros).
+template <typename T>
+cudaError_t launch_merge_triangle(const T* P, int64_t ldp, int64_t n, bool upper, T beta, T* C, int64_t ldc,
+                                  cudaStream_t stream);
+// X = alpha X by plain multiplication (NaN/Inf stay for alpha == 0).
+template <typename T>
+cudaError_t launch_multiply(int64_t m, int64_t n, T alpha, T* X, int64_t ldx, cudaStream_t stream);
+// x := E^-1 x (solve) or E x for `count` vectors (element r of vector t at X[r*vs + t*ts]),
+// E the nb x nb (nb <= kTriBlock) triangle `lower`/upper at E[r*er + c*ec], unit diagonal
+// if `unit` (then the stored diagonal is not read; neither is the other triangle).
+template <typename T>
+cudaError_t launch_tri_block(bool solve, const T* E, int64_t er, int64_t ec, int nb, bool lower, bool unit, T* X,
+                             int64_t vs, int64_t ts, int64_t count, cudaStream_t stream);
+
 }  // namespace eb2

@@ -1,0 +1,592 @@
+// level3_api.cpp -- the other level-3 BLAS routines Eigen's BLAS library exports, built on
+// the device GEMM: ?gemmtr_, ?syrk_, ?syr2k_, ?symm_, ?trmm_ and ?trsm_ (Fortran
+// convention, LP64 and ILP64 _64_ symbols), double and single precision.
+//
+// Argument checks, xerbla_ names and info codes, quick returns and the beta/alpha rules
+// restate blas/level3_impl.h (gemmtr :98-228, trsm :230-364, trmm :368-503, symm :507-592,
+// syrk :596-689, syr2k :693-754).  The products are Eigen's GEBP consumers
+// (GeneralMatrixMatrixTriangular.h, TriangularSolverMatrix.h, TriangularMatrixMatrix.h,
+// SelfadjointMatrixMatrix.h); here they are recursive block algorithms whose every product
+// is one device GEMM call (so DGEMM sub-products take the emulated or native FP64 kernels
+// the method setting and picker choose), with the triangles handled by the kernels of
+// tri.cu:
+//   gemmtr / syrk / syr2k  the n x n triangle split in two halves: the off-diagonal block
+//                          is one GEMM straight into C, the two diagonal halves recurse;
+//                          a diagonal block of at most kTrLeaf is a full GEMM into a
+//                          workspace merged into C's triangle;
+//   symm                   the symmetric operand expanded to a full matrix, then one GEMM;
+//   trmm / trsm            the triangular operand split in two halves: one GEMM for the
+//                          off-diagonal block, recursion on the diagonal halves, and a
+//                          shared-memory substitution (or multiply) kernel for diagonal
+//                          blocks of at most kTriBlock.
+// Host operands are staged through device buffers; device or managed operands are used in
+// place.  The calls are synchronous.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <functional>
+
+#include "blas_common.h"
+#include "context.h"
+#include "eigen_b200/blas.h"
+#include "gemm_driver.h"
+#include "kernels.h"
+
+namespace eb2 {
+namespace {
+
+constexpr int64_t kTrLeaf = 1024;   // largest diagonal block of gemmtr computed as a full product
+constexpr int64_t kTrSplit = 256;   // gemmtr halves are rounded to this
+
+int64_t imax1(int64_t v) { return std::max<int64_t>(1, v); }
+
+// ---------------------------------------------------------------- argument checks
+// blas/level3_impl.h:182-199
+int gemmtr_info(char uplo, char ta, char tb, int64_t n, int64_t k, int64_t lda, int64_t ldb, int64_t ldc) {
+  if (uplo_code(uplo) == kInvalid) return 1;
+  if (op_code(ta) == kInvalid) return 2;
+  if (op_code(tb) == kInvalid) return 3;
+  if (n < 0) return 4;
+  if (k < 0) return 5;
+  if (lda < imax1(op_code(ta) == kNoTr ? n : k)) return 8;
+  if (ldb < imax1(op_code(tb) == kNoTr ? k : n)) return 10;
+  if (ldc < imax1(n)) return 13;
+  return 0;
+}
+
+// blas/level3_impl.h:636-649
+int syrk_info(char uplo, char op, int64_t n, int64_t k, int64_t lda, int64_t ldc) {
+  if (uplo_code(uplo) == kInvalid) return 1;
+  if (op_code(op) == kInvalid) return 2;
+  if (n < 0) return 3;
+  if (k < 0) return 4;
+  if (lda < imax1(op_code(op) == kNoTr ? n : k)) return 7;
+  if (ldc < imax1(n)) return 10;
+  return 0;
+}
+
+// blas/level3_impl.h:702-717
+int syr2k_info(char uplo, char op, int64_t n, int64_t k, int64_t lda, int64_t ldb, int64_t ldc) {
+  if (uplo_code(uplo) == kInvalid) return 1;
+  if (op_code(op) == kInvalid) return 2;
+  if (n < 0) return 3;
+  if (k < 0) return 4;
+  if (lda < imax1(op_code(op) == kNoTr ? n : k)) return 7;
+  if (ldb < imax1(op_code(op) == kNoTr ? n : k)) return 9;
+  if (ldc < imax1(n)) return 12;
+  return 0;
+}
+
+// blas/level3_impl.h:516-531
+int symm_info(char side, char uplo, int64_t m, int64_t n, int64_t lda, int64_t ldb, int64_t ldc) {
+  if (side_code(side) == kInvalid) return 1;
+  if (uplo_code(uplo) == kInvalid) return 2;
+  if (m < 0) return 3;
+  if (n < 0) return 4;
+  if (lda < imax1(side_code(side) == kLeft ? m : n)) return 7;
+  if (ldb < imax1(m)) return 9;
+  if (ldc < imax1(m)) return 12;
+  return 0;
+}
+
+// trsm blas/level3_impl.h:330-347, trmm :467-484 (the same checks)
+int trxm_info(char side, char uplo, char op, char diag, int64_t m, int64_t n, int64_t lda, int64_t ldb) {
+  if (side_code(side) == kInvalid) return 1;
+  if (uplo_code(uplo) == kInvalid) return 2;
+  if (op_code(op) == kInvalid) return 3;
+  if (diag_code(diag) == kInvalid) return 4;
+  if (m < 0) return 5;
+  if (n < 0) return 6;
+  if (lda < imax1(side_code(side) == kLeft ? m : n)) return 9;
+  if (ldb < imax1(m)) return 11;
+  return 0;
+}
+
+// ---------------------------------------------------------------- products
+// Summary of the GEMM calls of one routine, reported through eb2_last_call_info.
+struct Summary {
+  int method = 0, slices = 0, escalations = 0, nonfinite = 0, launches = 0, calls = 0;
+  double err = -1.0;
+  int64_t biggest = -1;  // flops of the largest call (its method is reported)
+};
+
+bool cuda_ok(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return true;
+  (void)cudaGetLastError();
+  set_error(EB2_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return false;
+}
+
+// C = alpha op(A) op(B) + beta C on device pointers, queued on st.  DGEMM sub-products keep
+// the a-posteriori accuracy check of the emulated methods (which waits for its flags);
+// native products are only queued.
+int gemm(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
+         int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc, cudaStream_t st,
+         Summary& sum) {
+  if (m == 0 || n == 0) return EB2_OK;
+  DgemmOptions o;
+  o.sync = false;
+  o.check_accuracy = true;
+  o.timed = false;
+  eb2_call_info ci{};
+  const int rc = dgemm_on_device(cx, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, st, o, ci);
+  const int64_t flops = m * n * k;
+  if (flops > sum.biggest) {
+    sum.biggest = flops;
+    sum.method = ci.method;
+  }
+  sum.slices = std::max(sum.slices, ci.slices);
+  sum.escalations += ci.escalations;
+  sum.nonfinite |= ci.nonfinite;
+  sum.launches += ci.launches;
+  sum.err = std::max(sum.err, ci.err_estimate);
+  sum.calls += 1;
+  return rc;
+}
+
+int gemm(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, float alpha, const float* A, int64_t lda,
+         const float* B, int64_t ldb, float beta, float* C, int64_t ldc, cudaStream_t st, Summary& sum) {
+  if (m == 0 || n == 0) return EB2_OK;
+  SgemmOptions o;
+  o.sync = false;
+  o.timed = false;
+  eb2_call_info ci{};
+  const int rc = sgemm_on_device(cx, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, st, o, ci);
+  const int64_t flops = m * n * k;
+  if (flops > sum.biggest) {
+    sum.biggest = flops;
+    sum.method = ci.method;
+  }
+  sum.slices = std::max(sum.slices, ci.slices);
+  sum.nonfinite |= ci.nonfinite;
+  sum.launches += ci.launches;
+  sum.calls += 1;
+  return rc;
+}
+
+// An accuracy miss of one sub-product is reported at the end; everything else stops.
+bool keep_going(int rc, int& worst) {
+  if (rc == EB2_OK) return true;
+  if (rc == EB2_ERR_ACCURACY) {
+    worst = EB2_ERR_ACCURACY;
+    return true;
+  }
+  worst = rc;
+  return false;
+}
+
+// ---------------------------------------------------------------- device algorithms
+// Row block [r0, ..) of op(X) and column block [c0, ..) of op(X), X column-major (ld ldx).
+template <typename T>
+const T* op_rows(const T* X, int64_t ldx, bool trans, int64_t r0) {
+  return trans ? X + r0 * ldx : X + r0;
+}
+template <typename T>
+const T* op_cols(const T* X, int64_t ldx, bool trans, int64_t c0) {
+  return trans ? X + c0 : X + c0 * ldx;
+}
+
+// The triangle `upper` of the n x n C := alpha op(A) op(B) + beta C (op(A) n x k, op(B) k x n).
+template <typename T>
+int gemmtr_device(Context& cx, bool upper, bool ta, bool tb, int64_t n, int64_t k, T alpha, const T* A, int64_t lda,
+                  const T* B, int64_t ldb, T beta, T* C, int64_t ldc, cudaStream_t st, Summary& sum) {
+  if (n == 0) return EB2_OK;
+  if (k == 0 || alpha == T(0)) {
+    if (beta == T(1)) return EB2_OK;
+    return cuda_ok(launch_merge_triangle<T>(nullptr, 0, n, upper, beta, C, ldc, st), "scale triangle") ? EB2_OK
+                                                                                                     : EB2_ERR_CUDA;
+  }
+  const int64_t leaf = std::min(n, kTrLeaf);
+  if (!cx.tmp.ensure(size_t(leaf) * size_t(leaf) * sizeof(T))) {
+    set_error(EB2_ERR_ALLOC, "could not allocate the diagonal-block workspace");
+    return EB2_ERR_ALLOC;
+  }
+  T* P = static_cast<T*>(cx.tmp.ptr);
+  int worst = EB2_OK;
+  std::function<bool(int64_t, int64_t)> rec = [&](int64_t n0, int64_t size) -> bool {
+    if (size <= kTrLeaf) {
+      // the diagonal block as a full product, merged into the triangle
+      if (!keep_going(gemm(cx, ta, tb, size, size, k, alpha, op_rows(A, lda, ta, n0), lda, op_cols(B, ldb, tb, n0),
+                           ldb, T(0), P, size, st, sum),
+                      worst))
+        return false;
+      if (!cuda_ok(launch_merge_triangle<T>(P, size, size, upper, beta, C + n0 + n0 * ldc, ldc, st), "merge")) {
+        worst = EB2_ERR_CUDA;
+        return false;
+      }
+      return true;
+    }
+    const int64_t h = std::min(size - 1, (size / 2 + kTrSplit - 1) / kTrSplit * kTrSplit);
+    // the off-diagonal block straight into C
+    const int rc = upper ? gemm(cx, ta, tb, h, size - h, k, alpha, op_rows(A, lda, ta, n0), lda,
+                                op_cols(B, ldb, tb, n0 + h), ldb, beta, C + n0 + (n0 + h) * ldc, ldc, st, sum)
+                         : gemm(cx, ta, tb, size - h, h, k, alpha, op_rows(A, lda, ta, n0 + h), lda,
+                                op_cols(B, ldb, tb, n0), ldb, beta, C + (n0 + h) + n0 * ldc, ldc, st, sum);
+    if (!keep_going(rc, worst)) return false;
+    return rec(n0, h) && rec(n0 + h, size - h);
+  };
+  rec(0, n);
+  return worst;
+}
+
+// C := alpha A B + beta C (left, A m x m) or alpha B A + beta C (right, A n x n), A
+// symmetric with the triangle `upper` stored.
+template <typename T>
+int symm_device(Context& cx, bool left, bool upper, int64_t m, int64_t n, T alpha, const T* A, int64_t lda,
+                const T* B, int64_t ldb, T beta, T* C, int64_t ldc, cudaStream_t st, Summary& sum) {
+  if (m == 0 || n == 0) return EB2_OK;
+  const int64_t size = left ? m : n;
+  T* S = nullptr;
+  if (alpha != T(0)) {
+    if (!cx.tmp.ensure(size_t(size) * size_t(size) * sizeof(T))) {
+      set_error(EB2_ERR_ALLOC, "could not allocate the symmetric-operand workspace");
+      return EB2_ERR_ALLOC;
+    }
+    S = static_cast<T*>(cx.tmp.ptr);
+    if (!cuda_ok(launch_expand_symmetric<T>(A, lda, size, upper, S, size, st), "expand")) return EB2_ERR_CUDA;
+  }
+  // alpha == 0 reads neither operand (the GEMM then only scales C)
+  return left ? gemm(cx, false, false, m, n, m, alpha, S, size, B, ldb, beta, C, ldc, st, sum)
+              : gemm(cx, false, false, m, n, n, alpha, B, ldb, S, size, beta, C, ldc, st, sum);
+}
+
+// In place on the m x n B: B := op(A)^-1 B / B op(A)^-1 (solve) or op(A) B / B op(A)
+// (multiply), A triangular (triangle `upper` stored, unit diagonal if `unit`), then
+// B := alpha B.
+template <typename T>
+int trxm_device(Context& cx, bool solve, bool left, bool upper, bool trans, bool unit, int64_t m, int64_t n, T alpha,
+                const T* A, int64_t lda, T* B, int64_t ldb, cudaStream_t st, Summary& sum) {
+  if (m == 0 || n == 0) return EB2_OK;
+  // M = op(A); `lower` is M's triangle
+  const bool lower = trans ? upper : !upper;
+  // block M[r0.., c0..] as a GEMM operand (with transpose flag `trans`)
+  auto msub = [&](int64_t r0, int64_t c0) -> const T* { return trans ? A + c0 + r0 * lda : A + r0 + c0 * lda; };
+  const T sign = solve ? T(-1) : T(1);
+  int worst = EB2_OK;
+  auto leaf = [&](int64_t i0, int64_t nb) -> bool {
+    const T* D = A + i0 + i0 * lda;  // diagonal block of A (and of M)
+    // M(r, c) of the block at D[r*mr + c*mc]
+    const int64_t mr = trans ? lda : 1, mc = trans ? 1 : lda;
+    cudaError_t e;
+    if (left)  // vectors: the columns of B's rows [i0, i0+nb)
+      e = launch_tri_block<T>(solve, D, mr, mc, int(nb), lower, unit, B + i0, 1, ldb, n, st);
+    else  // x M = b is M^T x^T = b^T; vectors: the rows of B's columns [i0, i0+nb)
+      e = launch_tri_block<T>(solve, D, mc, mr, int(nb), !lower, unit, B + i0 * ldb, ldb, 1, m, st);
+    if (!cuda_ok(e, "triangular block")) {
+      worst = EB2_ERR_CUDA;
+      return false;
+    }
+    return true;
+  };
+  // B's rows (left) or columns (right) [d0, d0+dn) += sign * (M block) * B's [s0, s0+sn)
+  auto update = [&](int64_t d0, int64_t dn, int64_t s0, int64_t sn) -> bool {
+    const int rc = left ? gemm(cx, trans, false, dn, n, sn, sign, msub(d0, s0), lda, B + s0, ldb, T(1), B + d0, ldb,
+                               st, sum)
+                        : gemm(cx, false, trans, m, dn, sn, sign, B + s0 * ldb, ldb, msub(s0, d0), lda, T(1),
+                               B + d0 * ldb, ldb, st, sum);
+    return keep_going(rc, worst);
+  };
+  std::function<bool(int64_t, int64_t)> rec = [&](int64_t i0, int64_t size) -> bool {
+    if (size <= kTriBlock) return leaf(i0, size);
+    const int64_t h = (size / 2 + kTriBlock - 1) / kTriBlock * kTriBlock;
+    const int64_t a0 = i0, an = h, b0 = i0 + h, bn = size - h;
+    // The first half in the order below is the one whose new values the update does not
+    // need (solve) or whose old values it still needs (multiply).
+    bool first_is_a;
+    if (left)
+      first_is_a = solve ? lower : !lower;
+    else
+      first_is_a = solve ? !lower : lower;
+    if (first_is_a) {
+      if (solve) return rec(a0, an) && update(b0, bn, a0, an) && rec(b0, bn);
+      // multiply: update a from b (old), then a, then b
+      return rec(a0, an) && update(a0, an, b0, bn) && rec(b0, bn);
+    }
+    if (solve) return rec(b0, bn) && update(a0, an, b0, bn) && rec(a0, an);
+    return rec(b0, bn) && update(b0, bn, a0, an) && rec(a0, an);
+  };
+  if (!rec(0, left ? m : n)) return worst;
+  if (alpha != T(1) && !cuda_ok(launch_multiply<T>(m, n, alpha, B, ldb, st), "scale")) return EB2_ERR_CUDA;
+  return worst;
+}
+
+// ---------------------------------------------------------------- host entry points
+// A matrix argument as the device sees it: the caller's pointer when the device can use it
+// in place, else a device copy (leading dimension = rows).
+template <typename T>
+struct Operand {
+  T* ptr = nullptr;
+  int64_t ld = 0;
+  bool staged = false;
+};
+
+template <typename T>
+bool stage(DeviceBuffer& buf, const T* p, int64_t ld, int64_t rows, int64_t cols, bool copy_in, cudaStream_t st,
+           Operand<T>& out) {
+  out.ptr = const_cast<T*>(p);
+  out.ld = ld;
+  out.staged = false;
+  if (rows == 0 || cols == 0 || device_usable(p)) return true;
+  if (!buf.ensure(size_t(rows) * size_t(cols) * sizeof(T))) {
+    set_error(EB2_ERR_ALLOC, "could not allocate staging memory");
+    return false;
+  }
+  out.ptr = static_cast<T*>(buf.ptr);
+  out.ld = rows;
+  out.staged = true;
+  return !copy_in ||
+         copy_block(out.ptr, size_t(rows) * sizeof(T), p, size_t(ld) * sizeof(T), size_t(rows) * sizeof(T), cols,
+                    cudaMemcpyHostToDevice, st);
+}
+
+// One routine call: the device context locked for its duration, the call record, and the
+// end of the call (the output copied back when staged, the stream drained, errors printed
+// like the GEMM entry points do).
+struct Call {
+  Context* cx = nullptr;
+  std::unique_lock<std::mutex> lock;
+  cudaStream_t st = nullptr;
+  Summary sum;
+  char dtype = 'd';
+
+  explicit Call(char dt) : dtype(dt) {}
+
+  bool begin() {
+    cx = current_context();
+    if (!cx) {
+      std::fprintf(stderr, "eigen_b200: %s\n", eb2_last_error_string());
+      return false;
+    }
+    lock = std::unique_lock<std::mutex>(cx->mu);
+    st = cx->stream;
+    call_info() = eb2_call_info{};
+    set_pending_timing(nullptr, false);
+    return true;
+  }
+
+  // the operands are on the device: the routine's device time starts here
+  void started() { cudaEventRecord(cx->ev_start, st); }
+
+  void fail() {
+    std::fprintf(stderr, "eigen_b200: %s\n", eb2_last_error_string());
+    (void)cudaStreamSynchronize(st);
+  }
+
+  // rc of the device algorithm; `out` the output operand, copied back to (host, host_ld).
+  template <typename T>
+  void end(int rc, bool any_staged, const Operand<T>& out, T* host, int64_t host_ld, int64_t rows, int64_t cols) {
+    eb2_call_info& ci = call_info();
+    ci.dtype = dtype;
+    ci.method = sum.method;
+    ci.slices = sum.slices;
+    ci.escalations = sum.escalations;
+    ci.nonfinite = sum.nonfinite;
+    ci.staged = any_staged ? 1 : 0;
+    ci.err_estimate = sum.err;
+    ci.launches = sum.launches;
+    if (rc != EB2_OK && rc != EB2_ERR_ACCURACY) return fail();
+    if (out.staged && !copy_block(host, size_t(host_ld) * sizeof(T), out.ptr, size_t(rows) * sizeof(T),
+                                  size_t(rows) * sizeof(T), cols, cudaMemcpyDeviceToHost, st))
+      return fail();
+    cudaEventRecord(cx->ev_stop, st);
+    if (!cuda_ok(cudaStreamSynchronize(st), "level-3 routine")) return fail();
+    set_pending_timing(cx, false);
+  }
+};
+
+template <typename T>
+constexpr char dtype_of() {
+  return sizeof(T) == 8 ? 'd' : 's';
+}
+template <typename T>
+constexpr const char* prefixed(const char* d, const char* s) {
+  return sizeof(T) == 8 ? d : s;
+}
+
+// blas/level3_impl.h:98-228: C's triangle := alpha op(A) op(B) + beta C's triangle
+template <typename T>
+void blas_gemmtr(char uplo, char opa, char opb, int64_t n, int64_t k, T alpha, const T* a, int64_t lda, const T* b,
+                 int64_t ldb, T beta, T* c, int64_t ldc) {
+  int info = gemmtr_info(uplo, opa, opb, n, k, lda, ldb, ldc);
+  if (info) return xerbla_(prefixed<T>("DGEMMTR", "SGEMMTR"), &info, 7);
+  if (n == 0) return;
+  Call call(dtype_of<T>());
+  if (!call.begin()) return;
+  const bool ta = op_code(opa) != kNoTr, tb = op_code(opb) != kNoTr;
+  const bool need_ab = k > 0 && alpha != T(0);
+  Operand<T> A, B, C;
+  // C keeps its other triangle: the whole square goes to the device and back
+  if (!stage(call.cx->stage_a, a, lda, need_ab ? (ta ? k : n) : 0, ta ? n : k, true, call.st, A) ||
+      !stage(call.cx->stage_b, b, ldb, need_ab ? (tb ? n : k) : 0, tb ? k : n, true, call.st, B) ||
+      !stage(call.cx->stage_c, c, ldc, n, n, true, call.st, C))
+    return call.fail();
+  call.started();
+  const int rc = gemmtr_device<T>(*call.cx, uplo_code(uplo) == kUp, ta, tb, n, k, alpha, A.ptr, A.ld, B.ptr, B.ld,
+                                  beta, C.ptr, C.ld, call.st, call.sum);
+  call.end(rc, A.staged || B.staged || C.staged, C, c, ldc, n, n);
+}
+
+// blas/level3_impl.h:596-689: C's triangle := alpha op(A) op(A)^T + beta C's triangle
+template <typename T>
+void blas_syrk(char uplo, char op, int64_t n, int64_t k, T alpha, const T* a, int64_t lda, T beta, T* c,
+               int64_t ldc) {
+  int info = syrk_info(uplo, op, n, k, lda, ldc);
+  if (info) return xerbla_(prefixed<T>("DSYRK ", "SSYRK "), &info, 6);
+  if (n == 0) return;
+  Call call(dtype_of<T>());
+  if (!call.begin()) return;
+  const bool ta = op_code(op) != kNoTr;
+  const bool need_a = k > 0 && alpha != T(0);
+  Operand<T> A, C;
+  if (!stage(call.cx->stage_a, a, lda, need_a ? (ta ? k : n) : 0, ta ? n : k, true, call.st, A) ||
+      !stage(call.cx->stage_c, c, ldc, n, n, true, call.st, C))
+    return call.fail();
+  call.started();
+  // op(A) op(A)^T: the same matrix on both sides, with opposite transposes
+  const int rc = gemmtr_device<T>(*call.cx, uplo_code(uplo) == kUp, ta, !ta, n, k, alpha, A.ptr, A.ld, A.ptr, A.ld,
+                                  beta, C.ptr, C.ld, call.st, call.sum);
+  call.end(rc, A.staged || C.staged, C, c, ldc, n, n);
+}
+
+// blas/level3_impl.h:693-754: C's triangle := alpha (op(A) op(B)^T + op(B) op(A)^T) + beta C's
+template <typename T>
+void blas_syr2k(char uplo, char op, int64_t n, int64_t k, T alpha, const T* a, int64_t lda, const T* b, int64_t ldb,
+                T beta, T* c, int64_t ldc) {
+  int info = syr2k_info(uplo, op, n, k, lda, ldb, ldc);
+  if (info) return xerbla_(prefixed<T>("DSYR2K", "SSYR2K"), &info, 6);
+  if (n == 0) return;
+  Call call(dtype_of<T>());
+  if (!call.begin()) return;
+  const bool ta = op_code(op) != kNoTr;
+  const bool need_ab = k > 0 && alpha != T(0);
+  const int64_t rows = need_ab ? (ta ? k : n) : 0, cols = ta ? n : k;
+  Operand<T> A, B, C;
+  if (!stage(call.cx->stage_a, a, lda, rows, cols, true, call.st, A) ||
+      !stage(call.cx->stage_b, b, ldb, rows, cols, true, call.st, B) ||
+      !stage(call.cx->stage_c, c, ldc, n, n, true, call.st, C))
+    return call.fail();
+  call.started();
+  const bool up = uplo_code(uplo) == kUp;
+  int rc = gemmtr_device<T>(*call.cx, up, ta, !ta, n, k, alpha, A.ptr, A.ld, B.ptr, B.ld, beta, C.ptr, C.ld,
+                            call.st, call.sum);
+  if (rc == EB2_OK || rc == EB2_ERR_ACCURACY) {
+    const int rc2 = gemmtr_device<T>(*call.cx, up, ta, !ta, n, k, alpha, B.ptr, B.ld, A.ptr, A.ld, T(1), C.ptr, C.ld,
+                                     call.st, call.sum);
+    if (rc2 != EB2_OK) rc = rc2;
+  }
+  call.end(rc, A.staged || B.staged || C.staged, C, c, ldc, n, n);
+}
+
+// blas/level3_impl.h:507-592: C := alpha A B + beta C (left) or alpha B A + beta C (right)
+template <typename T>
+void blas_symm(char side, char uplo, int64_t m, int64_t n, T alpha, const T* a, int64_t lda, const T* b,
+               int64_t ldb, T beta, T* c, int64_t ldc) {
+  int info = symm_info(side, uplo, m, n, lda, ldb, ldc);
+  if (info) return xerbla_(prefixed<T>("DSYMM ", "SSYMM "), &info, 6);
+  if (m == 0 || n == 0) return;
+  Call call(dtype_of<T>());
+  if (!call.begin()) return;
+  const bool left = side_code(side) == kLeft;
+  const int64_t size = left ? m : n;
+  const bool need_ab = alpha != T(0);
+  Operand<T> A, B, C;
+  if (!stage(call.cx->stage_a, a, lda, need_ab ? size : 0, size, true, call.st, A) ||
+      !stage(call.cx->stage_b, b, ldb, need_ab ? m : 0, n, true, call.st, B) ||
+      !stage(call.cx->stage_c, c, ldc, m, n, beta != T(0), call.st, C))
+    return call.fail();
+  call.started();
+  const int rc = symm_device<T>(*call.cx, left, uplo_code(uplo) == kUp, m, n, alpha, A.ptr, A.ld, B.ptr, B.ld, beta,
+                                C.ptr, C.ld, call.st, call.sum);
+  call.end(rc, A.staged || B.staged || C.staged, C, c, ldc, m, n);
+}
+
+// blas/level3_impl.h:230-364 (solve) and :368-503 (multiply), in place on B
+template <typename T>
+void blas_trxm(bool solve, char side, char uplo, char op, char diag, int64_t m, int64_t n, T alpha, const T* a,
+               int64_t lda, T* b, int64_t ldb) {
+  int info = trxm_info(side, uplo, op, diag, m, n, lda, ldb);
+  if (info)
+    return xerbla_(solve ? prefixed<T>("DTRSM ", "STRSM ") : prefixed<T>("DTRMM ", "STRMM "), &info, 6);
+  if (m == 0 || n == 0) return;
+  Call call(dtype_of<T>());
+  if (!call.begin()) return;
+  const bool left = side_code(side) == kLeft;
+  const int64_t size = left ? m : n;
+  Operand<T> A, B;
+  if (!stage(call.cx->stage_a, a, lda, size, size, true, call.st, A) ||
+      !stage(call.cx->stage_b, b, ldb, m, n, true, call.st, B))
+    return call.fail();
+  call.started();
+  const int rc = trxm_device<T>(*call.cx, solve, left, uplo_code(uplo) == kUp, op_code(op) != kNoTr,
+                                diag_code(diag) == kUnit, m, n, alpha, A.ptr, A.ld, B.ptr, B.ld, call.st, call.sum);
+  call.end(rc, A.staged || B.staged, B, b, ldb, m, n);
+}
+
+}  // namespace
+}  // namespace eb2
+
+using eb2::blas_gemmtr;
+using eb2::blas_symm;
+using eb2::blas_syr2k;
+using eb2::blas_syrk;
+using eb2::blas_trxm;
+
+// The exported symbols: LP64 (int) and ILP64 (int64_t, _64_ suffix), as blas/level3_impl.h
+// declares them through EIGEN_BLAS_FUNC (blas/common.h).
+#define EB2_LEVEL3_SYMBOLS(I, SFX)                                                                                   \
+  void dgemmtr##SFX(const char* uplo, const char* ta, const char* tb, const I* n, const I* k, const double* alpha,    \
+                    const double* a, const I* lda, const double* b, const I* ldb, const double* beta, double* c,     \
+                    const I* ldc) {                                                                                  \
+    blas_gemmtr<double>(*uplo, *ta, *tb, *n, *k, *alpha, a, *lda, b, *ldb, *beta, c, *ldc);                          \
+  }                                                                                                                  \
+  void sgemmtr##SFX(const char* uplo, const char* ta, const char* tb, const I* n, const I* k, const float* alpha,     \
+                    const float* a, const I* lda, const float* b, const I* ldb, const float* beta, float* c,         \
+                    const I* ldc) {                                                                                  \
+    blas_gemmtr<float>(*uplo, *ta, *tb, *n, *k, *alpha, a, *lda, b, *ldb, *beta, c, *ldc);                           \
+  }                                                                                                                  \
+  void dsyrk##SFX(const char* uplo, const char* op, const I* n, const I* k, const double* alpha, const double* a,    \
+                  const I* lda, const double* beta, double* c, const I* ldc) {                                       \
+    blas_syrk<double>(*uplo, *op, *n, *k, *alpha, a, *lda, *beta, c, *ldc);                                          \
+  }                                                                                                                  \
+  void ssyrk##SFX(const char* uplo, const char* op, const I* n, const I* k, const float* alpha, const float* a,      \
+                  const I* lda, const float* beta, float* c, const I* ldc) {                                         \
+    blas_syrk<float>(*uplo, *op, *n, *k, *alpha, a, *lda, *beta, c, *ldc);                                           \
+  }                                                                                                                  \
+  void dsyr2k##SFX(const char* uplo, const char* op, const I* n, const I* k, const double* alpha, const double* a,   \
+                   const I* lda, const double* b, const I* ldb, const double* beta, double* c, const I* ldc) {       \
+    blas_syr2k<double>(*uplo, *op, *n, *k, *alpha, a, *lda, b, *ldb, *beta, c, *ldc);                                \
+  }                                                                                                                  \
+  void ssyr2k##SFX(const char* uplo, const char* op, const I* n, const I* k, const float* alpha, const float* a,     \
+                   const I* lda, const float* b, const I* ldb, const float* beta, float* c, const I* ldc) {          \
+    blas_syr2k<float>(*uplo, *op, *n, *k, *alpha, a, *lda, b, *ldb, *beta, c, *ldc);                                 \
+  }                                                                                                                  \
+  void dsymm##SFX(const char* side, const char* uplo, const I* m, const I* n, const double* alpha, const double* a,  \
+                  const I* lda, const double* b, const I* ldb, const double* beta, double* c, const I* ldc) {        \
+    blas_symm<double>(*side, *uplo, *m, *n, *alpha, a, *lda, b, *ldb, *beta, c, *ldc);                               \
+  }                                                                                                                  \
+  void ssymm##SFX(const char* side, const char* uplo, const I* m, const I* n, const float* alpha, const float* a,    \
+                  const I* lda, const float* b, const I* ldb, const float* beta, float* c, const I* ldc) {           \
+    blas_symm<float>(*side, *uplo, *m, *n, *alpha, a, *lda, b, *ldb, *beta, c, *ldc);                                \
+  }                                                                                                                  \
+  void dtrmm##SFX(const char* side, const char* uplo, const char* op, const char* diag, const I* m, const I* n,     \
+                  const double* alpha, const double* a, const I* lda, double* b, const I* ldb) {                     \
+    blas_trxm<double>(false, *side, *uplo, *op, *diag, *m, *n, *alpha, a, *lda, b, *ldb);                            \
+  }                                                                                                                  \
+  void strmm##SFX(const char* side, const char* uplo, const char* op, const char* diag, const I* m, const I* n,     \
+                  const float* alpha, const float* a, const I* lda, float* b, const I* ldb) {                        \
+    blas_trxm<float>(false, *side, *uplo, *op, *diag, *m, *n, *alpha, a, *lda, b, *ldb);                             \
+  }                                                                                                                  \
+  void dtrsm##SFX(const char* side, const char* uplo, const char* op, const char* diag, const I* m, const I* n,     \
+                  const double* alpha, const double* a, const I* lda, double* b, const I* ldb) {                     \
+    blas_trxm<double>(true, *side, *uplo, *op, *diag, *m, *n, *alpha, a, *lda, b, *ldb);                             \
+  }                                                                                                                  \
+  void strsm##SFX(const char* side, const char* uplo, const char* op, const char* diag, const I* m, const I* n,     \
+                  const float* alpha, const float* a, const I* lda, float* b, const I* ldb) {                        \
+    blas_trxm<float>(true, *side, *uplo, *op, *diag, *m, *n, *alpha, a, *lda, b, *ldb);                              \
+  }
+
+extern "C" {
+EB2_LEVEL3_SYMBOLS(int, _)
+EB2_LEVEL3_SYMBOLS(int64_t, _64_)
+}

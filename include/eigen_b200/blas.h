@@ -50,6 +50,89 @@ void sgemm_64_(const char* transa, const char* transb, const int64_t* m, const i
                const float* alpha, const float* a, const int64_t* lda, const float* b, const int64_t* ldb,
                const float* beta, float* c, const int64_t* ldc);
 
+/* ------------------------------------------------ the other level-3 routines
+ * Eigen's BLAS library exports these beside ?gemm_ (blas/level3_impl.h, instantiated by
+ * blas/double.cpp and blas/single.cpp); each replaces the routine of the same name, with
+ * its argument checks (xerbla_ name and info codes), quick returns and beta/alpha rules.
+ * Every product inside goes through the device GEMM above (DGEMM sub-products take the
+ * method and accuracy settings of dgemm_); pointers may be host or device memory.  LP64
+ * symbols take int, the _64_ symbols int64_t. */
+
+/* Triangle `uplo` of the n x n C := alpha*op(A)*op(B) + beta*C, the other triangle untouched.
+ * blas/level3_impl.h:98-228; info 1,2,3,4,5,8,10,13 to xerbla_("?GEMMTR", info, 7);
+ * n == 0 returns; beta scales the triangle (beta == 0: zeros) before k == 0 returns. */
+void dgemmtr_(const char* uplo, const char* transa, const char* transb, const int* n, const int* k,
+              const double* alpha, const double* a, const int* lda, const double* b, const int* ldb,
+              const double* beta, double* c, const int* ldc);
+void sgemmtr_(const char* uplo, const char* transa, const char* transb, const int* n, const int* k,
+              const float* alpha, const float* a, const int* lda, const float* b, const int* ldb, const float* beta,
+              float* c, const int* ldc);
+/* Triangle `uplo` of C := alpha*A*A^T + beta*C ('N') or alpha*A^T*A + beta*C ('T'/'C').
+ * blas/level3_impl.h:596-689; info 1,2,3,4,7,10 to xerbla_("?SYRK ", info, 6). */
+void dsyrk_(const char* uplo, const char* trans, const int* n, const int* k, const double* alpha, const double* a,
+            const int* lda, const double* beta, double* c, const int* ldc);
+void ssyrk_(const char* uplo, const char* trans, const int* n, const int* k, const float* alpha, const float* a,
+            const int* lda, const float* beta, float* c, const int* ldc);
+/* Triangle `uplo` of C := alpha*(A*B^T + B*A^T) + beta*C ('N'), transposed forms for 'T'/'C'.
+ * blas/level3_impl.h:693-754; info 1,2,3,4,7,9,12 to xerbla_("?SYR2K", info, 6). */
+void dsyr2k_(const char* uplo, const char* trans, const int* n, const int* k, const double* alpha, const double* a,
+             const int* lda, const double* b, const int* ldb, const double* beta, double* c, const int* ldc);
+void ssyr2k_(const char* uplo, const char* trans, const int* n, const int* k, const float* alpha, const float* a,
+             const int* lda, const float* b, const int* ldb, const float* beta, float* c, const int* ldc);
+/* C := alpha*A*B + beta*C ('L') or alpha*B*A + beta*C ('R'), A symmetric, triangle `uplo` read.
+ * blas/level3_impl.h:507-592; info 1,2,3,4,7,9,12 to xerbla_("?SYMM ", info, 6). */
+void dsymm_(const char* side, const char* uplo, const int* m, const int* n, const double* alpha, const double* a,
+            const int* lda, const double* b, const int* ldb, const double* beta, double* c, const int* ldc);
+void ssymm_(const char* side, const char* uplo, const int* m, const int* n, const float* alpha, const float* a,
+            const int* lda, const float* b, const int* ldb, const float* beta, float* c, const int* ldc);
+/* B := alpha*op(A)*B ('L') or alpha*B*op(A) ('R'), A triangular ('U'/'L'; diag 'N'/'U').
+ * blas/level3_impl.h:368-503; info 1,2,3,4,5,6,9,11 to xerbla_("?TRMM ", info, 6). */
+void dtrmm_(const char* side, const char* uplo, const char* transa, const char* diag, const int* m, const int* n,
+            const double* alpha, const double* a, const int* lda, double* b, const int* ldb);
+void strmm_(const char* side, const char* uplo, const char* transa, const char* diag, const int* m, const int* n,
+            const float* alpha, const float* a, const int* lda, float* b, const int* ldb);
+/* B := alpha*op(A)^-1*B ('L') or alpha*B*op(A)^-1 ('R'): the solve, then B *= alpha.
+ * blas/level3_impl.h:230-364; info 1,2,3,4,5,6,9,11 to xerbla_("?TRSM ", info, 6). */
+void dtrsm_(const char* side, const char* uplo, const char* transa, const char* diag, const int* m, const int* n,
+            const double* alpha, const double* a, const int* lda, double* b, const int* ldb);
+void strsm_(const char* side, const char* uplo, const char* transa, const char* diag, const int* m, const int* n,
+            const float* alpha, const float* a, const int* lda, float* b, const int* ldb);
+
+void dgemmtr_64_(const char* uplo, const char* transa, const char* transb, const int64_t* n, const int64_t* k,
+                 const double* alpha, const double* a, const int64_t* lda, const double* b, const int64_t* ldb,
+                 const double* beta, double* c, const int64_t* ldc);
+void sgemmtr_64_(const char* uplo, const char* transa, const char* transb, const int64_t* n, const int64_t* k,
+                 const float* alpha, const float* a, const int64_t* lda, const float* b, const int64_t* ldb,
+                 const float* beta, float* c, const int64_t* ldc);
+void dsyrk_64_(const char* uplo, const char* trans, const int64_t* n, const int64_t* k, const double* alpha,
+               const double* a, const int64_t* lda, const double* beta, double* c, const int64_t* ldc);
+void ssyrk_64_(const char* uplo, const char* trans, const int64_t* n, const int64_t* k, const float* alpha,
+               const float* a, const int64_t* lda, const float* beta, float* c, const int64_t* ldc);
+void dsyr2k_64_(const char* uplo, const char* trans, const int64_t* n, const int64_t* k, const double* alpha,
+                const double* a, const int64_t* lda, const double* b, const int64_t* ldb, const double* beta,
+                double* c, const int64_t* ldc);
+void ssyr2k_64_(const char* uplo, const char* trans, const int64_t* n, const int64_t* k, const float* alpha,
+                const float* a, const int64_t* lda, const float* b, const int64_t* ldb, const float* beta, float* c,
+                const int64_t* ldc);
+void dsymm_64_(const char* side, const char* uplo, const int64_t* m, const int64_t* n, const double* alpha,
+               const double* a, const int64_t* lda, const double* b, const int64_t* ldb, const double* beta,
+               double* c, const int64_t* ldc);
+void ssymm_64_(const char* side, const char* uplo, const int64_t* m, const int64_t* n, const float* alpha,
+               const float* a, const int64_t* lda, const float* b, const int64_t* ldb, const float* beta, float* c,
+               const int64_t* ldc);
+void dtrmm_64_(const char* side, const char* uplo, const char* transa, const char* diag, const int64_t* m,
+               const int64_t* n, const double* alpha, const double* a, const int64_t* lda, double* b,
+               const int64_t* ldb);
+void strmm_64_(const char* side, const char* uplo, const char* transa, const char* diag, const int64_t* m,
+               const int64_t* n, const float* alpha, const float* a, const int64_t* lda, float* b,
+               const int64_t* ldb);
+void dtrsm_64_(const char* side, const char* uplo, const char* transa, const char* diag, const int64_t* m,
+               const int64_t* n, const double* alpha, const double* a, const int64_t* lda, double* b,
+               const int64_t* ldb);
+void strsm_64_(const char* side, const char* uplo, const char* transa, const char* diag, const int64_t* m,
+               const int64_t* n, const float* alpha, const float* a, const int64_t* lda, float* b,
+               const int64_t* ldb);
+
 /* Argument-error hook, weak like blas/xerbla.cpp:18-20: prints
  * "Eigen BLAS ERROR #<info>: <name>" unless the program defines its own. */
 void xerbla_(const char* name, int* info, size_t len);
