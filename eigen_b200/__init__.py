@@ -176,6 +176,25 @@ def sgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, ilp64=Fa
     _gemm("sgemm", ctypes.c_float, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, ilp64)
 
 
+def complex_gemm(dtype, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, ilp64=False):
+    """C := alpha*op(A)*op(B) + beta*C through ``zgemm_`` (dtype "z") or ``cgemm_`` ("c"):
+    alpha, beta Python complex numbers; a, b, c complex numpy arrays / torch tensors (host or
+    CUDA, column-major) or raw addresses; op 'N', 'T' or 'C' (conjugate transpose)."""
+    lib = load()
+    real = ctypes.c_double if dtype == "z" else ctypes.c_float
+    it = ctypes.c_int64 if ilp64 else ctypes.c_int
+    al = (real * 2)(complex(alpha).real, complex(alpha).imag)
+    be = (real * 2)(complex(beta).real, complex(beta).imag)
+    dims = [it(v) for v in (m, n, k, lda, ldb, ldc)]
+    f = getattr(lib, ("zgemm" if dtype == "z" else "cgemm") + ("_64_" if ilp64 else "_"))
+    f.restype = None
+    enc = lambda x: x.encode() if isinstance(x, str) else bytes(x)
+    f(ctypes.c_char_p(enc(transa)), ctypes.c_char_p(enc(transb)), ctypes.byref(dims[0]), ctypes.byref(dims[1]),
+      ctypes.byref(dims[2]), ctypes.cast(al, ctypes.c_void_p), ctypes.c_void_p(_ptr(a)), ctypes.byref(dims[3]),
+      ctypes.c_void_p(_ptr(b)), ctypes.byref(dims[4]), ctypes.cast(be, ctypes.c_void_p), ctypes.c_void_p(_ptr(c)),
+      ctypes.byref(dims[5]))
+
+
 # Argument kinds of the other exported level-3 routines, in the order of their Fortran
 # signatures: c = character, i = dimension, s = scalar, a = array.
 LEVEL3_SIGNATURES = {

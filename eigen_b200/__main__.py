@@ -2,13 +2,21 @@
 
     python -m eigen_b200 gemm --dtype d --method crt --m 4096 --n 4096 --k 4096 [--reps 3] [--r 0]
     python -m eigen_b200 batch --dtype d --count 10000 [--reps 3]
+    python -m eigen_b200 level3 --routine trsm --chars LLNN --m 8192 --n 8192 [--k 8192] [--reps 3]
 
-`gemm` runs C = A*B (NN, column-major, alpha = 1, beta = 0) on device-resident random
+`gemm` runs C = A*B (NN, column-major, alpha = 1, beta = 0; --dtype z / c: the complex
+product through zgemm_ / cgemm_, rated at 8mnk flops) on device-resident random
 inputs (entries u*2^e, u ~ U[-1,1], e ~ U{-r..r}) with eb2_dgemm_device / eb2_sgemm_device
 (method auto | native | emulated | crt; for SGEMM emulated means split-BF16), once to warm
 up and then `reps` times, and prints one JSON line: the device time of each call (CUDA
 events on the launching stream) and the library's record of the last call.  `batch` runs
-the uneven 10,000-product batch of the benchmark as one grouped launch.
+the uneven 10,000-product batch of the benchmark as one grouped launch.  `level3` runs one of
+the other level-3 routines (gemmtr, syrk, syr2k, symm, trmm, trsm; `--chars` its character
+arguments in order) on device-resident operands through its BLAS symbol and reports the
+routine's device time (CUDA events the library records on its stream) and its rate in the
+routine's own flop count (syrk/gemmtr n(n+1)k, syr2k 2n(n+1)k, symm 2m^2n or 2mn^2, trmm/trsm
+m^2n or mn^2).  Triangular operands of trsm get a dominant diagonal (entries of the stored
+triangle ~ U[-1,1]/size, diagonal ~ +-U[1,2]).
 """
 from __future__ import annotations
 
@@ -21,7 +29,38 @@ import eigen_b200 as eb
 METHODS = {"auto": eb.METHOD_AUTO, "native": eb.METHOD_NATIVE, "emulated": eb.METHOD_EMULATED, "crt": eb.METHOD_CRT}
 
 
+def _complex_gemm(a, torch):
+    """zgemm_ / cgemm_ on device operands (8mnk real flops); time = the library's device events."""
+    dt = torch.complex128 if a.dtype == "z" else torch.complex64
+    g = torch.Generator(device="cuda")
+    g.manual_seed(a.seed)
+    A = torch.randn((a.k, a.m), dtype=dt, device="cuda", generator=g)
+    B = torch.randn((a.n, a.k), dtype=dt, device="cuda", generator=g)
+    C = torch.zeros((a.n, a.m), dtype=dt, device="cuda")
+    if a.dtype == "z":
+        eb.set_dgemm_method(METHODS[a.method])
+    else:
+        eb.set_sgemm_method(METHODS[a.method] if a.method != "crt" else eb.METHOD_EMULATED)
+    times = []
+    for i in range(a.reps + 1):
+        eb.complex_gemm(a.dtype, "N", "N", a.m, a.n, a.k, 1.0, A, a.m, B, a.k, 0.0, C, a.m)
+        err = eb.last_error()
+        if err[0] != eb.EB2_OK:
+            print(json.dumps({"error": err}))
+            return 1
+        if i:
+            times.append(eb.last_call_info()["kernel_ms"])
+    best = min(times)
+    print(json.dumps({"op": a.dtype + "gemm", "m": a.m, "n": a.n, "k": a.k, "method": a.method,
+                      "ms": [round(t, 4) for t in times],
+                      "tflops": round(8.0 * a.m * a.n * a.k / (best * 1e-3) / 1e12, 3),
+                      "call": eb.last_call_info()}))
+    return 0
+
+
 def _gemm(a, torch):
+    if a.dtype in ("z", "c"):
+        return _complex_gemm(a, torch)
     dt = torch.float64 if a.dtype == "d" else torch.float32
     g = torch.Generator(device="cuda")
     g.manual_seed(a.seed)
@@ -62,6 +101,70 @@ def _gemm(a, torch):
     return 0
 
 
+def _level3(a, torch):
+    dt = torch.float64 if a.dtype == "d" else torch.float32
+    g = torch.Generator(device="cuda")
+    g.manual_seed(a.seed)
+    ch = a.chars.upper()
+
+    def rnd(rows, cols):
+        return torch.rand((cols, rows), dtype=dt, device="cuda", generator=g) * 2 - 1  # column-major
+
+    r, m, n, k = a.routine, a.m, a.n, a.k
+    if r in ("gemmtr", "syrk", "syr2k"):
+        ta = ch[1] != "N"
+        tb = (ch[2] != "N") if r == "gemmtr" else not ta
+        A = rnd(k, n) if ta else rnd(n, k)
+        B = (rnd(n, k) if tb else rnd(k, n)) if r == "gemmtr" else (rnd(k, n) if ta else rnd(n, k))
+        C = rnd(n, n)
+        lda, ldb = A.shape[1], B.shape[1]
+        args = {"gemmtr": [*ch, n, k, 1.0, A, lda, B, ldb, 0.5, C, n],
+                "syrk": [*ch, n, k, 1.0, A, lda, 0.5, C, n],
+                "syr2k": [*ch, n, k, 1.0, A, lda, B, ldb, 0.5, C, n]}[r]
+        flops = (2 if r == "syr2k" else 1) * n * (n + 1) * k
+        dims = {"n": n, "k": k}
+    else:
+        left = ch[0] == "L"
+        size = m if left else n
+        A = rnd(size, size)
+        B = rnd(m, n)
+        if r == "symm":
+            C = rnd(m, n)
+            args = [*ch, m, n, 1.0, A, size, B, m, 0.5, C, m]
+            flops = 2 * size * m * n
+        else:
+            if r == "trsm":
+                A = A / size
+                d = (torch.rand(size, dtype=dt, device="cuda", generator=g) + 1) * torch.where(
+                    torch.rand(size, device="cuda", generator=g) < 0.5, -1.0, 1.0).to(dt)
+                A.diagonal().copy_(d)
+            args = [*ch, m, n, 1.0, A, size, B, m]
+            flops = size * m * n
+        dims = {"m": m, "n": n}
+    name = a.dtype + r
+    if a.dtype == "d":
+        eb.set_dgemm_method(METHODS[a.method])
+    else:
+        eb.set_sgemm_method(METHODS[a.method] if a.method != "crt" else eb.METHOD_EMULATED)
+    out = B if r in ("trmm", "trsm") else C
+    keep = out.clone()
+    times = []
+    for i in range(a.reps + 1):
+        out.copy_(keep)  # trmm / trsm overwrite their operand: every call starts from the same B
+        torch.cuda.synchronize()
+        eb.level3(name, *args)
+        err = eb.last_error()
+        if err[0] != eb.EB2_OK:
+            print(json.dumps({"error": err}))
+            return 1
+        if i:
+            times.append(eb.last_call_info()["kernel_ms"])
+    best = min(times)
+    print(json.dumps({"op": name, "chars": a.chars, **dims, "method": a.method, "ms": [round(t, 4) for t in times],
+                      "tflops": round(flops / (best * 1e-3) / 1e12, 3), "call": eb.last_call_info()}))
+    return 0
+
+
 def _batch(a, torch):
     import importlib.util
     from pathlib import Path
@@ -77,8 +180,11 @@ def _batch(a, torch):
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m eigen_b200", description=__doc__,
                                  formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("op", choices=["gemm", "batch"])
-    ap.add_argument("--dtype", choices=["d", "s"], default="d")
+    ap.add_argument("op", choices=["gemm", "batch", "level3"])
+    ap.add_argument("--routine", choices=["gemmtr", "syrk", "syr2k", "symm", "trmm", "trsm"], default="trsm")
+    ap.add_argument("--chars", default="LLNN", help="level3: the routine's character arguments, in order")
+    ap.add_argument("--dtype", choices=["d", "s", "z", "c"], default="d",
+                    help="z / c: complex GEMM through zgemm_ / cgemm_ (gemm only)")
     ap.add_argument("--method", choices=sorted(METHODS), default="auto")
     ap.add_argument("--m", type=int, default=4096)
     ap.add_argument("--n", type=int, default=4096)
@@ -93,7 +199,7 @@ def main(argv=None):
 
     eb.load()
     eb.set_timing(True)
-    return _gemm(a, torch) if a.op == "gemm" else _batch(a, torch)
+    return {"gemm": _gemm, "batch": _batch, "level3": _level3}[a.op](a, torch)
 
 
 if __name__ == "__main__":

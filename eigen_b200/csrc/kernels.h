@@ -201,4 +201,20 @@ template <typename T>
 cudaError_t launch_tri_block(bool solve, const T* E, int64_t er, int64_t ec, int nb, bool lower, bool unit, T* X,
                              int64_t vs, int64_t ts, int64_t count, cudaStream_t stream);
 
+// ------------------------------------------------------------ complex GEMM (two real products)
+// op(X) (rows x cols complex; element (r, c) at complex index r*sr + c*sc of the interleaved
+// array X; imaginary parts negated if conj) -> Y = [Re | Im] (rows x 2 cols, ld rows).
+template <typename T>
+cudaError_t launch_pack_complex_lhs(const T* X, int64_t sr, int64_t sc, bool conj, int64_t rows, int64_t cols, T* Y,
+                                    cudaStream_t stream);
+// op(X) (rows x cols complex) -> Y1 = [Re; -Im], Y2 = [Im; Re] (2 rows x cols each, ld 2 rows).
+template <typename T>
+cudaError_t launch_pack_complex_rhs(const T* X, int64_t sr, int64_t sc, bool conj, int64_t rows, int64_t cols, T* Y1,
+                                    T* Y2, cudaStream_t stream);
+// C (m x n complex, interleaved, ld ldc) = (ar + i ai)(Pr + i Pi) + (br + i bi) C; beta == 0
+// does not read C; Pr == null: C = beta C.
+template <typename T>
+cudaError_t launch_combine_complex(const T* Pr, const T* Pi, int64_t ldp, int64_t m, int64_t n, T ar, T ai, T br,
+                                   T bi, T* C, int64_t ldc, cudaStream_t stream);
+
 }  // namespace eb2

@@ -1,6 +1,7 @@
 // level3_api.cpp -- the other level-3 BLAS routines Eigen's BLAS library exports, built on
-// the device GEMM: ?gemmtr_, ?syrk_, ?syr2k_, ?symm_, ?trmm_ and ?trsm_ (Fortran
-// convention, LP64 and ILP64 _64_ symbols), double and single precision.
+// the device GEMM: ?gemmtr_, ?syrk_, ?syr2k_, ?symm_, ?trmm_ and ?trsm_ (double and single
+// precision) and the complex zgemm_ / cgemm_ (Fortran convention, LP64 and ILP64 _64_
+// symbols).
 //
 // Argument checks, xerbla_ names and info codes, quick returns and the beta/alpha rules
 // restate blas/level3_impl.h (gemmtr :98-228, trsm :230-364, trmm :368-503, symm :507-592,
@@ -385,6 +386,8 @@ struct Call {
     ci.staged = any_staged ? 1 : 0;
     ci.err_estimate = sum.err;
     ci.launches = sum.launches;
+    ci.kernel_ms = -1.0;
+    ci.gemm_kernel_ms = -1.0;
     if (rc != EB2_OK && rc != EB2_ERR_ACCURACY) return fail();
     if (out.staged && !copy_block(host, size_t(host_ld) * sizeof(T), out.ptr, size_t(rows) * sizeof(T),
                                   size_t(rows) * sizeof(T), cols, cudaMemcpyDeviceToHost, st))
@@ -523,9 +526,93 @@ void blas_trxm(bool solve, char side, char uplo, char op, char diag, int64_t m, 
   call.end(rc, A.staged || B.staged, B, b, ldb, m, n);
 }
 
+// blas/level3_impl.h:12-96 with Scalar = std::complex (blas/complex_double.cpp,
+// blas/complex_single.cpp): C := alpha op(A) op(B) + beta C, op in {N, T, C = conjugate
+// transpose}.  beta scales C first (0: zeros); k == 0 or alpha == 0 stops there
+// (Eigen/src/Core/products/GeneralMatrixMatrix.h:129-130).  The product is two real GEMMs of
+// inner dimension 2k on packed real operands (complex.cu), combined with complex alpha/beta.
+template <typename T>
+void blas_complex_gemm(char opa, char opb, int64_t m, int64_t n, int64_t k, const T* alpha, const T* a, int64_t lda,
+                       const T* b, int64_t ldb, const T* beta, T* c, int64_t ldc) {
+  int info = 0;
+  {
+    const int oa = op_code(opa), ob = op_code(opb);
+    if (oa == kInvalid) info = 1;
+    else if (ob == kInvalid) info = 2;
+    else if (m < 0) info = 3;
+    else if (n < 0) info = 4;
+    else if (k < 0) info = 5;
+    else if (lda < imax1(oa == kNoTr ? m : k)) info = 8;
+    else if (ldb < imax1(ob == kNoTr ? k : n)) info = 10;
+    else if (ldc < imax1(m)) info = 13;
+  }
+  if (info) return xerbla_(prefixed<T>("ZGEMM ", "CGEMM "), &info, 6);
+  if (m == 0 || n == 0) return;
+  const T ar = alpha[0], ai = alpha[1], br = beta[0], bi = beta[1];
+  const bool alpha_zero = ar == T(0) && ai == T(0);
+  const bool beta_one = br == T(1) && bi == T(0), beta_zero = br == T(0) && bi == T(0);
+  const bool need_ab = k > 0 && !alpha_zero;
+  if (!need_ab && beta_one) return;
+  Call call(dtype_of<T>() == 'd' ? 'z' : 'c');
+  if (!call.begin()) return;
+  const int oa = op_code(opa), ob = op_code(opb);
+  const int64_t a_rows = oa == kNoTr ? m : k, a_cols = oa == kNoTr ? k : m;
+  const int64_t b_rows = ob == kNoTr ? k : n, b_cols = ob == kNoTr ? n : k;
+  // complex column-major = real column-major with twice the rows and leading dimension
+  Operand<T> A, B, C;
+  if (!stage(call.cx->stage_a, a, 2 * lda, need_ab ? 2 * a_rows : 0, a_cols, true, call.st, A) ||
+      !stage(call.cx->stage_b, b, 2 * ldb, need_ab ? 2 * b_rows : 0, b_cols, true, call.st, B) ||
+      !stage(call.cx->stage_c, c, 2 * ldc, 2 * m, n, !beta_zero, call.st, C))
+    return call.fail();
+  call.started();
+  int rc = EB2_OK;
+  const int64_t ldc_c = C.ld / 2;
+  if (!need_ab) {
+    if (!cuda_ok(launch_combine_complex<T>(nullptr, nullptr, 0, m, n, ar, ai, br, bi, C.ptr, ldc_c, call.st),
+                 "scale C"))
+      rc = EB2_ERR_CUDA;
+    call.sum.launches += 1;
+  } else {
+    // workspace: A' (m x 2k), B1 and B2 (2k x n), Pr and Pi (m x n)
+    const size_t e_a = size_t(m) * 2 * k, e_b = size_t(2 * k) * n, e_p = size_t(m) * n;
+    if (!call.cx->tmp.ensure((e_a + 2 * e_b + 2 * e_p) * sizeof(T))) {
+      set_error(EB2_ERR_ALLOC, "could not allocate the complex-product workspace");
+      return call.fail();
+    }
+    T* Ap = static_cast<T*>(call.cx->tmp.ptr);
+    T* B1 = Ap + e_a;
+    T* B2 = B1 + e_b;
+    T* Pr = B2 + e_b;
+    T* Pi = Pr + e_p;
+    const int64_t lda_c = A.ld / 2, ldb_c = B.ld / 2;
+    bool ok = cuda_ok(launch_pack_complex_lhs<T>(A.ptr, oa == kNoTr ? 1 : lda_c, oa == kNoTr ? lda_c : 1,
+                                                 oa == kAdj, m, k, Ap, call.st),
+                      "pack op(A)");
+    ok = ok && cuda_ok(launch_pack_complex_rhs<T>(B.ptr, ob == kNoTr ? 1 : ldb_c, ob == kNoTr ? ldb_c : 1,
+                                                  ob == kAdj, k, n, B1, B2, call.st),
+                       "pack op(B)");
+    if (!ok) return call.fail();
+    call.sum.launches += 2;
+    int worst = EB2_OK;
+    if (keep_going(gemm(*call.cx, false, false, m, n, 2 * k, T(1), Ap, m, B1, 2 * k, T(0), Pr, m, call.st,
+                        call.sum),
+                   worst) &&
+        keep_going(gemm(*call.cx, false, false, m, n, 2 * k, T(1), Ap, m, B2, 2 * k, T(0), Pi, m, call.st,
+                        call.sum),
+                   worst)) {
+      if (!cuda_ok(launch_combine_complex<T>(Pr, Pi, m, m, n, ar, ai, br, bi, C.ptr, ldc_c, call.st), "combine"))
+        worst = EB2_ERR_CUDA;
+      call.sum.launches += 1;
+    }
+    rc = worst;
+  }
+  call.end(rc, A.staged || B.staged || C.staged, C, c, 2 * ldc, 2 * m, n);
+}
+
 }  // namespace
 }  // namespace eb2
 
+using eb2::blas_complex_gemm;
 using eb2::blas_gemmtr;
 using eb2::blas_symm;
 using eb2::blas_syr2k;
@@ -586,7 +673,23 @@ using eb2::blas_trxm;
     blas_trxm<float>(true, *side, *uplo, *op, *diag, *m, *n, *alpha, a, *lda, b, *ldb);                              \
   }
 
+// Complex GEMM: alpha, beta and the matrices as interleaved (re, im) pairs of the real type,
+// the prototypes of blas/blas.h:393-398.
+#define EB2_COMPLEX_GEMM_SYMBOLS(I, SFX)                                                                             \
+  void zgemm##SFX(const char* ta, const char* tb, const I* m, const I* n, const I* k, const double* alpha,          \
+                  const double* a, const I* lda, const double* b, const I* ldb, const double* beta, double* c,       \
+                  const I* ldc) {                                                                                    \
+    blas_complex_gemm<double>(*ta, *tb, *m, *n, *k, alpha, a, *lda, b, *ldb, beta, c, *ldc);                         \
+  }                                                                                                                  \
+  void cgemm##SFX(const char* ta, const char* tb, const I* m, const I* n, const I* k, const float* alpha,           \
+                  const float* a, const I* lda, const float* b, const I* ldb, const float* beta, float* c,           \
+                  const I* ldc) {                                                                                    \
+    blas_complex_gemm<float>(*ta, *tb, *m, *n, *k, alpha, a, *lda, b, *ldb, beta, c, *ldc);                          \
+  }
+
 extern "C" {
 EB2_LEVEL3_SYMBOLS(int, _)
 EB2_LEVEL3_SYMBOLS(int64_t, _64_)
+EB2_COMPLEX_GEMM_SYMBOLS(int, _)
+EB2_COMPLEX_GEMM_SYMBOLS(int64_t, _64_)
 }

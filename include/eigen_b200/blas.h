@@ -98,6 +98,25 @@ void dtrsm_(const char* side, const char* uplo, const char* transa, const char* 
 void strsm_(const char* side, const char* uplo, const char* transa, const char* diag, const int* m, const int* n,
             const float* alpha, const float* a, const int* lda, float* b, const int* ldb);
 
+/* Complex C := alpha*op(A)*op(B) + beta*C, op 'N', 'T' or 'C' (conjugate transpose); alpha,
+ * beta and the matrices hold interleaved (re, im) pairs.  Replaces Eigen's zgemm_/cgemm_
+ * (blas/level3_impl.h:12-96 instantiated by blas/complex_double.cpp / complex_single.cpp;
+ * prototypes blas/blas.h:393-398), which Eigen's operator* on complex matrices binds
+ * (GeneralMatrixMatrix_BLAS.h:116-117).  Same info codes as ?gemm_ to xerbla_("ZGEMM ", ..)
+ * / ("CGEMM ", ..); beta scales C first (0: zeros); k == 0 or alpha == 0 then returns. */
+void zgemm_(const char* transa, const char* transb, const int* m, const int* n, const int* k, const double* alpha,
+            const double* a, const int* lda, const double* b, const int* ldb, const double* beta, double* c,
+            const int* ldc);
+void cgemm_(const char* transa, const char* transb, const int* m, const int* n, const int* k, const float* alpha,
+            const float* a, const int* lda, const float* b, const int* ldb, const float* beta, float* c,
+            const int* ldc);
+void zgemm_64_(const char* transa, const char* transb, const int64_t* m, const int64_t* n, const int64_t* k,
+               const double* alpha, const double* a, const int64_t* lda, const double* b, const int64_t* ldb,
+               const double* beta, double* c, const int64_t* ldc);
+void cgemm_64_(const char* transa, const char* transb, const int64_t* m, const int64_t* n, const int64_t* k,
+               const float* alpha, const float* a, const int64_t* lda, const float* b, const int64_t* ldb,
+               const float* beta, float* c, const int64_t* ldc);
+
 void dgemmtr_64_(const char* uplo, const char* transa, const char* transb, const int64_t* n, const int64_t* k,
                  const double* alpha, const double* a, const int64_t* lda, const double* b, const int64_t* ldb,
                  const double* beta, double* c, const int64_t* ldc);

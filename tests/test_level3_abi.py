@@ -1,21 +1,22 @@
 """The other level-3 routines' C ABI without a GPU: exported symbols, and the argument errors of
-?gemmtr_, ?syrk_, ?syr2k_, ?symm_, ?trmm_ and ?trsm_ against the reference's info codes and
-xerbla_ names (blas/level3_impl.h:98-754), recorded from the reference in
-tests/golden/level3_golden.npz.  Argument errors and n == 0 quick returns touch neither the
-device nor the operands."""
+?gemmtr_, ?syrk_, ?syr2k_, ?symm_, ?trmm_, ?trsm_ and zgemm_/cgemm_ against the reference's info
+codes and xerbla_ names (blas/level3_impl.h:12-754), recorded from the reference in
+tests/golden/level3_golden.npz and tests/golden/complex_golden.npz.  Argument errors and n == 0
+quick returns touch neither the device nor the operands."""
 from __future__ import annotations
 
 import json
 import subprocess
+from pathlib import Path
 
 import numpy as np
 import pytest
 
 import eigen_b200 as eb
 from _helpers import load_xerbla_recorder
-from pathlib import Path
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "level3_golden.npz"
+COMPLEX_GOLDEN = Path(__file__).resolve().parent / "golden" / "complex_golden.npz"
 ROUTINES = ("gemmtr", "syrk", "syr2k", "symm", "trmm", "trsm")
 
 
@@ -32,6 +33,8 @@ def test_every_level3_symbol_is_exported():
         for d in "ds":
             for sfx in ("_", "_64_"):
                 assert d + r + sfx in exported
+    for sfx in ("_", "_64_"):
+        assert "zgemm" + sfx in exported and "cgemm" + sfx in exported
 
 
 def test_golden_covers_every_info_code():
@@ -73,3 +76,23 @@ def test_xerbla_lengths_follow_the_reference():
     rec.record_xerbla_reset()
     eb.level3("strsm", "L", "U", "N", "N", 2, 2, 1.0, a, 1, a, 2)
     assert rec.record_xerbla_last_info() == 9 and rec.record_xerbla_last_name().decode() == "STRSM "
+
+
+
+@pytest.mark.parametrize("ilp64", [False, True])
+@pytest.mark.parametrize("dtype", ["z", "c"])
+def test_complex_gemm_argument_errors_match_reference(ilp64, dtype):
+    """zgemm_/cgemm_: the info codes of blas/level3_impl.h:61-78 recorded from the reference."""
+    rec = load_xerbla_recorder()
+    errors = json.loads(bytes(np.load(COMPLEX_GOLDEN)["meta"]).decode())["errors"]
+    assert {e["info"] for e in errors} == {0, 1, 2, 3, 4, 5, 8, 10, 13}
+    sentinel = np.full(64, 7 + 7j, dtype=np.complex128 if dtype == "z" else np.complex64)
+    for e in errors:
+        rec.record_xerbla_reset()
+        eb.complex_gemm(dtype, e["ta"], e["tb"], e["m"], e["n"], e["k"], 1.0, sentinel, e["lda"], sentinel, e["ldb"],
+                        0.0, sentinel, e["ldc"], ilp64=ilp64)
+        got = rec.record_xerbla_last_info() if rec.record_xerbla_calls() else 0
+        assert got == e["info"], e
+        if got:
+            assert rec.record_xerbla_last_name().decode() == dtype.upper() + "GEMM "
+        assert np.all(sentinel == 7 + 7j)
