@@ -497,7 +497,14 @@ struct CrtRecParams {
   const int* skip_if_flag;
   int write_c;
   int cols_per_block;  // columns one block handles per pass (fewer when the grid would be small)
+  int uplo;            // 0: all of C; 1: i <= j only; 2: i >= j only
 };
+
+// The columns [jb, je) of row i within [j0, j1) that the triangle `uplo` keeps.
+__device__ __forceinline__ void triangle_cols(int uplo, int64_t i, int64_t j0, int64_t j1, int64_t& jb, int64_t& je) {
+  jb = (uplo == 1 && j0 < i) ? i : j0;
+  je = (uplo == 2 && j1 > i + 1) ? i + 1 : j1;
+}
 
 // RN(|R|) of a 192-bit magnitude as d * 2^shift, d an integer-valued double < 2^64:
 // the top 64 bits below the leading one, with a sticky bit for everything under them.
@@ -604,8 +611,9 @@ __global__ void __launch_bounds__(256) crt_reconstruct_kernel(const __grid_const
   const int cpb = R.cols_per_block;
   const int64_t jstep = int64_t(gridDim.y) * cpb;
   for (int64_t j0 = int64_t(blockIdx.y) * cpb; i < R.m && j0 < R.ncols; j0 += jstep) {
-    const int64_t j1 = j0 + cpb < R.ncols ? j0 + cpb : R.ncols;
-    for (int64_t j = j0; j < j1; ++j) {
+    int64_t jb, je;
+    triangle_cols(R.uplo, i, j0, j0 + cpb < R.ncols ? j0 + cpb : R.ncols, jb, je);
+    for (int64_t j = jb; j < je; ++j) {
       const uint8_t* rp = R.res + j * R.ld_res + i;
       unsigned long long acc[kCrtLimbs] = {0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
       // unrolled over the largest modulus count: the weights are immediate constant-bank operands
@@ -701,12 +709,14 @@ __global__ void __launch_bounds__(256) crt_reconstruct128_kernel(const __grid_co
   const int cpb = R.cols_per_block;
   const int64_t jstep = int64_t(gridDim.y) * cpb;
   for (int64_t j0 = int64_t(blockIdx.y) * cpb; i < m && j0 < ncols; j0 += jstep) {
-    const int64_t j1 = j0 + cpb < ncols ? j0 + cpb : ncols;
+    int64_t jb, j1;
+    triangle_cols(R.uplo, i, j0, j0 + cpb < ncols ? j0 + cpb : ncols, jb, j1);
+    if (jb >= j1) continue;
     // software pipeline: the residues of column j+1 are loaded while column j is reduced
     uint32_t rn[N];
 #pragma unroll
-    for (int l = 0; l < N; ++l) rn[l] = res[j0 * ld_res + i + l * plane];
-    for (int64_t j = j0; j < j1; ++j) {
+    for (int l = 0; l < N; ++l) rn[l] = res[jb * ld_res + i + l * plane];
+    for (int64_t j = jb; j < j1; ++j) {
       uint32_t rc[N];
 #pragma unroll
       for (int l = 0; l < N; ++l) rc[l] = rn[l];
@@ -788,6 +798,9 @@ cudaError_t launch_gemm_config(const CrtOperand& a, const CrtOperand& b, const C
   P.crt = 1;
   P.residues = args.cres;
   P.ld_res = args.ld_res;
+  P.tile_list = args.tile_list;
+  P.num_listed = args.num_listed;
+  if (P.tile_list && (P.num_listed < 1 || P.num_listed > P.tiles_m * P.tiles_n)) return cudaErrorInvalidValue;
   return launch_slice_gemm<kModeCrtI8, BN, STAGES, 4, PAIR>(tmA, tmB, P, args.num_sms, stream);
 }
 
@@ -795,6 +808,26 @@ cudaError_t launch_gemm_config(const CrtOperand& a, const CrtOperand& b, const C
 
 int64_t crt_tile_rows(int tile_n) { return tile_n == kTilePair ? 256 : 128; }
 int64_t crt_tile_cols(int tile_n) { return tile_n == 128 ? 128 : 256; }
+
+void crt_triangle_tiles(int tile_n, int64_t rows_pad, int64_t cols_pad, int64_t n, bool upper, int group_m, int* out,
+                        int* count) {
+  const int64_t br = crt_tile_rows(tile_n), bc = crt_tile_cols(tile_n);
+  const int tiles_m = int(rows_pad / br), tiles_n = int(cols_pad / bc);
+  const int gm_all = group_m > 0 ? group_m : tiles_m;
+  int c = 0;
+  for (int tile = 0; tile < tiles_m * tiles_n; ++tile) {
+    // the raster of tile_coords() in the GEMM kernel
+    const int group_size = gm_all * tiles_n;
+    const int first_m = (tile / group_size) * gm_all;
+    const int gm = std::min(tiles_m - first_m, gm_all);
+    const int r = tile % group_size;
+    const int64_t r0 = int64_t(first_m + r % gm) * br, c0 = int64_t(r / gm) * bc;
+    // tiles wholly in the padding hold no output
+    const bool meets = r0 < n && c0 < n && (upper ? (r0 <= c0 + bc - 1) : (r0 + br - 1 >= c0));
+    if (meets) out[c++] = tile;
+  }
+  *count = c;
+}
 
 cudaError_t launch_crt_scan_norms(const StridedView<double>& x, const CrtOperand& op, int* nonfinite, double* spread,
                                   cudaStream_t stream) {
@@ -864,6 +897,7 @@ cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t 
   R.err_sq = args.err_sq;
   R.skip_if_flag = args.skip_if_flag;
   R.write_c = args.write_c ? 1 : 0;
+  R.uplo = args.uplo;
   const unsigned gx = unsigned((args.m + 255) / 256);
   // up to kRecCols columns per block, fewer while the grid is under ~4 blocks per SM
   int64_t cpb = int64_t(gx) * args.n / (4 * 148);

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 
 #include "kernels.h"
 #include "mlp.h"
@@ -113,9 +114,15 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   const bool stage2 = picker_weights() != nullptr && (auto_tile || forced == 0);
   const int nmax = (check || stage2) ? std::max(nmod, kCrtMaxModuli) : nmod;
   int tile = (opt.tile_n == kTilePair || opt.tile_n == 256) ? opt.tile_n : choose_crt_tile(cx, m, n);
+  const StridedView<double> va = view_a(ta, A, lda, m, k);
+  const StridedView<double> vb = view_bt(tb, B, ldb, n, k);
+  // op(B)^T == op(A) (a product A A^T, as in syrk): one scan and one split serve both
+  const bool same = m == n && va.ptr == vb.ptr && va.sr == vb.sr && va.sl == vb.sl;
   // rows padded for the pair tile whenever the picker may still choose it
-  const int64_t m_pad = round_up(m, stage2 ? 256 : crt_tile_rows(tile)), n_pad = round_up(n, crt_tile_cols(tile)),
-                k_pad = round_up(k, kOzakiKBlock);
+  const int64_t m_pad = round_up(m, (stage2 || same) ? 256 : crt_tile_rows(tile)),
+                n_pad = round_up(n, crt_tile_cols(tile)), k_pad = round_up(k, kOzakiKBlock);
+  const bool tri = opt.uplo == 1 || opt.uplo == 2;
+  const int64_t max_tiles = (m_pad / 128) * (n_pad / 256);
   size_t off = 0;
   const size_t o_mb_a = off;
   off = align256(off + size_t(m) * 8);
@@ -140,26 +147,31 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   off = align256(off + size_t(nmax) * n_pad * k_pad);
   const size_t o_res_c = off;
   off = align256(off + size_t(nmax) * m_pad * n_pad);
+  // triangle only: the tile list, and the non-finite fallback's full product
+  const size_t o_tiles = off;
+  off = align256(off + (tri ? size_t(max_tiles) * 4 : 0));
+  const size_t o_full = off;
+  off = align256(off + (tri ? size_t(m) * n * 8 : 0));
   if (!cx.ws.ensure(off)) {
     set_error(EB2_ERR_ALLOC, "could not allocate %zu bytes of emulation workspace", off);
     return EB2_ERR_ALLOC;
   }
   uint8_t* ws = static_cast<uint8_t*>(cx.ws.ptr);
-  const StridedView<double> va = view_a(ta, A, lda, m, k);
-  const StridedView<double> vb = view_bt(tb, B, ldb, n, k);
   DeviceFlags* df = cx.dflags;
   CrtOperand oa{reinterpret_cast<int8_t*>(ws + o_res_a), reinterpret_cast<int32_t*>(ws + o_mu_a),
                 reinterpret_cast<uint64_t*>(ws + o_mb_a), reinterpret_cast<uint64_t*>(ws + o_ss_a),
                 reinterpret_cast<int32_t*>(ws + o_ce_a), m, m_pad, k, k_pad, nmax};
-  CrtOperand ob{reinterpret_cast<int8_t*>(ws + o_res_b), reinterpret_cast<int32_t*>(ws + o_mu_b),
-                reinterpret_cast<uint64_t*>(ws + o_mb_b), reinterpret_cast<uint64_t*>(ws + o_ss_b),
-                reinterpret_cast<int32_t*>(ws + o_ce_b), n, n_pad, k, k_pad, nmax};
+  const CrtOperand ob = same ? oa
+                             : CrtOperand{reinterpret_cast<int8_t*>(ws + o_res_b), reinterpret_cast<int32_t*>(ws + o_mu_b),
+                                          reinterpret_cast<uint64_t*>(ws + o_mb_b),
+                                          reinterpret_cast<uint64_t*>(ws + o_ss_b),
+                                          reinterpret_cast<int32_t*>(ws + o_ce_b), n, n_pad, k, k_pad, nmax};
 
   bool ok = check_cuda(cudaMemsetAsync(df, 0, sizeof(DeviceFlags), st), "reset flags");
   ok = ok && check_cuda(launch_crt_scan_norms(va, oa, &df->nonfinite, &df->spread[0], st), "scan A");
-  ok = ok && check_cuda(launch_crt_scan_norms(vb, ob, &df->nonfinite, &df->spread[0], st), "scan B");
+  if (!same) ok = ok && check_cuda(launch_crt_scan_norms(vb, ob, &df->nonfinite, &df->spread[0], st), "scan B");
   if (!ok) return EB2_ERR_CUDA;
-  info.launches = 2;
+  info.launches = same ? 1 : 2;
   if (stage2) {
     if (!check_cuda(cudaMemcpyAsync(cx.hflags, df, sizeof(DeviceFlags), cudaMemcpyDeviceToHost, st), "read scan") ||
         !check_cuda(cudaStreamSynchronize(st), "scan"))
@@ -183,6 +195,18 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   g.num_sms = cx.num_sms;
   g.cres = ws + o_res_c;
   g.ld_res = m_pad;
+  if (tri) {
+    // the tiles meeting the triangle, in the kernel's raster order
+    std::vector<int> tiles(static_cast<size_t>(max_tiles));
+    int count = 0;
+    crt_triangle_tiles(tile, m_pad, n_pad, m, opt.uplo == 1, tuning().group_m, tiles.data(), &count);
+    int* dtiles = reinterpret_cast<int*>(ws + o_tiles);
+    if (!check_cuda(cudaMemcpyAsync(dtiles, tiles.data(), size_t(count) * 4, cudaMemcpyHostToDevice, st),
+                    "tile list"))
+      return EB2_ERR_CUDA;
+    g.tile_list = dtiles;
+    g.num_listed = count;
+  }
   CrtReconstructArgs r{};
   r.m = m;
   r.n = n;
@@ -197,11 +221,12 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   r.mu_b = ob.mu;
   r.err_sq = df->err_sq;
   r.skip_if_flag = &df->nonfinite;
+  r.uplo = tri ? opt.uplo : 0;
   // with beta != 0 and the check on, C is written only once the estimate has passed
   const bool deferred = check && beta != 0.0;
   auto product = [&](bool first) -> bool {
     bool good = check_cuda(launch_crt_split(va, oa, nmod, st), "residues A");
-    good = good && check_cuda(launch_crt_split(vb, ob, nmod, st), "residues B");
+    if (!same) good = good && check_cuda(launch_crt_split(vb, ob, nmod, st), "residues B");
     g.moduli = r.moduli = nmod;
     if (first && opt.timed) cudaEventRecord(cx.ev_gemm0, st);
     good = good && check_cuda(launch_crt_gemm(oa, ob, g, st), "CRT GEMM");
@@ -212,12 +237,23 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
     return good;
   };
   ok = product(true);
-  // IEEE semantics for NaN/Inf inputs: the FP64 kernel runs only when the scan saw one.
-  ok = ok && check_cuda(launch_dgemm_native(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, &df->nonfinite,
-                                            st),
-                        "non-finite fallback");
+  // IEEE semantics for NaN/Inf inputs: the FP64 kernel runs only when the scan saw one
+  // (for a triangle into the workspace, then merged into the triangle).
+  if (!tri) {
+    ok = ok && check_cuda(launch_dgemm_native(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, &df->nonfinite,
+                                              st),
+                          "non-finite fallback");
+    info.launches += 1;
+  } else {
+    double* full = reinterpret_cast<double*>(ws + o_full);
+    ok = ok && check_cuda(launch_dgemm_native(ta, tb, m, n, k, alpha, A, lda, B, ldb, 0.0, full, m, &df->nonfinite,
+                                              st),
+                          "non-finite fallback");
+    ok = ok && check_cuda(launch_merge_triangle<double>(full, m, n, opt.uplo == 1, beta, C, ldc, st, &df->nonfinite),
+                          "non-finite merge");
+    info.launches += 2;
+  }
   if (!ok) return EB2_ERR_CUDA;
-  info.launches += 1;
   info.slices = nmod;
   info.tile_n = tile;
   auto finish_timing = [&](bool gemm_timed) {
@@ -293,6 +329,10 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   info.spread = 0.0;
   set_pending_timing(nullptr, false);
   if (m == 0 || n == 0) return EB2_OK;
+  if (opt.uplo != 0 && (m != n || opt.method != EB2_METHOD_CRT || k == 0 || alpha == 0.0)) {
+    set_error(EB2_ERR_ARG, "a triangle-only product needs m == n, k > 0, alpha != 0 and the CRT method");
+    return EB2_ERR_ARG;
+  }
   if (k == 0 || alpha == 0.0) {
     info.method = EB2_METHOD_NATIVE;
     if (beta == 1.0) return EB2_OK;

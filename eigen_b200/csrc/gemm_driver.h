@@ -17,6 +17,8 @@ struct DgemmOptions {
   bool check_accuracy = true;  // a-posteriori estimate + added slices (needs a host sync)
   bool sync = true;      // wait for the stream before returning
   bool timed = false;    // record kernel time in call_info
+  int uplo = 0;          // CRT only, m == n: 1 = compute and write only C's upper triangle
+                         // (i <= j), 2 = only the lower (i >= j); the other is not touched
 };
 
 struct SgemmOptions {

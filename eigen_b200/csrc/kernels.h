@@ -137,6 +137,8 @@ struct CrtGemmArgs {
   int num_sms;
   uint8_t* cres;   // [moduli][n_pad][ld_res] residues of C' (uint8 in [0, p))
   int64_t ld_res;  // = a.rows_pad
+  const int* tile_list = nullptr;  // device: the output tiles to compute (null: all)
+  int num_listed = 0;
 };
 cudaError_t launch_crt_gemm(const CrtOperand& a, const CrtOperand& b, const CrtGemmArgs& args, cudaStream_t stream);
 
@@ -153,6 +155,7 @@ struct CrtReconstructArgs {
   double* err_sq;  // [2]: += estimated squared error, += squared alpha*A*B entries (may be null)
   const int* skip_if_flag;
   bool write_c;    // false: only the estimate
+  int uplo = 0;    // 0: all of C; 1: only i <= j (upper triangle); 2: only i >= j (lower)
 };
 cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t stream);
 
@@ -186,11 +189,21 @@ constexpr int kTriVecs = 64;   // vectors per CTA of launch_tri_block
 template <typename T>
 cudaError_t launch_expand_symmetric(const T* A, int64_t lda, int64_t n, bool upper, T* out, int64_t ldo,
                                     cudaStream_t stream);
+// out (n x n) = the triangular matrix in the triangle `upper` (else lower) of A, zeros
+// elsewhere, ones on the diagonal if `unit` (the stored diagonal then unread).
+template <typename T>
+cudaError_t launch_expand_triangular(const T* A, int64_t lda, int64_t n, bool upper, bool unit, T* out, int64_t ldo,
+                                     cudaStream_t stream);
 // On the triangle `upper` of the n x n C only: C = P + beta C (beta == 0 does not read C;
 // P == null: C = beta C, beta == 0 writing zeros).
 template <typename T>
 cudaError_t launch_merge_triangle(const T* P, int64_t ldp, int64_t n, bool upper, T beta, T* C, int64_t ldc,
-                                  cudaStream_t stream);
+                                  cudaStream_t stream, const int* only_if_flag = nullptr);
+// The tiles of the CRT GEMM's raster (configuration `tile_n` over rows_pad x cols_pad, raster
+// groups of group_m tile rows, 0 = all) that meet the triangle `upper` / lower of the n x n C,
+// in raster order.
+void crt_triangle_tiles(int tile_n, int64_t rows_pad, int64_t cols_pad, int64_t n, bool upper, int group_m, int* out,
+                        int* count);
 // X = alpha X by plain multiplication (NaN/Inf stay for alpha == 0).
 template <typename T>
 cudaError_t launch_multiply(int64_t m, int64_t n, T alpha, T* X, int64_t ldx, cudaStream_t stream);

@@ -11,14 +11,19 @@
 // is one device GEMM call (so DGEMM sub-products take the emulated or native FP64 kernels
 // the method setting and picker choose), with the triangles handled by the kernels of
 // tri.cu:
-//   gemmtr / syrk / syr2k  the n x n triangle split in two halves: the off-diagonal block
-//                          is one GEMM straight into C, the two diagonal halves recurse;
-//                          a diagonal block of at most kTrLeaf is a full GEMM into a
-//                          workspace merged into C's triangle;
+//   gemmtr / syrk / syr2k  with the CRT emulation, one product restricted to the output
+//                          tiles that meet C's triangle (its GEMM launch walks only those
+//                          tiles; the reconstruction writes only the triangle; A A^T splits
+//                          A once); otherwise the triangle split in two halves: the
+//                          off-diagonal block is one GEMM straight into C, the two diagonal
+//                          halves recurse, and a diagonal block of at most kTrLeaf is a full
+//                          GEMM into a workspace merged into C's triangle;
 //   symm                   the symmetric operand expanded to a full matrix, then one GEMM;
-//   trmm / trsm            the triangular operand split in two halves: one GEMM for the
-//                          off-diagonal block, recursion on the diagonal halves, and a
-//                          shared-memory substitution (or multiply) kernel for diagonal
+//   trmm                   with an emulated GEMM and size >= 1024, one product with the
+//                          triangle expanded into a workspace (zeros, unit diagonal);
+//   trmm / trsm            otherwise the triangular operand split in two halves: one GEMM
+//                          for the off-diagonal block, recursion on the diagonal halves, and
+//                          a shared-memory substitution (or multiply) kernel for diagonal
 //                          blocks of at most kTriBlock.
 // Host operands are staged through device buffers; device or managed operands are used in
 // place.  The calls are synchronous.
@@ -122,14 +127,19 @@ bool cuda_ok(cudaError_t e, const char* what) {
 // C = alpha op(A) op(B) + beta C on device pointers, queued on st.  DGEMM sub-products keep
 // the a-posteriori accuracy check of the emulated methods (which waits for its flags);
 // native products are only queued.
+// uplo != 0: the CRT product of only C's upper (1) or lower (2) triangle (m == n).
 int gemm(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
          int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc, cudaStream_t st,
-         Summary& sum) {
+         Summary& sum, int uplo = 0) {
   if (m == 0 || n == 0) return EB2_OK;
   DgemmOptions o;
   o.sync = false;
   o.check_accuracy = true;
   o.timed = false;
+  if (uplo) {
+    o.method = EB2_METHOD_CRT;
+    o.uplo = uplo;
+  }
   eb2_call_info ci{};
   const int rc = dgemm_on_device(cx, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, st, o, ci);
   const int64_t flops = m * n * k;
@@ -198,6 +208,11 @@ int gemmtr_device(Context& cx, bool upper, bool ta, bool tb, int64_t n, int64_t 
     return cuda_ok(launch_merge_triangle<T>(nullptr, 0, n, upper, beta, C, ldc, st), "scale triangle") ? EB2_OK
                                                                                                      : EB2_ERR_CUDA;
   }
+  if constexpr (sizeof(T) == 8) {
+    // the CRT product computes only the tiles that meet the triangle: one call, one split
+    if (resolve_dgemm_method(n, n, k) == EB2_METHOD_CRT)
+      return gemm(cx, ta, tb, n, n, k, alpha, A, lda, B, ldb, beta, C, ldc, st, sum, upper ? 1 : 2);
+  }
   const int64_t leaf = std::min(n, kTrLeaf);
   if (!cx.tmp.ensure(size_t(leaf) * size_t(leaf) * sizeof(T))) {
     set_error(EB2_ERR_ALLOC, "could not allocate the diagonal-block workspace");
@@ -252,6 +267,15 @@ int symm_device(Context& cx, bool left, bool upper, int64_t m, int64_t n, T alph
               : gemm(cx, false, false, m, n, n, alpha, B, ldb, S, size, beta, C, ldc, st, sum);
 }
 
+// trmm as one product with the expanded triangle: where the emulated GEMM runs (its rate
+// more than pays for the doubled flops and removes the recursion's many small calls).
+template <typename T>
+bool trmm_as_one_product(int64_t size, int64_t m, int64_t n) {
+  if (size < 1024) return false;
+  if constexpr (sizeof(T) == 8) return resolve_dgemm_method(m, n, size) == EB2_METHOD_CRT;
+  return settings().sgemm_method.load() != EB2_METHOD_NATIVE;
+}
+
 // In place on the m x n B: B := op(A)^-1 B / B op(A)^-1 (solve) or op(A) B / B op(A)
 // (multiply), A triangular (triangle `upper` stored, unit diagonal if `unit`), then
 // B := alpha B.
@@ -259,6 +283,27 @@ template <typename T>
 int trxm_device(Context& cx, bool solve, bool left, bool upper, bool trans, bool unit, int64_t m, int64_t n, T alpha,
                 const T* A, int64_t lda, T* B, int64_t ldb, cudaStream_t st, Summary& sum) {
   if (m == 0 || n == 0) return EB2_OK;
+  if (!solve && alpha != T(0) && trmm_as_one_product<T>(left ? m : n, m, n)) {
+    // one GEMM with the triangle expanded (zeros, unit diagonal) into a workspace, out of
+    // place, then copied back: twice the flops of the recursion, but a single large product
+    const int64_t size = left ? m : n;
+    if (!cx.tmp.ensure((size_t(size) * size + size_t(m) * n) * sizeof(T))) {
+      set_error(EB2_ERR_ALLOC, "could not allocate the triangular-product workspace");
+      return EB2_ERR_ALLOC;
+    }
+    T* Tf = static_cast<T*>(cx.tmp.ptr);
+    T* P = Tf + size_t(size) * size;
+    if (!cuda_ok(launch_expand_triangular<T>(A, lda, size, upper, unit, Tf, size, st), "expand")) return EB2_ERR_CUDA;
+    sum.launches += 1;
+    const int rc = left ? gemm(cx, trans, false, m, n, m, alpha, Tf, size, B, ldb, T(0), P, m, st, sum)
+                        : gemm(cx, false, trans, m, n, n, alpha, B, ldb, Tf, size, T(0), P, m, st, sum);
+    if (rc != EB2_OK && rc != EB2_ERR_ACCURACY) return rc;
+    if (!cuda_ok(cudaMemcpy2DAsync(B, size_t(ldb) * sizeof(T), P, size_t(m) * sizeof(T), size_t(m) * sizeof(T),
+                                   size_t(n), cudaMemcpyDeviceToDevice, st),
+                 "copy back"))
+      return EB2_ERR_CUDA;
+    return rc;
+  }
   // M = op(A); `lower` is M's triangle
   const bool lower = trans ? upper : !upper;
   // block M[r0.., c0..] as a GEMM operand (with transpose flag `trans`)

@@ -79,6 +79,8 @@ struct SliceGemmParams {
   int crt;               // 1: CRT mode (unit t = modulus t, one slice pair (t, t))
   uint8_t* residues;     // CRT: [moduli][cols][ld_res] residue planes (uint8 in [0, p))
   int64_t ld_res;        // CRT: rows of one residue plane (padded m)
+  const int* tile_list;  // CRT: the tiles to compute (indices of the full raster), or null for all
+  int num_listed;        // CRT: entries of tile_list
 };
 
 // Pair range of diagonal t: p = p_lo .. p_lo + total/num_kb - 1 (q = t - p).
@@ -110,13 +112,15 @@ __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, 
 // Work items: one per output tile, or in CRT mode one per (tile, modulus): the moduli are
 // independent products, so small outputs still spread over the SMs, and the items in
 // flight at any time share one modulus (its residue planes stay in L2).
+// A tile list restricts a CRT launch to some tiles (the triangle of C of a gemmtr / syrk).
 __host__ __device__ __forceinline__ int num_work(const SliceGemmParams& P) {
+  if (P.crt && P.tile_list) return P.num_listed * P.slices;
   return P.tiles_m * P.tiles_n * (P.crt ? P.slices : 1);
 }
 __device__ __forceinline__ void work_item(const SliceGemmParams& P, int w, int& tile, int& t_hi, int& t_lo) {
   if (P.crt) {
-    const int nt = P.tiles_m * P.tiles_n;
-    tile = w % nt;
+    const int nt = P.tile_list ? P.num_listed : P.tiles_m * P.tiles_n;
+    tile = P.tile_list ? P.tile_list[w % nt] : w % nt;
     t_hi = t_lo = w / nt;
   } else {
     tile = w;

@@ -1,5 +1,5 @@
 // tri.cu -- the element-wise kernels the symmetric and triangular level-3 routines need
-// around the GEMM: expanding a stored symmetric triangle into a full matrix, merging a
+// around the GEMM: expanding a stored symmetric or triangular matrix into a full one, merging a
 // product into one triangle of C, scaling a triangle or a matrix, and applying a small
 // triangular diagonal block (multiply or solve) to a panel in place.
 //
@@ -54,12 +54,33 @@ __global__ void expand_symmetric_kernel(const T* __restrict__ A, int64_t lda, in
   }
 }
 
+// out (n x n, ld ldo) = the triangular matrix stored in the triangle `upper` of A: A(i,j)
+// inside the triangle, 0 outside, 1 on the diagonal when `unit` (then the stored diagonal is
+// not read).
+template <typename T>
+__global__ void expand_triangular_kernel(const T* __restrict__ A, int64_t lda, int64_t n, bool upper, bool unit,
+                                         T* __restrict__ out, int64_t ldo) {
+  const int64_t bi = int64_t(blockIdx.x) * kTile, bj = int64_t(blockIdx.y) * kTile;
+  for (int q = 0; q < kRowsPerThread; ++q) {
+    const int64_t i = bi + threadIdx.x, j = bj + threadIdx.y + 8 * q;
+    if (i >= n || j >= n) continue;
+    T v = T(0);
+    if (i == j)
+      v = unit ? T(1) : A[i + j * lda];
+    else if (in_triangle(i, j, upper))
+      v = A[i + j * lda];
+    out[i + j * ldo] = v;
+  }
+}
+
 // C(i,j) = P(i,j) + beta C(i,j) on the triangle `upper` of the n x n C; beta == 0 writes P
 // and never reads C; P == null stands for a zero product (C := beta C, beta == 0 writing
-// exact zeros).  The other triangle is not touched.
+// exact zeros).  The other triangle is not touched.  With `only_if_flag` the kernel does
+// nothing unless *only_if_flag != 0.
 template <typename T>
 __global__ void merge_triangle_kernel(const T* __restrict__ P, int64_t ldp, int64_t n, bool upper, T beta,
-                                      T* __restrict__ C, int64_t ldc) {
+                                      T* __restrict__ C, int64_t ldc, const int* only_if_flag) {
+  if (only_if_flag && *only_if_flag == 0) return;
   const int64_t bi = int64_t(blockIdx.x) * kTile, bj = int64_t(blockIdx.y) * kTile;
   for (int q = 0; q < kRowsPerThread; ++q) {
     const int64_t i = bi + threadIdx.x, j = bj + threadIdx.y + 8 * q;
@@ -177,11 +198,20 @@ cudaError_t launch_expand_symmetric(const T* A, int64_t lda, int64_t n, bool upp
 }
 
 template <typename T>
-cudaError_t launch_merge_triangle(const T* P, int64_t ldp, int64_t n, bool upper, T beta, T* C, int64_t ldc,
-                                  cudaStream_t st) {
+cudaError_t launch_expand_triangular(const T* A, int64_t lda, int64_t n, bool upper, bool unit, T* out, int64_t ldo,
+                                     cudaStream_t st) {
   if (n == 0) return cudaSuccess;
   if (!grid_fits(n, n)) return cudaErrorInvalidConfiguration;
-  merge_triangle_kernel<T><<<tile_grid(n, n), dim3(kTile, 8), 0, st>>>(P, ldp, n, upper, beta, C, ldc);
+  expand_triangular_kernel<T><<<tile_grid(n, n), dim3(kTile, 8), 0, st>>>(A, lda, n, upper, unit, out, ldo);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_merge_triangle(const T* P, int64_t ldp, int64_t n, bool upper, T beta, T* C, int64_t ldc,
+                                  cudaStream_t st, const int* only_if_flag) {
+  if (n == 0) return cudaSuccess;
+  if (!grid_fits(n, n)) return cudaErrorInvalidConfiguration;
+  merge_triangle_kernel<T><<<tile_grid(n, n), dim3(kTile, 8), 0, st>>>(P, ldp, n, upper, beta, C, ldc, only_if_flag);
   return cudaGetLastError();
 }
 
@@ -215,7 +245,10 @@ cudaError_t launch_tri_block(bool solve, const T* E, int64_t er, int64_t ec, int
 
 #define EB2_TRI_INSTANTIATE(T)                                                                                     \
   template cudaError_t launch_expand_symmetric<T>(const T*, int64_t, int64_t, bool, T*, int64_t, cudaStream_t);     \
-  template cudaError_t launch_merge_triangle<T>(const T*, int64_t, int64_t, bool, T, T*, int64_t, cudaStream_t);    \
+  template cudaError_t launch_expand_triangular<T>(const T*, int64_t, int64_t, bool, bool, T*, int64_t,             \
+                                                   cudaStream_t);                                                  \
+  template cudaError_t launch_merge_triangle<T>(const T*, int64_t, int64_t, bool, T, T*, int64_t, cudaStream_t,    \
+                                                const int*);                                                       \
   template cudaError_t launch_multiply<T>(int64_t, int64_t, T, T*, int64_t, cudaStream_t);                          \
   template cudaError_t launch_tri_block<T>(bool, const T*, int64_t, int64_t, int, bool, bool, T*, int64_t, int64_t, \
                                            int64_t, cudaStream_t);

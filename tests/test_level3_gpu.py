@@ -314,7 +314,8 @@ BIG = [("gemmtr", "UNN", (1500, 700)), ("gemmtr", "LTN", (1500, 700)), ("gemmtr"
        ("syr2k", "LN", (1100, 300)), ("syr2k", "UT", (1030, 200)), ("symm", "LU", (700, 500)),
        ("symm", "RL", (300, 900))]
 TRI = [(r, s + u + t + d, dims) for r in ("trmm", "trsm") for s in "LR" for u in "UL" for t in "NT" for d in "NU"
-       for dims in ((300, 200),)] + [("trsm", "LLNN", (700, 200)), ("trmm", "RUTN", (500, 1000))]
+       for dims in ((300, 200),)] + [("trsm", "LLNN", (700, 200)), ("trmm", "RUTN", (500, 1000)),
+                                   ("trmm", "LUNU", (1100, 300)), ("trmm", "RLTN", (200, 1300))]
 
 
 @pytest.mark.parametrize("routine,chars,dims", BIG + TRI)
@@ -387,3 +388,73 @@ def test_trsm_alpha_applied_after_the_solve():
     B[5, 3] = np.inf
     eb.level3("dtrsm", "L", "L", "N", "N", m, n, 0.0, A, m, B, m)
     assert np.isnan(B[5, 3]) and np.all(B[:5, :] == 0.0) and np.all(np.isnan(B[5:, 3]) | (B[5:, 3] == 0.0))
+
+
+# ------------------------------------------------------------------ the CRT triangle product
+@pytest.mark.parametrize("tile_n", [256, 512])
+@pytest.mark.parametrize("n,k,uplo,trans,group", [(700, 300, "L", "N", 0), (1024, 512, "U", "T", 0),
+                                                  (1500, 257, "U", "N", 3), (2100, 1000, "L", "T", 2)])
+def test_crt_syrk_is_the_triangle_of_the_full_product(tile_n, n, k, uplo, trans, group):
+    """dsyrk on the CRT path computes only the tiles meeting the triangle (one split of A serves
+    both operands): bit for bit the triangle of the full CRT product of A and a separate copy of
+    A, the other triangle untouched."""
+    eb.set_dgemm_method(eb.METHOD_CRT)
+    eb.set_dgemm_moduli(16)
+    eb.set_tile_n(tile_n)
+    eb.set_slice_tuning(group, 0)
+    try:
+        rng = np.random.default_rng(n + k)
+        rows, cols = (n, k) if trans == "N" else (k, n)
+        A = np.asfortranarray(rng.uniform(-1, 1, (rows + 2, cols)))
+        C = np.asfortranarray(rng.uniform(-1, 1, (n + 1, n)))
+        up = np.triu(np.ones((n, n), bool)) if uplo == "U" else np.tril(np.ones((n, n), bool))
+        C[:n, :n][~up] = np.nan
+        got = C.copy(order="F")
+        eb.level3("dsyrk", uplo, trans, n, k, 0.75, A, rows + 2, -0.5, got, n + 1)
+        assert eb.last_error()[0] == eb.EB2_OK, eb.last_error()
+        info = eb.last_call_info()
+        assert info["method"] == eb.METHOD_CRT and info["slices"] == 16
+        full = C.copy(order="F")
+        full[:n, :n][~up] = 0.0
+        A2 = A.copy(order="F")  # a distinct operand: the general two-operand path
+        ta, tb = ("N", "T") if trans == "N" else ("T", "N")
+        eb.dgemm(ta, tb, n, n, k, 0.75, A, rows + 2, A2, rows + 2, -0.5, full, n + 1)
+        np.testing.assert_array_equal(got[:n, :n][up], full[:n, :n][up])
+        np.testing.assert_array_equal(got[:n, :n][~up], C[:n, :n][~up])
+        np.testing.assert_array_equal(got[n:], C[n:])
+        # the device entry with one tensor in both roles: bit for bit the two-operand product
+        dA = torch.from_numpy(np.ascontiguousarray(A.T)).cuda()
+        dC = torch.from_numpy(np.ascontiguousarray(np.where(np.isnan(C), 0.0, C).T)).cuda()
+        dC[:n, :n][torch.from_numpy(~up.T).cuda()] = 0.0
+        rc = eb.dgemm_device(ta, tb, n, n, k, 0.75, dA, rows + 2, dA, rows + 2, -0.5, dC, n + 1)
+        torch.cuda.synchronize()
+        assert rc == eb.EB2_OK, eb.last_error()
+        np.testing.assert_array_equal(np.asfortranarray(dC.cpu().numpy().T)[:n], full[:n])
+    finally:
+        eb.set_dgemm_moduli(0)
+        eb.set_tile_n(0)
+        eb.set_slice_tuning(0, 0)
+
+
+def test_crt_syrk_nonfinite_input_keeps_the_other_triangle():
+    """A NaN in A sends the triangle product to the FP64 kernel (into a workspace, merged into
+    the triangle): the other triangle stays untouched, the NaN row and column propagate."""
+    eb.set_dgemm_method(eb.METHOD_CRT)
+    n, k = 600, 400
+    rng = np.random.default_rng(5)
+    A = np.asfortranarray(rng.uniform(-1, 1, (n, k)))
+    A[17, 3] = np.nan
+    C = np.asfortranarray(rng.uniform(-1, 1, (n, n)))
+    got = C.copy(order="F")
+    eb.level3("dsyrk", "L", "N", n, k, 1.0, A, n, 1.0, got, n)
+    assert eb.last_call_info()["nonfinite"] == 1
+    low = np.tril(np.ones((n, n), bool))
+    np.testing.assert_array_equal(got[~low], C[~low])
+    nan_rows = np.isnan(got)
+    expect = np.zeros((n, n), bool)
+    expect[17, :] = True
+    expect[:, 17] = True
+    np.testing.assert_array_equal(nan_rows, expect & low)
+    want = C + A @ A.T
+    fin = low & ~expect
+    assert np.max(np.abs(got[fin] - want[fin])) < 1e-12
