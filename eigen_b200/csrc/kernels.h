@@ -183,8 +183,8 @@ cudaError_t launch_sgemm_split_bf16(const Bf16Operand& a, const Bf16Operand& b, 
                                     cudaStream_t stream);
 
 // ------------------------------------------------------------ triangles (level-3 routines)
-constexpr int kTriBlock = 64;  // largest diagonal block launch_tri_block takes
-constexpr int kTriVecs = 64;   // vectors per CTA of launch_tri_block
+constexpr int kTriBlock = 64;  // largest diagonal block launch_tri_block_multiply takes
+constexpr int kTriVecs = 64;   // vectors per CTA of launch_tri_block_multiply
 // out (n x n) = the symmetric matrix whose triangle `upper` (else lower) is stored in A.
 template <typename T>
 cudaError_t launch_expand_symmetric(const T* A, int64_t lda, int64_t n, bool upper, T* out, int64_t ldo,
@@ -207,12 +207,19 @@ void crt_triangle_tiles(int tile_n, int64_t rows_pad, int64_t cols_pad, int64_t 
 // X = alpha X by plain multiplication (NaN/Inf stay for alpha == 0).
 template <typename T>
 cudaError_t launch_multiply(int64_t m, int64_t n, T alpha, T* X, int64_t ldx, cudaStream_t stream);
-// x := E^-1 x (solve) or E x for `count` vectors (element r of vector t at X[r*vs + t*ts]),
-// E the nb x nb (nb <= kTriBlock) triangle `lower`/upper at E[r*er + c*ec], unit diagonal
-// if `unit` (then the stored diagonal is not read; neither is the other triangle).
+// x := E x for `count` vectors (element r of vector t at X[r*vs + t*ts]), E the nb x nb
+// (nb <= kTriBlock) triangle `lower`/upper at E[r*er + c*ec], unit diagonal if `unit` (then
+// the stored diagonal is not read; neither is the other triangle).
 template <typename T>
-cudaError_t launch_tri_block(bool solve, const T* E, int64_t er, int64_t ec, int nb, bool lower, bool unit, T* X,
-                             int64_t vs, int64_t ts, int64_t count, cudaStream_t stream);
+cudaError_t launch_tri_block_multiply(const T* E, int64_t er, int64_t ec, int nb, bool lower, bool unit, T* X,
+                                      int64_t vs, int64_t ts, int64_t count, cudaStream_t stream);
+constexpr int kPanelMax = 256;  // largest diagonal block launch_tri_panel_solve takes
+constexpr int kPanelVecs = 64;  // vectors per CTA of launch_tri_panel_solve
+// x := E^-1 x for `count` vectors laid out as for launch_tri_block_multiply, E the nb x nb
+// (nb <= kPanelMax) triangle, by blocked substitution.
+template <typename T>
+cudaError_t launch_tri_panel_solve(const T* E, int64_t er, int64_t ec, int nb, bool lower, bool unit, T* X,
+                                   int64_t vs, int64_t ts, int64_t count, cudaStream_t stream);
 
 // ------------------------------------------------------------ complex GEMM (two real products)
 // op(X) (rows x cols complex; element (r, c) at complex index r*sr + c*sc of the interleaved

@@ -23,8 +23,9 @@
 //                          triangle expanded into a workspace (zeros, unit diagonal);
 //   trmm / trsm            otherwise the triangular operand split in two halves: one GEMM
 //                          for the off-diagonal block, recursion on the diagonal halves, and
-//                          a shared-memory substitution (or multiply) kernel for diagonal
-//                          blocks of at most kTriBlock.
+//                          a shared-memory kernel for the diagonal blocks: a blocked
+//                          substitution over blocks of up to kPanelMax rows (trsm), a
+//                          multiply over blocks of up to kTriBlock (trmm).
 // Host operands are staged through device buffers; device or managed operands are used in
 // place.  The calls are synchronous.
 #include <cuda_runtime.h>
@@ -314,11 +315,14 @@ int trxm_device(Context& cx, bool solve, bool left, bool upper, bool trans, bool
     const T* D = A + i0 + i0 * lda;  // diagonal block of A (and of M)
     // M(r, c) of the block at D[r*mr + c*mc]
     const int64_t mr = trans ? lda : 1, mc = trans ? 1 : lda;
-    cudaError_t e;
-    if (left)  // vectors: the columns of B's rows [i0, i0+nb)
-      e = launch_tri_block<T>(solve, D, mr, mc, int(nb), lower, unit, B + i0, 1, ldb, n, st);
-    else  // x M = b is M^T x^T = b^T; vectors: the rows of B's columns [i0, i0+nb)
-      e = launch_tri_block<T>(solve, D, mc, mr, int(nb), !lower, unit, B + i0 * ldb, ldb, 1, m, st);
+    // vectors: the columns of B's rows [i0, i0+nb) (left), or the rows of B's columns
+    // [i0, i0+nb) (right: x M = b is M^T x^T = b^T)
+    const int64_t er = left ? mr : mc, ec = left ? mc : mr;
+    const bool elower = left ? lower : !lower;
+    T* X = left ? B + i0 : B + i0 * ldb;
+    const int64_t vs = left ? 1 : ldb, ts = left ? ldb : 1, count = left ? n : m;
+    const cudaError_t e = solve ? launch_tri_panel_solve<T>(D, er, ec, int(nb), elower, unit, X, vs, ts, count, st)
+                                : launch_tri_block_multiply<T>(D, er, ec, int(nb), elower, unit, X, vs, ts, count, st);
     if (!cuda_ok(e, "triangular block")) {
       worst = EB2_ERR_CUDA;
       return false;
@@ -333,9 +337,12 @@ int trxm_device(Context& cx, bool solve, bool left, bool upper, bool trans, bool
                                B + d0 * ldb, ldb, st, sum);
     return keep_going(rc, worst);
   };
+  // diagonal blocks: up to kPanelMax rows for the solve (one launch per block, all of its
+  // vectors resident in shared memory), kTriBlock for the multiply
+  const int64_t leaf_max = solve ? kPanelMax : kTriBlock;
   std::function<bool(int64_t, int64_t)> rec = [&](int64_t i0, int64_t size) -> bool {
-    if (size <= kTriBlock) return leaf(i0, size);
-    const int64_t h = (size / 2 + kTriBlock - 1) / kTriBlock * kTriBlock;
+    if (size <= leaf_max) return leaf(i0, size);
+    const int64_t h = (size / 2 + leaf_max - 1) / leaf_max * leaf_max;
     const int64_t a0 = i0, an = h, b0 = i0 + h, bn = size - h;
     // The first half in the order below is the one whose new values the update does not
     // need (solve) or whose old values it still needs (multiply).

@@ -1,14 +1,14 @@
 // tri.cu -- the element-wise kernels the symmetric and triangular level-3 routines need
 // around the GEMM: expanding a stored symmetric or triangular matrix into a full one, merging a
-// product into one triangle of C, scaling a triangle or a matrix, and applying a small
-// triangular diagonal block (multiply or solve) to a panel in place.
+// product into one triangle of C, scaling a triangle or a matrix, and applying a triangular
+// diagonal block to a panel in place (a multiply, or a solve by blocked substitution).
 //
 // Eigen's routines (blas/level3_impl.h:98-760) feed the GEBP kernel through triangular and
 // self-adjoint packing (GeneralMatrixMatrixTriangular.h, SelfadjointMatrixMatrix.h,
 // TriangularMatrixMatrix.h, TriangularSolverMatrix.h).  Here every product of any size goes
 // through the device GEMM, and these kernels handle the triangles: they are memory-bound
 // (expand, merge, scale: one read and one write per element) or, for the diagonal blocks,
-// small (kTriBlock x kTriBlock) in shared memory.
+// work on vectors staged in shared memory.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -102,17 +102,16 @@ __global__ void multiply_kernel(int64_t m, int64_t n, T alpha, T* __restrict__ X
   }
 }
 
-// The triangular block E (nb x nb, nb <= kTriBlock, element (r, c) at E[r*er + c*ec]; the
-// triangle `lower` or upper is used, the diagonal is taken as 1 when `unit`) applied in
-// place to `count` vectors x (element r of vector t at X[r*vs + t*ts]):
-//   kSolve: x := E^-1 x by substitution;  otherwise x := E x.
-// One thread per vector; E and a tile of kTriVecs vectors are staged in shared memory with
-// coalesced loads and stores (the vector index runs fastest when ts == 1, the element index
-// otherwise).
-template <typename T, bool kSolve>
-__global__ void __launch_bounds__(kTriVecs) tri_block_kernel(const T* __restrict__ E, int64_t er, int64_t ec, int nb,
-                                                             bool lower, bool unit, T* __restrict__ X, int64_t vs,
-                                                             int64_t ts, int64_t count) {
+// x := E x in place for `count` vectors x (element r of vector t at X[r*vs + t*ts]), E the
+// triangular block (nb x nb, nb <= kTriBlock, element (r, c) at E[r*er + c*ec]; the triangle
+// `lower` or upper is used, the diagonal is taken as 1 when `unit`).  One thread per vector;
+// E and a tile of kTriVecs vectors are staged in shared memory with coalesced loads and stores
+// (the vector index runs fastest when ts == 1, the element index otherwise).
+template <typename T>
+__global__ void __launch_bounds__(kTriVecs) tri_block_multiply_kernel(const T* __restrict__ E, int64_t er, int64_t ec,
+                                                                      int nb, bool lower, bool unit,
+                                                                      T* __restrict__ X, int64_t vs, int64_t ts,
+                                                                      int64_t count) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* Es = reinterpret_cast<T*>(smem_raw);  // [nb][nb]
   T* Xs = Es + nb * nb;                    // [nb][kTriVecs + 1], Xs[r * (kTriVecs+1) + t]
@@ -138,35 +137,19 @@ __global__ void __launch_bounds__(kTriVecs) tri_block_kernel(const T* __restrict
   __syncthreads();
   if (tid < nv) {
     T* x = Xs + tid;
-    if (kSolve) {
-      if (lower) {
-        for (int r = 0; r < nb; ++r) {
-          T s = x[r * kXld];
-          for (int c = 0; c < r; ++c) s = fma_rn(-Es[r * nb + c], x[c * kXld], s);
-          x[r * kXld] = unit ? s : s / Es[r * nb + r];
-        }
-      } else {
-        for (int r = nb - 1; r >= 0; --r) {
-          T s = x[r * kXld];
-          for (int c = r + 1; c < nb; ++c) s = fma_rn(-Es[r * nb + c], x[c * kXld], s);
-          x[r * kXld] = unit ? s : s / Es[r * nb + r];
-        }
+    // each new x[r] uses only entries that are still old: descending rows for a lower
+    // triangle, ascending for an upper one
+    if (lower) {
+      for (int r = nb - 1; r >= 0; --r) {
+        T s = Es[r * nb + r] * x[r * kXld];
+        for (int c = 0; c < r; ++c) s = fma_rn(Es[r * nb + c], x[c * kXld], s);
+        x[r * kXld] = s;
       }
     } else {
-      // each new x[r] uses only entries that are still old: descending rows for a lower
-      // triangle, ascending for an upper one
-      if (lower) {
-        for (int r = nb - 1; r >= 0; --r) {
-          T s = Es[r * nb + r] * x[r * kXld];
-          for (int c = 0; c < r; ++c) s = fma_rn(Es[r * nb + c], x[c * kXld], s);
-          x[r * kXld] = s;
-        }
-      } else {
-        for (int r = 0; r < nb; ++r) {
-          T s = Es[r * nb + r] * x[r * kXld];
-          for (int c = r + 1; c < nb; ++c) s = fma_rn(Es[r * nb + c], x[c * kXld], s);
-          x[r * kXld] = s;
-        }
+      for (int r = 0; r < nb; ++r) {
+        T s = Es[r * nb + r] * x[r * kXld];
+        for (int c = r + 1; c < nb; ++c) s = fma_rn(Es[r * nb + c], x[c * kXld], s);
+        x[r * kXld] = s;
       }
     }
   }
@@ -175,6 +158,117 @@ __global__ void __launch_bounds__(kTriVecs) tri_block_kernel(const T* __restrict
     const int t = vec_fast ? idx % kTriVecs : idx / nb;
     const int r = vec_fast ? idx / kTriVecs : idx % nb;
     if (t < nv) X[r * vs + (t0 + t) * ts] = Xs[r * kXld + t];
+  }
+}
+
+// x := E^-1 x for a diagonal block E of up to kPanelMax rows and `count` vectors (laid out
+// as above), kPanelVecs per CTA, the CTA's vectors resident in shared memory for the whole
+// block.  Blocked substitution over 32-row sub-blocks:
+//   * two warps solve the sub-block (one lane per vector) against its 32 x 32 triangle,
+//     multiplying by the reciprocal of each diagonal entry as Eigen's triangular solve
+//     kernel does (Eigen/src/Core/products/TriangularSolverMatrix.h:67);
+//   * all threads subtract its contribution from the rows below, a register-tiled product
+//     (4 rows x 4 vectors per thread) with the coefficient panel staged in shared memory
+//     128 rows at a time.
+// An upper triangle is solved as the lower one of the index-reversed system (row r <->
+// nb-1-r), so both run forward.
+constexpr int kPanelSub = 32;
+constexpr int kPanelThreads = 512;
+constexpr int kPanelChunk = 128;            // coefficient rows staged per pass
+constexpr int kPanelXld = kPanelVecs + 4;   // row stride of the resident vectors (16 B aligned)
+constexpr int kPanelDld = kPanelSub + 1;    // row stride of the diagonal sub-block
+
+template <typename T>
+__global__ void __launch_bounds__(kPanelThreads) tri_panel_solve_kernel(const T* __restrict__ E, int64_t er, int64_t ec,
+                                                                        int nb, bool lower, bool unit,
+                                                                        T* __restrict__ X, int64_t vs, int64_t ts,
+                                                                        int64_t count) {
+  static_assert(kPanelVecs == 64 && kPanelThreads == 512 && kPanelChunk == 128, "thread tiling");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Xs = reinterpret_cast<T*>(smem_raw);      // [nb][kPanelXld]: Xs[r * kPanelXld + t], forward row order
+  T* Ds = Xs + nb * kPanelXld;                 // [kPanelSub][kPanelDld]: the diagonal sub-block
+  T* Dinv = Ds + kPanelSub * kPanelDld;        // [kPanelSub]: reciprocals of the diagonal
+  T* Cs = Dinv + kPanelSub;                    // [kPanelSub][kPanelChunk]: coefficients, Cs[c * chunk + row]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tx = tid & 15, ty = tid >> 4;      // product tiling: vectors 4tx.., rows 4ty..
+  const int64_t t0 = int64_t(blockIdx.x) * kPanelVecs;
+  const int nv = int(count - t0 < kPanelVecs ? count - t0 : kPanelVecs);
+  // forward row r is row ro(r) of the stored system
+  auto ro = [&](int r) -> int64_t { return lower ? r : nb - 1 - r; };
+  const bool vec_fast = (ts == 1);
+  for (int idx = tid; idx < nb * kPanelVecs; idx += kPanelThreads) {
+    const int t = vec_fast ? idx % kPanelVecs : idx / nb;
+    const int r = vec_fast ? idx / kPanelVecs : idx % nb;
+    Xs[r * kPanelXld + t] = t < nv ? X[ro(r) * vs + (t0 + t) * ts] : T(0);
+  }
+  // the coefficient (r, c) of a panel is contiguous along r when the stored rows are
+  const bool row_fast = (er == 1 || er == -1);
+  for (int jb = 0; jb < nb; jb += kPanelSub) {
+    const int bs = nb - jb < kPanelSub ? nb - jb : kPanelSub;
+    __syncthreads();  // the rows of this sub-block are final (and, first, the load is done)
+    for (int idx = tid; idx < bs * bs; idx += kPanelThreads) {
+      const int r = idx / bs, c = idx % bs;
+      T v = T(0);
+      if (r == c)
+        v = unit ? T(1) : E[ro(jb + r) * er + ro(jb + c) * ec];
+      else if (r > c)
+        v = E[ro(jb + r) * er + ro(jb + c) * ec];
+      Ds[r * kPanelDld + c] = v;
+      if (r == c) Dinv[r] = unit ? T(1) : T(1) / v;
+    }
+    __syncthreads();
+    if (warp < 2) {
+      T* x = Xs + warp * 32 + lane;
+      for (int r = 0; r < bs; ++r) {
+        T s = x[(jb + r) * kPanelXld];
+        for (int c = 0; c < r; ++c) s = fma_rn(-Ds[r * kPanelDld + c], x[(jb + c) * kPanelXld], s);
+        x[(jb + r) * kPanelXld] = s * Dinv[r];
+      }
+    }
+    // rows below: x[r] -= E'(r, jb..jb+bs) x[jb..jb+bs], kPanelChunk rows per pass
+    for (int r0 = jb + bs; r0 < nb; r0 += kPanelChunk) {
+      const int rows = nb - r0 < kPanelChunk ? nb - r0 : kPanelChunk;
+      __syncthreads();  // the sub-block solve is done / the previous chunk's Cs is consumed
+      for (int idx = tid; idx < kPanelSub * kPanelChunk; idx += kPanelThreads) {
+        const int rr = row_fast ? idx % kPanelChunk : idx / kPanelSub;
+        const int c = row_fast ? idx / kPanelChunk : idx % kPanelSub;
+        Cs[c * kPanelChunk + rr] = (rr < rows && c < bs) ? E[ro(r0 + rr) * er + ro(jb + c) * ec] : T(0);
+      }
+      __syncthreads();
+      T acc[4][4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
+#pragma unroll 8
+      for (int c = 0; c < kPanelSub; ++c) {
+        T a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = Cs[c * kPanelChunk + 4 * ty + i];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = Xs[(jb + (c < bs ? c : 0)) * kPanelXld + 4 * tx + j];
+        if (c < bs) {
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = fma_rn(a[i], b[j], acc[i][j]);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int rr = 4 * ty + i;
+        if (rr < rows) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) Xs[(r0 + rr) * kPanelXld + 4 * tx + j] -= acc[i][j];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int idx = tid; idx < nb * kPanelVecs; idx += kPanelThreads) {
+    const int t = vec_fast ? idx % kPanelVecs : idx / nb;
+    const int r = vec_fast ? idx / kPanelVecs : idx % nb;
+    if (t < nv) X[ro(r) * vs + (t0 + t) * ts] = Xs[r * kPanelXld + t];
   }
 }
 
@@ -226,20 +320,41 @@ cudaError_t launch_multiply(int64_t m, int64_t n, T alpha, T* X, int64_t ldx, cu
 size_t tri_block_smem(int nb, size_t elem) { return (size_t(nb) * nb + size_t(nb) * (kTriVecs + 1)) * elem; }
 
 template <typename T>
-cudaError_t launch_tri_block(bool solve, const T* E, int64_t er, int64_t ec, int nb, bool lower, bool unit, T* X,
-                             int64_t vs, int64_t ts, int64_t count, cudaStream_t st) {
+cudaError_t launch_tri_block_multiply(const T* E, int64_t er, int64_t ec, int nb, bool lower, bool unit, T* X,
+                                      int64_t vs, int64_t ts, int64_t count, cudaStream_t st) {
   if (count == 0 || nb == 0) return cudaSuccess;
   if (nb < 0 || nb > kTriBlock || count < 0) return cudaErrorInvalidValue;
   const size_t smem = tri_block_smem(nb, sizeof(T));
   const int64_t blocks = (count + kTriVecs - 1) / kTriVecs;
   if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
-  auto kern = solve ? tri_block_kernel<T, true> : tri_block_kernel<T, false>;
+  auto kern = tri_block_multiply_kernel<T>;
   // one attribute call per instantiation: the largest block's footprint
   static_assert(sizeof(T) <= 8, "element size");
   cudaError_t e =
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tri_block_smem(kTriBlock, 8)));
   if (e != cudaSuccess) return e;
   kern<<<unsigned(blocks), kTriVecs, smem, st>>>(E, er, ec, nb, lower, unit, X, vs, ts, count);
+  return cudaGetLastError();
+}
+
+size_t tri_panel_smem(int nb, size_t elem) {
+  return (size_t(nb) * kPanelXld + size_t(kPanelSub) * kPanelDld + kPanelSub + size_t(kPanelSub) * kPanelChunk) *
+         elem;
+}
+
+template <typename T>
+cudaError_t launch_tri_panel_solve(const T* E, int64_t er, int64_t ec, int nb, bool lower, bool unit, T* X, int64_t vs,
+                                   int64_t ts, int64_t count, cudaStream_t st) {
+  if (count == 0 || nb == 0) return cudaSuccess;
+  if (nb < 0 || nb > kPanelMax || count < 0) return cudaErrorInvalidValue;
+  const int64_t blocks = (count + kPanelVecs - 1) / kPanelVecs;
+  if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
+  auto kern = tri_panel_solve_kernel<T>;
+  cudaError_t e =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tri_panel_smem(kPanelMax, 8)));
+  if (e != cudaSuccess) return e;
+  kern<<<unsigned(blocks), kPanelThreads, tri_panel_smem(nb, sizeof(T)), st>>>(E, er, ec, nb, lower, unit, X, vs, ts,
+                                                                              count);
   return cudaGetLastError();
 }
 
@@ -250,8 +365,10 @@ cudaError_t launch_tri_block(bool solve, const T* E, int64_t er, int64_t ec, int
   template cudaError_t launch_merge_triangle<T>(const T*, int64_t, int64_t, bool, T, T*, int64_t, cudaStream_t,    \
                                                 const int*);                                                       \
   template cudaError_t launch_multiply<T>(int64_t, int64_t, T, T*, int64_t, cudaStream_t);                          \
-  template cudaError_t launch_tri_block<T>(bool, const T*, int64_t, int64_t, int, bool, bool, T*, int64_t, int64_t, \
-                                           int64_t, cudaStream_t);
+  template cudaError_t launch_tri_block_multiply<T>(const T*, int64_t, int64_t, int, bool, bool, T*, int64_t,       \
+                                                    int64_t, int64_t, cudaStream_t);                               \
+  template cudaError_t launch_tri_panel_solve<T>(const T*, int64_t, int64_t, int, bool, bool, T*, int64_t, int64_t, \
+                                                 int64_t, cudaStream_t);
 EB2_TRI_INSTANTIATE(double)
 EB2_TRI_INSTANTIATE(float)
 #undef EB2_TRI_INSTANTIATE
