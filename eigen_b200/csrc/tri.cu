@@ -165,8 +165,8 @@ __global__ void __launch_bounds__(kTriVecs) tri_block_multiply_kernel(const T* _
 // as above), kPanelVecs per CTA, the CTA's vectors resident in shared memory for the whole
 // block.  Blocked substitution over 32-row sub-blocks:
 //   * two warps solve the sub-block (one lane per vector) against its 32 x 32 triangle,
-//     multiplying by the reciprocal of each diagonal entry as Eigen's triangular solve
-//     kernel does (Eigen/src/Core/products/TriangularSolverMatrix.h:67);
+//     column by column with the reciprocal of each diagonal entry, in the order of Eigen's
+//     column-major triangular solve kernel (Eigen/src/Core/products/TriangularSolverMatrix.h:61-82);
 //   * all threads subtract its contribution from the rows below, a register-tiled product
 //     (4 rows x 4 vectors per thread) with the coefficient panel staged in shared memory
 //     128 rows at a time.
@@ -218,12 +218,23 @@ __global__ void __launch_bounds__(kPanelThreads) tri_panel_solve_kernel(const T*
     }
     __syncthreads();
     if (warp < 2) {
+      // column by column, as Eigen's column-major kernel: x_c = s_c / d_c, then s_r -= d_rc x_c
+      // for every later row r -- independent updates, so the dependent chain is two
+      // operations per row instead of one per coefficient
       T* x = Xs + warp * 32 + lane;
-      for (int r = 0; r < bs; ++r) {
-        T s = x[(jb + r) * kPanelXld];
-        for (int c = 0; c < r; ++c) s = fma_rn(-Ds[r * kPanelDld + c], x[(jb + c) * kPanelXld], s);
-        x[(jb + r) * kPanelXld] = s * Dinv[r];
+      T sv[kPanelSub];
+#pragma unroll
+      for (int r = 0; r < kPanelSub; ++r) sv[r] = r < bs ? x[(jb + r) * kPanelXld] : T(0);
+#pragma unroll
+      for (int c = 0; c < kPanelSub; ++c) {
+        const T xc = sv[c] * Dinv[c < bs ? c : 0];
+        sv[c] = xc;
+#pragma unroll
+        for (int r = c + 1; r < kPanelSub; ++r) sv[r] = fma_rn(-Ds[r * kPanelDld + c], xc, sv[r]);
       }
+#pragma unroll
+      for (int r = 0; r < kPanelSub; ++r)
+        if (r < bs) x[(jb + r) * kPanelXld] = sv[r];
     }
     // rows below: x[r] -= E'(r, jb..jb+bs) x[jb..jb+bs], kPanelChunk rows per pass
     for (int r0 = jb + bs; r0 < nb; r0 += kPanelChunk) {
