@@ -58,6 +58,7 @@ def parse_args():
     ap.add_argument("--no-native", action="store_true")
     ap.add_argument("--no-grouped", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-level3", action="store_true", help="skip the level-3 routine and complex GEMM leg")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     a.steps = max(a.steps, 1)
@@ -194,6 +195,61 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------ peaks / profiles
+def level3_cpu_reference(n=2048, nz=1024):
+    """The reference's own level-3 routines and complex GEMM (Eigen's BLAS library built from
+    the reference sources into oracle/_ref, as its BLAS shim runs them: one thread per call) on a
+    bounded sample: one call each after a small warm-up, n = 2048 (complex: 1024)."""
+    import ctypes
+
+    import numpy as np
+
+    path = ROOT / "oracle" / "_ref" / "libeigen_ref_blas.so"
+    if not path.exists():
+        return {"error": "oracle/_ref/libeigen_ref_blas.so not built (make -C oracle ref)"}
+    lib = ctypes.CDLL(str(path), mode=ctypes.RTLD_LOCAL)
+    rng = np.random.default_rng(0)
+    i, d = ctypes.c_int, ctypes.c_double
+    P = lambda x: ctypes.c_void_p(x.ctypes.data)  # noqa: E731
+    R = ctypes.byref
+
+    def calls(m):
+        A = np.asfortranarray(rng.uniform(-1, 1, (m, m)))
+        B = np.asfortranarray(rng.uniform(-1, 1, (m, m)))
+        C = np.asfortranarray(rng.uniform(-1, 1, (m, m)))
+        T = np.asfortranarray(np.tril(A) / m + 1.5 * np.eye(m))
+        Z = np.asfortranarray(A + 1j * B)
+        W = np.asfortranarray(B + 1j * A)
+        Y = np.zeros((m, m), complex, order="F")
+        one, half = d(1.0), d(0.5)
+        zal, zbe = (d * 2)(1.0, 0.0), (d * 2)(0.0, 0.0)
+        M = i(m)
+        return {
+            "dsyrk UN": (lambda: lib.dsyrk_(b"U", b"N", R(M), R(M), R(one), P(A), R(M), R(half), P(C), R(M)),
+                         m * (m + 1) * m),
+            "dsymm LU": (lambda: lib.dsymm_(b"L", b"U", R(M), R(M), R(one), P(A), R(M), P(B), R(M), R(half), P(C),
+                                            R(M)), 2 * m ** 3),
+            "dtrmm LLNN": (lambda: lib.dtrmm_(b"L", b"L", b"N", b"N", R(M), R(M), R(one), P(T), R(M), P(B), R(M)),
+                           m ** 3),
+            "dtrsm LLNN": (lambda: lib.dtrsm_(b"L", b"L", b"N", b"N", R(M), R(M), R(one), P(T), R(M), P(B), R(M)),
+                           m ** 3),
+            "zgemm NN": (lambda: lib.zgemm_(b"N", b"N", R(M), R(M), R(M), zal, P(Z), R(M), P(W), R(M), zbe, P(Y),
+                                            R(M)), 8 * m ** 3),
+        }
+
+    for f, _ in calls(128).values():  # warm-up: code and page faults
+        f()
+    out = {}
+    for name, (f, flops) in calls(n).items():
+        if name.startswith("zgemm"):
+            f, flops = calls(nz)[name]
+        t0 = time.perf_counter()
+        f()
+        dt = time.perf_counter() - t0
+        out[name] = {"size": nz if name.startswith("zgemm") else n, "s": round(dt, 3),
+                     "tflops": round(flops / dt / 1e12, 5)}
+    return out
+
+
 def peaks():
     try:
         p = json.loads(PEAKS_FILE.read_text())
@@ -388,6 +444,33 @@ def reference_arm(a, world, rank):
     return 0
 
 
+# The other level-3 routines and the complex GEMM, on device operands at the benchmark size,
+# through their BLAS symbols with the default method: (routine, character arguments, dtype).
+LEVEL3_CASES = [("syrk", "UN", "d"), ("gemmtr", "UNT", "d"), ("symm", "LU", "d"), ("trmm", "LLNN", "d"),
+                ("trsm", "LLNN", "d"), ("trsm", "LLNN", "s"), ("zgemm", "NN", "z"), ("cgemm", "NN", "c")]
+
+
+def level3_leg(torch, S, reps=3):
+    """Device time (the library's events around each call, best of `reps` after a warm-up) and
+    rate in each routine's own flop count; see eigen_b200.__main__."""
+    from eigen_b200.__main__ import time_complex_gemm, time_level3
+
+    out = []
+    for routine, chars, dtype in LEVEL3_CASES:
+        if dtype in ("z", "c"):
+            res = time_complex_gemm(torch, dtype, S, S, S, reps)
+        else:
+            res = time_level3(torch, routine, chars, dtype, S, S, S, reps)
+        if "error" in res:
+            out.append({"op": dtype + routine, "error": res["error"]})
+            continue
+        call = res["call"]
+        out.append({"op": res["op"], "chars": chars, "size": S, "ms": min(res["ms"]), "tflops": res["tflops"],
+                    "method": call["method"], "moduli_or_slices": call["slices"],
+                    "err_estimate": call["err_estimate"], "launches": call["launches"]})
+    return out
+
+
 def our_arm(a, world, rank, local):
     import torch
     import torch.distributed as dist
@@ -509,6 +592,10 @@ def our_arm(a, world, rank, local):
     if not a.no_grouped:
         grouped = grouped_bench(eb, torch, dev, stream, a.steps, a.warmup)
 
+    level3 = None
+    if not a.no_level3:
+        level3 = level3_leg(torch, S)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         model, _ = host_cpu_info()
@@ -519,6 +606,8 @@ def our_arm(a, world, rank, local):
                              f"{res['reps']} reps median after 1 warm-up"}
         else:
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": err}
+        if not a.no_level3:
+            cpu["level3_reference"] = level3_cpu_reference()
 
     bf16, bf16_sus, hbm, basis = peaks()
     method = infos[-1]["method"]
@@ -552,6 +641,7 @@ def our_arm(a, world, rank, local):
                            err_estimate=infos[-1]["err_estimate"], escalations=infos[-1]["escalations"]),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "native_fp64": native, "accuracy": accuracy, "grouped_batch": grouped,
+            "level3_routines": level3,
             "emulated_over_native": round(value / native["tflops"], 3) if native else None,
         }
         print(json.dumps(line))

@@ -29,33 +29,36 @@ import eigen_b200 as eb
 METHODS = {"auto": eb.METHOD_AUTO, "native": eb.METHOD_NATIVE, "emulated": eb.METHOD_EMULATED, "crt": eb.METHOD_CRT}
 
 
-def _complex_gemm(a, torch):
-    """zgemm_ / cgemm_ on device operands (8mnk real flops); time = the library's device events."""
-    dt = torch.complex128 if a.dtype == "z" else torch.complex64
+def time_complex_gemm(torch, dtype, m, n, k, reps, method="auto", seed=0) -> dict:
+    """zgemm_ / cgemm_ (dtype "z" / "c") on device operands, NN, alpha = 1, beta = 0: the
+    library's device time of each of `reps` calls after one warm-up, rated at 8mnk flops."""
+    dt = torch.complex128 if dtype == "z" else torch.complex64
     g = torch.Generator(device="cuda")
-    g.manual_seed(a.seed)
-    A = torch.randn((a.k, a.m), dtype=dt, device="cuda", generator=g)
-    B = torch.randn((a.n, a.k), dtype=dt, device="cuda", generator=g)
-    C = torch.zeros((a.n, a.m), dtype=dt, device="cuda")
-    if a.dtype == "z":
-        eb.set_dgemm_method(METHODS[a.method])
+    g.manual_seed(seed)
+    A = torch.randn((k, m), dtype=dt, device="cuda", generator=g)
+    B = torch.randn((n, k), dtype=dt, device="cuda", generator=g)
+    C = torch.zeros((n, m), dtype=dt, device="cuda")
+    if dtype == "z":
+        eb.set_dgemm_method(METHODS[method])
     else:
-        eb.set_sgemm_method(METHODS[a.method] if a.method != "crt" else eb.METHOD_EMULATED)
+        eb.set_sgemm_method(METHODS[method] if method != "crt" else eb.METHOD_EMULATED)
     times = []
-    for i in range(a.reps + 1):
-        eb.complex_gemm(a.dtype, "N", "N", a.m, a.n, a.k, 1.0, A, a.m, B, a.k, 0.0, C, a.m)
+    for i in range(reps + 1):
+        eb.complex_gemm(dtype, "N", "N", m, n, k, 1.0, A, m, B, k, 0.0, C, m)
         err = eb.last_error()
         if err[0] != eb.EB2_OK:
-            print(json.dumps({"error": err}))
-            return 1
+            return {"error": err}
         if i:
             times.append(eb.last_call_info()["kernel_ms"])
     best = min(times)
-    print(json.dumps({"op": a.dtype + "gemm", "m": a.m, "n": a.n, "k": a.k, "method": a.method,
-                      "ms": [round(t, 4) for t in times],
-                      "tflops": round(8.0 * a.m * a.n * a.k / (best * 1e-3) / 1e12, 3),
-                      "call": eb.last_call_info()}))
-    return 0
+    return {"op": dtype + "gemm", "m": m, "n": n, "k": k, "method": method, "ms": [round(t, 4) for t in times],
+            "tflops": round(8.0 * m * n * k / (best * 1e-3) / 1e12, 3), "call": eb.last_call_info()}
+
+
+def _complex_gemm(a, torch):
+    res = time_complex_gemm(torch, a.dtype, a.m, a.n, a.k, a.reps, a.method, a.seed)
+    print(json.dumps(res))
+    return 0 if "error" not in res else 1
 
 
 def _gemm(a, torch):
@@ -101,16 +104,19 @@ def _gemm(a, torch):
     return 0
 
 
-def _level3(a, torch):
-    dt = torch.float64 if a.dtype == "d" else torch.float32
+def time_level3(torch, routine, chars, dtype, m, n, k, reps, method="auto", seed=0) -> dict:
+    """One of gemmtr, syrk, syr2k, symm, trmm, trsm (`chars` its character arguments in order)
+    on device operands through its BLAS symbol: the library's device time of each of `reps`
+    calls after one warm-up and the rate in the routine's own flop count."""
+    dt = torch.float64 if dtype == "d" else torch.float32
     g = torch.Generator(device="cuda")
-    g.manual_seed(a.seed)
-    ch = a.chars.upper()
+    g.manual_seed(seed)
+    ch = chars.upper()
 
     def rnd(rows, cols):
         return torch.rand((cols, rows), dtype=dt, device="cuda", generator=g) * 2 - 1  # column-major
 
-    r, m, n, k = a.routine, a.m, a.n, a.k
+    r = routine
     if r in ("gemmtr", "syrk", "syr2k"):
         ta = ch[1] != "N"
         tb = (ch[2] != "N") if r == "gemmtr" else not ta
@@ -141,28 +147,32 @@ def _level3(a, torch):
             args = [*ch, m, n, 1.0, A, size, B, m]
             flops = size * m * n
         dims = {"m": m, "n": n}
-    name = a.dtype + r
-    if a.dtype == "d":
-        eb.set_dgemm_method(METHODS[a.method])
+    name = dtype + r
+    if dtype == "d":
+        eb.set_dgemm_method(METHODS[method])
     else:
-        eb.set_sgemm_method(METHODS[a.method] if a.method != "crt" else eb.METHOD_EMULATED)
+        eb.set_sgemm_method(METHODS[method] if method != "crt" else eb.METHOD_EMULATED)
     out = B if r in ("trmm", "trsm") else C
     keep = out.clone()
     times = []
-    for i in range(a.reps + 1):
+    for i in range(reps + 1):
         out.copy_(keep)  # trmm / trsm overwrite their operand: every call starts from the same B
         torch.cuda.synchronize()
         eb.level3(name, *args)
         err = eb.last_error()
         if err[0] != eb.EB2_OK:
-            print(json.dumps({"error": err}))
-            return 1
+            return {"error": err}
         if i:
             times.append(eb.last_call_info()["kernel_ms"])
     best = min(times)
-    print(json.dumps({"op": name, "chars": a.chars, **dims, "method": a.method, "ms": [round(t, 4) for t in times],
-                      "tflops": round(flops / (best * 1e-3) / 1e12, 3), "call": eb.last_call_info()}))
-    return 0
+    return {"op": name, "chars": chars, **dims, "method": method, "ms": [round(t, 4) for t in times],
+            "tflops": round(flops / (best * 1e-3) / 1e12, 3), "call": eb.last_call_info()}
+
+
+def _level3(a, torch):
+    res = time_level3(torch, a.routine, a.chars, a.dtype, a.m, a.n, a.k, a.reps, a.method, a.seed)
+    print(json.dumps(res))
+    return 0 if "error" not in res else 1
 
 
 def _batch(a, torch):

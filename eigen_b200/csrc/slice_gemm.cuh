@@ -32,7 +32,10 @@
 
 namespace eb2 {
 
-enum SliceMode : int { kModeOzakiI8 = 0, kModeSplitBF16 = 1, kModeCrtI8 = 2 };
+enum SliceMode : int { kModeOzakiI8 = 0, kModeSplitBF16 = 1, kModeCrtI8 = 2, kModeCrtI8Listed = 3 };
+// kModeCrtI8Listed: the CRT product over the tiles of P.tile_list only (a separate
+// instantiation, so the ordinary CRT kernel carries no list lookup)
+__host__ __device__ constexpr bool is_crt_mode(int mode) { return mode == kModeCrtI8 || mode == kModeCrtI8Listed; }
 
 constexpr int kSliceBM = 128;      // rows of A per CTA (TMEM lanes)
 constexpr int kSliceKBytes = 128;  // bytes of K per pipeline stage
@@ -112,15 +115,20 @@ __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, 
 // Work items: one per output tile, or in CRT mode one per (tile, modulus): the moduli are
 // independent products, so small outputs still spread over the SMs, and the items in
 // flight at any time share one modulus (its residue planes stay in L2).
-// A tile list restricts a CRT launch to some tiles (the triangle of C of a gemmtr / syrk).
+// LISTED: the tiles are P.tile_list[0 .. num_listed) (the triangle of C of a gemmtr / syrk).
+template <bool LISTED>
 __host__ __device__ __forceinline__ int num_work(const SliceGemmParams& P) {
-  if (P.crt && P.tile_list) return P.num_listed * P.slices;
+  if (LISTED) return P.num_listed * P.slices;
   return P.tiles_m * P.tiles_n * (P.crt ? P.slices : 1);
 }
+template <bool LISTED>
 __device__ __forceinline__ void work_item(const SliceGemmParams& P, int w, int& tile, int& t_hi, int& t_lo) {
-  if (P.crt) {
-    const int nt = P.tile_list ? P.num_listed : P.tiles_m * P.tiles_n;
-    tile = P.tile_list ? P.tile_list[w % nt] : w % nt;
+  if (LISTED) {
+    tile = P.tile_list[w % P.num_listed];
+    t_hi = t_lo = w / P.num_listed;
+  } else if (P.crt) {
+    const int nt = P.tiles_m * P.tiles_n;
+    tile = w % nt;
     t_hi = t_lo = w / nt;
   } else {
     tile = w;
@@ -130,12 +138,13 @@ __device__ __forceinline__ void work_item(const SliceGemmParams& P, int w, int& 
 }
 
 // Walks the (work item, diagonal, pair, k-block) schedule in issue order.
+template <bool LISTED>
 struct BlockIter {
   int work, tile, t, t_lo, f, p_lo, total, stride;
   bool valid;
   __device__ __forceinline__ void load(const SliceGemmParams& P) {
     int t_hi;
-    work_item(P, work, tile, t_hi, t_lo);
+    work_item<LISTED>(P, work, tile, t_hi, t_lo);
     t = t_hi;
     f = 0;
   }
@@ -183,7 +192,7 @@ struct SliceTraits {
   // instruction descriptor: s8 x s8 -> s32 (Ozaki, CRT), bf16 x bf16 -> f32 (split-BF16); M = 128 or 256
   static constexpr uint32_t kIdesc = kInt8 ? make_idesc(2u, 1u, 1u, PAIR ? 256 : 128, BN)
                                            : make_idesc(1u, 1u, 1u, PAIR ? 256 : 128, BN);
-  static constexpr int kUnitKb = MODE == kModeCrtI8 ? kMaxUnitKbCrt : kMaxUnitKb;
+  static constexpr int kUnitKb = is_crt_mode(MODE) ? kMaxUnitKbCrt : kMaxUnitKb;
 };
 
 // B slice of a block: q - 1 = t - p - 1 for Ozaki/split-BF16 diagonals, t for CRT moduli.
@@ -208,10 +217,11 @@ __device__ __forceinline__ void slice_producer(const CUtensorMap* tmA, const CUt
   using L = SliceLayout<BN, STAGES, PAIR>;
   constexpr int ke = SliceTraits<MODE, BN, PAIR>::kKElems;  // innermost coordinate step (elements)
   constexpr uint32_t kTx = (PAIR ? 2u : 1u) * uint32_t(L::kABytes + L::kBBytes);
-  const int nwork = num_work(P);
+  constexpr bool kListed = MODE == kModeCrtI8Listed;
+  const int nwork = num_work<kListed>(P);
   const int a_row_off = PAIR ? int(rank) * kSliceBM : 0;
   const int b_row_off = PAIR ? int(rank) * L::kBRows : 0;
-  BlockIter it;
+  BlockIter<kListed> it;
   it.start(P, nwork, first_tile<PAIR>(), tile_step<PAIR>());
   uint32_t issued = 0;  // stage = issued % STAGES, phase = (issued / STAGES) & 1
   bool ok = true;
@@ -271,14 +281,15 @@ __device__ __forceinline__ void slice_mma(uint8_t* smem, uint64_t* full, uint64_
   using L = SliceLayout<BN, STAGES, PAIR>;
   constexpr uint32_t idesc = SliceTraits<MODE, BN, PAIR>::kIdesc;
   constexpr bool kTileUnit = (MODE == kModeSplitBF16);
-  const int nwork = num_work(P);
+  constexpr bool kListed = MODE == kModeCrtI8Listed;
+  const int nwork = num_work<kListed>(P);
   uint32_t consumed = 0;  // stage = consumed % STAGES, phase = (consumed / STAGES) & 1
   int buf = 0;
   uint32_t tphase = 0u;  // bit b: phase of accumulator buffer b
   bool ok = true;
   for (int w = first_tile<PAIR>(); w < nwork && ok; w += tile_step<PAIR>()) {
     int tile, t_hi, t_lo;
-    work_item(P, w, tile, t_hi, t_lo);
+    work_item<kListed>(P, w, tile, t_hi, t_lo);
     bool fresh = true;  // the next MMA overwrites the accumulator
     if (kTileUnit) {
       if (!mbar_wait(&tempty[buf], ((tphase >> buf) & 1u) ^ 1u, abort_flag, P.status)) break;
@@ -286,7 +297,7 @@ __device__ __forceinline__ void slice_mma(uint8_t* smem, uint64_t* full, uint64_
     }
     for (int t = t_hi; t >= t_lo && ok; --t) {
       int p_lo, total;
-      if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, MODE == kModeCrtI8)) continue;
+      if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, is_crt_mode(MODE))) continue;
       constexpr int kUnit = SliceTraits<MODE, BN, PAIR>::kUnitKb;
       for (int u0 = 0; u0 < total && ok;) {
         const int u1 = (kTileUnit || total - u0 <= kUnit) ? total : u0 + kUnit;
@@ -471,7 +482,7 @@ __device__ __forceinline__ uint32_t mod_small(uint32_t x, uint32_t p, uint32_t m
 // CRT: unit t is modulus p_t; every INT32 product entry is reduced to [0, p_t) and stored
 // as one byte of residue plane t (column-major, ld_res).  K beyond one unit comes in
 // further chunks whose residues are added mod p_t.
-template <int BN, int NW, bool PAIR>
+template <int BN, int NW, bool PAIR, bool LISTED>
 __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull, uint64_t* tempty,
                                              volatile int* abort_flag, const SliceGemmParams& P) {
   constexpr int kCols = BN * 4 / NW;
@@ -480,7 +491,7 @@ __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull
   const int quad = warp & 3;
   const int col_base = ((warp - 2) >> 2) * kCols;
   const int row = quad * 32 + lane;
-  const int nwork = num_work(P);
+  const int nwork = num_work<LISTED>(P);
   const int row_base = PAIR ? int(cluster_ctarank()) * kSliceBM : 0;
   const int64_t plane = P.ld_res * int64_t(P.tiles_n) * BN;
   int buf = 0;
@@ -488,7 +499,7 @@ __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull
   bool ok = true;
   for (int w = first_tile<PAIR>(); w < nwork && ok; w += tile_step<PAIR>()) {
     int tile, t_hi, t_lo, tm, tn;
-    work_item(P, w, tile, t_hi, t_lo);
+    work_item<LISTED>(P, w, tile, t_hi, t_lo);
     tile_coords(tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
     const int64_t m0 = int64_t(tm) * (PAIR ? 2 * kSliceBM : kSliceBM) + row_base;
     const int64_t n0 = int64_t(tn) * BN + col_base;
@@ -649,8 +660,8 @@ __global__ void __launch_bounds__(64 + 32 * NW, 1)
   } else {
     if constexpr (MODE == kModeOzakiI8)
       ozaki_epilogue<BN, NW, PAIR>(tmem_base, tfull, tempty, col_exp, abort_flag, P);
-    else if constexpr (MODE == kModeCrtI8)
-      crt_epilogue<BN, NW, PAIR>(tmem_base, tfull, tempty, abort_flag, P);
+    else if constexpr (is_crt_mode(MODE))
+      crt_epilogue<BN, NW, PAIR, MODE == kModeCrtI8Listed>(tmem_base, tfull, tempty, abort_flag, P);
     else
       bf16_epilogue<BN, NW, PAIR>(tmem_base, tfull, tempty, abort_flag, P);
   }
@@ -677,7 +688,7 @@ inline cudaError_t launch_slice_gemm(const CUtensorMap& tmA, const CUtensorMap& 
   auto kern = slice_gemm_kernel<MODE, BN, STAGES, NW, PAIR>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kAlloc);
   if (e != cudaSuccess) return e;
-  const int tiles = num_work(P);
+  const int tiles = num_work<MODE == kModeCrtI8Listed>(P);
   const int ctas = PAIR ? 2 * (tiles < num_sms / 2 ? tiles : num_sms / 2) : (tiles < num_sms ? tiles : num_sms);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(unsigned(ctas), 1, 1);
