@@ -309,6 +309,14 @@ def clear_error() -> None:
     load().eb2_clear_error()
 
 
+def routine_calls(name: str) -> int:
+    """Calls of the named BLAS routine (e.g. "dtrsm") that reached the device in this process."""
+    f = load().eb2_routine_calls
+    f.argtypes = [ctypes.c_char_p]
+    f.restype = ctypes.c_longlong
+    return int(f(name.encode()))
+
+
 def last_call_info() -> dict:
     ci = CallInfo()
     load().eb2_last_call_info(ctypes.byref(ci))

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 
@@ -23,6 +24,26 @@ extern "C" __attribute__((weak)) void xerbla_(const char* name, int* info, size_
 }
 
 namespace eb2 {
+
+namespace {
+// The routines this library exports, in the order of their counters.
+constexpr const char* kRoutines[] = {"sgemm", "dgemm", "cgemm", "zgemm", "sgemmtr", "dgemmtr", "ssyrk", "dsyrk",
+                                     "ssyr2k", "dsyr2k", "ssymm", "dsymm", "strmm", "dtrmm", "strsm", "dtrsm"};
+constexpr int kNumRoutines = int(sizeof(kRoutines) / sizeof(kRoutines[0]));
+std::atomic<long long> g_calls[kNumRoutines];
+
+int routine_index(const char* name) {
+  if (!name) return -1;
+  for (int i = 0; i < kNumRoutines; ++i)
+    if (std::strcmp(kRoutines[i], name) == 0) return i;
+  return -1;
+}
+}  // namespace
+
+void count_call(const char* name) {
+  const int i = routine_index(name);
+  if (i >= 0) g_calls[i].fetch_add(1, std::memory_order_relaxed);
+}
 
 bool device_usable(const void* p) {
   if (!p) return false;
@@ -101,6 +122,7 @@ void blas_gemm(char transa, char transb, int64_t m, int64_t n, int64_t k, T alph
     return;
   }
   if (m == 0 || n == 0) return;
+  count_call(sizeof(T) == 8 ? "dgemm" : "sgemm");
   Context* cx = current_context();
   if (!cx) {
     std::fprintf(stderr, "eigen_b200: %s\n", eb2_last_error_string());
@@ -323,6 +345,11 @@ int eb2_sgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, 
   ci = eb2_call_info{};
   return eb2::sgemm_on_device(*cx, eb2::op_code(transa) != eb2::kNoTr, eb2::op_code(transb) != eb2::kNoTr, m, n, k,
                               alpha, a, lda, b, ldb, beta, c, ldc, static_cast<cudaStream_t>(stream), o, ci);
+}
+
+long long eb2_routine_calls(const char* name) {
+  const int i = eb2::routine_index(name);
+  return i < 0 ? -1 : eb2::g_calls[i].load(std::memory_order_relaxed);
 }
 
 const char* eb2_version(void) { return "eigen_b200 0.1 (sm_100a)"; }

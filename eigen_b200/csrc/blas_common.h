@@ -28,6 +28,11 @@ inline int side_code(char c) { return (c == 'L' || c == 'l') ? kLeft : (c == 'R'
 inline int uplo_code(char c) { return (c == 'U' || c == 'u') ? kUp : (c == 'L' || c == 'l') ? kLo : kInvalid; }
 inline int diag_code(char c) { return (c == 'N' || c == 'n') ? kNonUnit : (c == 'U' || c == 'u') ? kUnit : kInvalid; }
 
+// Per-routine call counters behind eb2_routine_calls: a routine counts once per call that
+// gets past its argument checks and quick returns (name lower-case without the trailing
+// underscore, e.g. "dtrsm").
+void count_call(const char* name);
+
 // True when the device can use the pointer in place (device or managed memory).
 bool device_usable(const void* p);
 

@@ -466,6 +466,7 @@ void blas_gemmtr(char uplo, char opa, char opb, int64_t n, int64_t k, T alpha, c
   int info = gemmtr_info(uplo, opa, opb, n, k, lda, ldb, ldc);
   if (info) return xerbla_(prefixed<T>("DGEMMTR", "SGEMMTR"), &info, 7);
   if (n == 0) return;
+  count_call(prefixed<T>("dgemmtr", "sgemmtr"));
   Call call(dtype_of<T>());
   if (!call.begin()) return;
   const bool ta = op_code(opa) != kNoTr, tb = op_code(opb) != kNoTr;
@@ -489,6 +490,7 @@ void blas_syrk(char uplo, char op, int64_t n, int64_t k, T alpha, const T* a, in
   int info = syrk_info(uplo, op, n, k, lda, ldc);
   if (info) return xerbla_(prefixed<T>("DSYRK ", "SSYRK "), &info, 6);
   if (n == 0) return;
+  count_call(prefixed<T>("dsyrk", "ssyrk"));
   Call call(dtype_of<T>());
   if (!call.begin()) return;
   const bool ta = op_code(op) != kNoTr;
@@ -511,6 +513,7 @@ void blas_syr2k(char uplo, char op, int64_t n, int64_t k, T alpha, const T* a, i
   int info = syr2k_info(uplo, op, n, k, lda, ldb, ldc);
   if (info) return xerbla_(prefixed<T>("DSYR2K", "SSYR2K"), &info, 6);
   if (n == 0) return;
+  count_call(prefixed<T>("dsyr2k", "ssyr2k"));
   Call call(dtype_of<T>());
   if (!call.begin()) return;
   const bool ta = op_code(op) != kNoTr;
@@ -540,6 +543,7 @@ void blas_symm(char side, char uplo, int64_t m, int64_t n, T alpha, const T* a, 
   int info = symm_info(side, uplo, m, n, lda, ldb, ldc);
   if (info) return xerbla_(prefixed<T>("DSYMM ", "SSYMM "), &info, 6);
   if (m == 0 || n == 0) return;
+  count_call(prefixed<T>("dsymm", "ssymm"));
   Call call(dtype_of<T>());
   if (!call.begin()) return;
   const bool left = side_code(side) == kLeft;
@@ -564,6 +568,7 @@ void blas_trxm(bool solve, char side, char uplo, char op, char diag, int64_t m, 
   if (info)
     return xerbla_(solve ? prefixed<T>("DTRSM ", "STRSM ") : prefixed<T>("DTRMM ", "STRMM "), &info, 6);
   if (m == 0 || n == 0) return;
+  count_call(solve ? prefixed<T>("dtrsm", "strsm") : prefixed<T>("dtrmm", "strmm"));
   Call call(dtype_of<T>());
   if (!call.begin()) return;
   const bool left = side_code(side) == kLeft;
@@ -605,6 +610,7 @@ void blas_complex_gemm(char opa, char opb, int64_t m, int64_t n, int64_t k, cons
   const bool beta_one = br == T(1) && bi == T(0), beta_zero = br == T(0) && bi == T(0);
   const bool need_ab = k > 0 && !alpha_zero;
   if (!need_ab && beta_one) return;
+  count_call(prefixed<T>("zgemm", "cgemm"));
   Call call(dtype_of<T>() == 'd' ? 'z' : 'c');
   if (!call.begin()) return;
   const int oa = op_code(opa), ob = op_code(opb);

@@ -225,6 +225,12 @@ typedef struct eb2_call_info {
 } eb2_call_info;
 int eb2_last_call_info(eb2_call_info* out);
 
+/* How many calls of the named BLAS routine ("dgemm", "zgemm", "dtrsm", "ssyrk", ...: lower
+ * case, no underscore) reached the device in this process: every call past its argument
+ * checks and quick returns.  -1 for a name this library does not export.  No counterpart in
+ * the reference; it lets a caller see which routines an Eigen build routed here. */
+long long eb2_routine_calls(const char* name);
+
 /* Record CUDA events around every product (1) or not (0, default for the
  * eb2_*_device calls; the BLAS entry points always time).  The times appear in
  * eb2_last_call_info (which waits for the events) until the next call on the device. */
