@@ -204,20 +204,22 @@ LEVEL3_SIGNATURES = {
     "symm": "ccii" "s" "ai" "ai" "s" "ai",     # side uplo m n alpha a lda b ldb beta c ldc
     "trmm": "ccccii" "s" "ai" "ai",            # side uplo transa diag m n alpha a lda b ldb
     "trsm": "ccccii" "s" "ai" "ai",            # side uplo transa diag m n alpha a lda b ldb
+    "hemm": "ccii" "s" "ai" "ai" "s" "ai",     # side uplo m n alpha a lda b ldb beta c ldc (complex)
 }
 
 
 def level3(name: str, *args, ilp64: bool = False) -> None:
-    """Call an exported level-3 routine by its BLAS name (``dsyrk``, ``strsm``, ``dgemmtr`` ...)
-    with its Fortran argument list in order (see ``LEVEL3_SIGNATURES``): characters as str,
-    dimensions and scalars as Python numbers, matrices as numpy arrays / torch tensors (host or
-    CUDA) or raw addresses.  ``ilp64`` calls the ``_64_`` symbol."""
+    """Call an exported level-3 routine by its BLAS name (``dsyrk``, ``strsm``, ``dgemmtr``,
+    ``ztrsm``, ``chemm`` ...) with its Fortran argument list in order (see
+    ``LEVEL3_SIGNATURES``): characters as str, dimensions and scalars as Python numbers (complex
+    for the z / c routines), matrices as numpy arrays / torch tensors (host or CUDA) or raw
+    addresses.  ``ilp64`` calls the ``_64_`` symbol."""
     lib = load()
     dtype, routine = name[0], name[1:]
     kinds = LEVEL3_SIGNATURES[routine]
-    if dtype not in "ds" or len(args) != len(kinds):
+    if dtype not in "dszc" or len(args) != len(kinds):
         raise ValueError(f"{name}: expected {len(kinds)} arguments")
-    ctype = ctypes.c_double if dtype == "d" else ctypes.c_float
+    ctype = ctypes.c_double if dtype in "dz" else ctypes.c_float
     itype = ctypes.c_int64 if ilp64 else ctypes.c_int
     out, keep = [], []
     for kind, v in zip(kinds, args):
@@ -227,7 +229,10 @@ def level3(name: str, *args, ilp64: bool = False) -> None:
         if kind == "a":
             out.append(ctypes.c_void_p(_ptr(v)))
             continue
-        x = itype(v) if kind == "i" else ctype(v)
+        if kind == "s" and dtype in "zc":
+            x = (ctype * 2)(complex(v).real, complex(v).imag)
+        else:
+            x = itype(v) if kind == "i" else ctype(v)
         keep.append(x)
         out.append(ctypes.cast(ctypes.byref(x), ctypes.c_void_p))
     f = getattr(lib, name + ("_64_" if ilp64 else "_"))

@@ -28,7 +28,8 @@ namespace eb2 {
 namespace {
 // The routines this library exports, in the order of their counters.
 constexpr const char* kRoutines[] = {"sgemm", "dgemm", "cgemm", "zgemm", "sgemmtr", "dgemmtr", "ssyrk", "dsyrk",
-                                     "ssyr2k", "dsyr2k", "ssymm", "dsymm", "strmm", "dtrmm", "strsm", "dtrsm"};
+                                     "ssyr2k", "dsyr2k", "ssymm", "dsymm", "strmm", "dtrmm", "strsm", "dtrsm",
+                                     "csymm",  "zsymm",  "chemm", "zhemm", "ctrmm", "ztrmm", "ctrsm", "ztrsm"};
 constexpr int kNumRoutines = int(sizeof(kRoutines) / sizeof(kRoutines[0]));
 std::atomic<long long> g_calls[kNumRoutines];
 

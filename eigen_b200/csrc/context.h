@@ -40,6 +40,7 @@ struct Context {
   DeviceBuffer ws;                // emulation workspace (digits, exponents, scan results)
   DeviceBuffer stage_a, stage_b, stage_c;  // device copies of host operands
   DeviceBuffer tmp;               // level-3 routines: expanded operands, diagonal-block products
+  DeviceBuffer cplx;              // complex products: packed real operands and the two real results
   DeviceFlags* dflags = nullptr;  // device
   DeviceFlags* hflags = nullptr;  // pinned host mirror
   // Host-buffer pipeline of the BLAS entry (copies overlapped with the product by column

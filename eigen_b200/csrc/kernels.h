@@ -236,5 +236,19 @@ cudaError_t launch_pack_complex_rhs(const T* X, int64_t sr, int64_t sc, bool con
 template <typename T>
 cudaError_t launch_combine_complex(const T* Pr, const T* Pi, int64_t ldp, int64_t m, int64_t n, T ar, T ai, T br,
                                    T bi, T* C, int64_t ldc, cudaStream_t stream);
+// out (n x n complex) from the triangle `upper` of the complex A: mode 0 symmetric (mirror),
+// 1 Hermitian (conjugate mirror, real diagonal), 2 triangular (zeros outside, unit diagonal
+// if `unit`).  Only the stored triangle of A is read.
+template <typename T>
+cudaError_t launch_expand_complex(const T* A, int64_t lda, int64_t n, bool upper, int mode, bool unit, T* out,
+                                  int64_t ldo, cudaStream_t stream);
+// x := E^-1 x for `count` complex vectors (element r of vector t at complex index
+// r*vs + t*ts), E the nb x nb (nb <= kPanelMaxComplex) complex triangle `lower`/upper at
+// complex index r*er + c*ec, conjugated when `conj`, unit diagonal if `unit`.
+constexpr int kPanelMaxComplex = 128;
+template <typename T>
+cudaError_t launch_tri_panel_solve_complex(const T* E, int64_t er, int64_t ec, int nb, bool lower, bool unit,
+                                           bool conj, T* X, int64_t vs, int64_t ts, int64_t count,
+                                           cudaStream_t stream);
 
 }  // namespace eb2

@@ -364,6 +364,147 @@ int trxm_device(Context& cx, bool solve, bool left, bool upper, bool trans, bool
   return worst;
 }
 
+// ---------------------------------------------------------------- complex products
+// C := (ar + i ai) op(A) op(B) + (br + i bi) C on device pointers to interleaved complex
+// matrices (leading dimensions in complex elements), op codes kNoTr / kTr / kAdj.  The
+// product is two real GEMMs of inner dimension 2k on packed operands (complex.cu):
+// Re = [Ar Ai][Br; -Bi], Im = [Ar Ai][Bi; Br].  Workspace: cx.cplx.
+template <typename T>
+int complex_gemm_device(Context& cx, int oa, int ob, int64_t m, int64_t n, int64_t k, T ar, T ai, const T* A,
+                        int64_t lda, const T* B, int64_t ldb, T br, T bi, T* C, int64_t ldc, cudaStream_t st,
+                        Summary& sum) {
+  if (m == 0 || n == 0) return EB2_OK;
+  if (k == 0 || (ar == T(0) && ai == T(0))) {
+    if (br == T(1) && bi == T(0)) return EB2_OK;
+    sum.launches += 1;
+    return cuda_ok(launch_combine_complex<T>(nullptr, nullptr, 0, m, n, ar, ai, br, bi, C, ldc, st), "scale C")
+               ? EB2_OK
+               : EB2_ERR_CUDA;
+  }
+  // workspace: A' (m x 2k), B1 and B2 (2k x n), Pr and Pi (m x n)
+  const size_t e_a = size_t(m) * 2 * k, e_b = size_t(2 * k) * n, e_p = size_t(m) * n;
+  if (!cx.cplx.ensure((e_a + 2 * e_b + 2 * e_p) * sizeof(T))) {
+    set_error(EB2_ERR_ALLOC, "could not allocate the complex-product workspace");
+    return EB2_ERR_ALLOC;
+  }
+  T* Ap = static_cast<T*>(cx.cplx.ptr);
+  T* B1 = Ap + e_a;
+  T* B2 = B1 + e_b;
+  T* Pr = B2 + e_b;
+  T* Pi = Pr + e_p;
+  bool ok = cuda_ok(launch_pack_complex_lhs<T>(A, oa == kNoTr ? 1 : lda, oa == kNoTr ? lda : 1, oa == kAdj, m, k, Ap,
+                                               st),
+                    "pack op(A)");
+  ok = ok && cuda_ok(launch_pack_complex_rhs<T>(B, ob == kNoTr ? 1 : ldb, ob == kNoTr ? ldb : 1, ob == kAdj, k, n, B1,
+                                                B2, st),
+                     "pack op(B)");
+  if (!ok) return EB2_ERR_CUDA;
+  sum.launches += 2;
+  int worst = EB2_OK;
+  if (keep_going(gemm(cx, false, false, m, n, 2 * k, T(1), Ap, m, B1, 2 * k, T(0), Pr, m, st, sum), worst) &&
+      keep_going(gemm(cx, false, false, m, n, 2 * k, T(1), Ap, m, B2, 2 * k, T(0), Pi, m, st, sum), worst)) {
+    if (!cuda_ok(launch_combine_complex<T>(Pr, Pi, m, m, n, ar, ai, br, bi, C, ldc, st), "combine"))
+      worst = EB2_ERR_CUDA;
+    sum.launches += 1;
+  }
+  return worst;
+}
+
+// C := alpha S B + beta C (left, S m x m) or alpha B S + beta C (right, S n x n), S the
+// symmetric (hermitian = false) or Hermitian matrix whose triangle `upper` is stored in A;
+// all complex, interleaved.
+template <typename T>
+int complex_symm_device(Context& cx, bool hermitian, bool left, bool upper, int64_t m, int64_t n, T ar, T ai,
+                        const T* A, int64_t lda, const T* B, int64_t ldb, T br, T bi, T* C, int64_t ldc,
+                        cudaStream_t st, Summary& sum) {
+  if (m == 0 || n == 0) return EB2_OK;
+  const int64_t size = left ? m : n;
+  T* S = nullptr;
+  if (ar != T(0) || ai != T(0)) {
+    if (!cx.tmp.ensure(size_t(size) * size * 2 * sizeof(T))) {
+      set_error(EB2_ERR_ALLOC, "could not allocate the symmetric-operand workspace");
+      return EB2_ERR_ALLOC;
+    }
+    S = static_cast<T*>(cx.tmp.ptr);
+    if (!cuda_ok(launch_expand_complex<T>(A, lda, size, upper, hermitian ? 1 : 0, false, S, size, st), "expand"))
+      return EB2_ERR_CUDA;
+    sum.launches += 1;
+  }
+  return left ? complex_gemm_device<T>(cx, kNoTr, kNoTr, m, n, m, ar, ai, S, size, B, ldb, br, bi, C, ldc, st, sum)
+              : complex_gemm_device<T>(cx, kNoTr, kNoTr, m, n, n, ar, ai, B, ldb, S, size, br, bi, C, ldc, st, sum);
+}
+
+// In place on the complex m x n B: B := op(A)^-1 B / B op(A)^-1 (solve) or op(A) B / B op(A)
+// (multiply), A triangular (triangle `upper` stored, unit diagonal if `unit`), op code `op`
+// (kNoTr, kTr, kAdj), then B := alpha B.
+template <typename T>
+int complex_trxm_device(Context& cx, bool solve, bool left, bool upper, int op, bool unit, int64_t m, int64_t n,
+                        T ar, T ai, const T* A, int64_t lda, T* B, int64_t ldb, cudaStream_t st, Summary& sum) {
+  if (m == 0 || n == 0) return EB2_OK;
+  const int64_t size = left ? m : n;
+  const bool trans = op != kNoTr;
+  if (!solve) {
+    // one product with the triangle expanded (zeros, unit diagonal), out of place, copied back
+    if (!cx.tmp.ensure((size_t(size) * size + size_t(m) * n) * 2 * sizeof(T))) {
+      set_error(EB2_ERR_ALLOC, "could not allocate the triangular-product workspace");
+      return EB2_ERR_ALLOC;
+    }
+    T* Tf = static_cast<T*>(cx.tmp.ptr);
+    T* P = Tf + size_t(size) * size * 2;
+    if (!cuda_ok(launch_expand_complex<T>(A, lda, size, upper, 2, unit, Tf, size, st), "expand")) return EB2_ERR_CUDA;
+    sum.launches += 1;
+    const int rc = left ? complex_gemm_device<T>(cx, op, kNoTr, m, n, m, ar, ai, Tf, size, B, ldb, T(0), T(0), P, m,
+                                                 st, sum)
+                        : complex_gemm_device<T>(cx, kNoTr, op, m, n, n, ar, ai, B, ldb, Tf, size, T(0), T(0), P, m,
+                                                 st, sum);
+    if (rc != EB2_OK && rc != EB2_ERR_ACCURACY) return rc;
+    if (!cuda_ok(cudaMemcpy2DAsync(B, size_t(ldb) * 2 * sizeof(T), P, size_t(m) * 2 * sizeof(T),
+                                   size_t(m) * 2 * sizeof(T), size_t(n), cudaMemcpyDeviceToDevice, st),
+                 "copy back"))
+      return EB2_ERR_CUDA;
+    return rc;
+  }
+  // the solve: recursion on halves as in trxm_device, complex GEMM updates, complex panels
+  const bool lower = trans ? upper : !upper;  // the triangle of M = op(A)
+  auto msub = [&](int64_t r0, int64_t c0) -> const T* { return A + 2 * (trans ? c0 + r0 * lda : r0 + c0 * lda); };
+  int worst = EB2_OK;
+  auto leaf = [&](int64_t i0, int64_t nb) -> bool {
+    const T* D = A + 2 * (i0 + i0 * lda);
+    const int64_t mr = trans ? lda : 1, mc = trans ? 1 : lda;
+    const int64_t er = left ? mr : mc, ec = left ? mc : mr;
+    T* X = left ? B + 2 * i0 : B + 2 * i0 * ldb;
+    const int64_t vs = left ? 1 : ldb, ts = left ? ldb : 1, count = left ? n : m;
+    if (!cuda_ok(launch_tri_panel_solve_complex<T>(D, er, ec, int(nb), left ? lower : !lower, unit, op == kAdj, X, vs,
+                                                   ts, count, st),
+                 "triangular block")) {
+      worst = EB2_ERR_CUDA;
+      return false;
+    }
+    sum.launches += 1;
+    return true;
+  };
+  auto update = [&](int64_t d0, int64_t dn, int64_t s0, int64_t sn) -> bool {
+    const int rc = left ? complex_gemm_device<T>(cx, op, kNoTr, dn, n, sn, T(-1), T(0), msub(d0, s0), lda, B + 2 * s0,
+                                                 ldb, T(1), T(0), B + 2 * d0, ldb, st, sum)
+                        : complex_gemm_device<T>(cx, kNoTr, op, m, dn, sn, T(-1), T(0), B + 2 * s0 * ldb, ldb,
+                                                 msub(s0, d0), lda, T(1), T(0), B + 2 * d0 * ldb, ldb, st, sum);
+    return keep_going(rc, worst);
+  };
+  std::function<bool(int64_t, int64_t)> rec = [&](int64_t i0, int64_t sz) -> bool {
+    if (sz <= kPanelMaxComplex) return leaf(i0, sz);
+    const int64_t h = (sz / 2 + kPanelMaxComplex - 1) / kPanelMaxComplex * kPanelMaxComplex;
+    const int64_t a0 = i0, an = h, b0 = i0 + h, bn = sz - h;
+    const bool first_is_a = left ? lower : !lower;
+    if (first_is_a) return rec(a0, an) && update(b0, bn, a0, an) && rec(b0, bn);
+    return rec(b0, bn) && update(a0, an, b0, bn) && rec(a0, an);
+  };
+  if (!rec(0, size)) return worst;
+  if ((ar != T(1) || ai != T(0)) &&
+      !cuda_ok(launch_combine_complex<T>(nullptr, nullptr, 0, m, n, T(0), T(0), ar, ai, B, ldb, st), "scale"))
+    return EB2_ERR_CUDA;
+  return worst;
+}
+
 // ---------------------------------------------------------------- host entry points
 // A matrix argument as the device sees it: the caller's pointer when the device can use it
 // in place, else a device copy (leading dimension = rows).
@@ -586,8 +727,7 @@ void blas_trxm(bool solve, char side, char uplo, char op, char diag, int64_t m, 
 // blas/level3_impl.h:12-96 with Scalar = std::complex (blas/complex_double.cpp,
 // blas/complex_single.cpp): C := alpha op(A) op(B) + beta C, op in {N, T, C = conjugate
 // transpose}.  beta scales C first (0: zeros); k == 0 or alpha == 0 stops there
-// (Eigen/src/Core/products/GeneralMatrixMatrix.h:129-130).  The product is two real GEMMs of
-// inner dimension 2k on packed real operands (complex.cu), combined with complex alpha/beta.
+// (Eigen/src/Core/products/GeneralMatrixMatrix.h:129-130).
 template <typename T>
 void blas_complex_gemm(char opa, char opb, int64_t m, int64_t n, int64_t k, const T* alpha, const T* a, int64_t lda,
                        const T* b, int64_t ldb, const T* beta, T* c, int64_t ldc) {
@@ -623,54 +763,71 @@ void blas_complex_gemm(char opa, char opb, int64_t m, int64_t n, int64_t k, cons
       !stage(call.cx->stage_c, c, 2 * ldc, 2 * m, n, !beta_zero, call.st, C))
     return call.fail();
   call.started();
-  int rc = EB2_OK;
-  const int64_t ldc_c = C.ld / 2;
-  if (!need_ab) {
-    if (!cuda_ok(launch_combine_complex<T>(nullptr, nullptr, 0, m, n, ar, ai, br, bi, C.ptr, ldc_c, call.st),
-                 "scale C"))
-      rc = EB2_ERR_CUDA;
-    call.sum.launches += 1;
-  } else {
-    // workspace: A' (m x 2k), B1 and B2 (2k x n), Pr and Pi (m x n)
-    const size_t e_a = size_t(m) * 2 * k, e_b = size_t(2 * k) * n, e_p = size_t(m) * n;
-    if (!call.cx->tmp.ensure((e_a + 2 * e_b + 2 * e_p) * sizeof(T))) {
-      set_error(EB2_ERR_ALLOC, "could not allocate the complex-product workspace");
-      return call.fail();
-    }
-    T* Ap = static_cast<T*>(call.cx->tmp.ptr);
-    T* B1 = Ap + e_a;
-    T* B2 = B1 + e_b;
-    T* Pr = B2 + e_b;
-    T* Pi = Pr + e_p;
-    const int64_t lda_c = A.ld / 2, ldb_c = B.ld / 2;
-    bool ok = cuda_ok(launch_pack_complex_lhs<T>(A.ptr, oa == kNoTr ? 1 : lda_c, oa == kNoTr ? lda_c : 1,
-                                                 oa == kAdj, m, k, Ap, call.st),
-                      "pack op(A)");
-    ok = ok && cuda_ok(launch_pack_complex_rhs<T>(B.ptr, ob == kNoTr ? 1 : ldb_c, ob == kNoTr ? ldb_c : 1,
-                                                  ob == kAdj, k, n, B1, B2, call.st),
-                       "pack op(B)");
-    if (!ok) return call.fail();
-    call.sum.launches += 2;
-    int worst = EB2_OK;
-    if (keep_going(gemm(*call.cx, false, false, m, n, 2 * k, T(1), Ap, m, B1, 2 * k, T(0), Pr, m, call.st,
-                        call.sum),
-                   worst) &&
-        keep_going(gemm(*call.cx, false, false, m, n, 2 * k, T(1), Ap, m, B2, 2 * k, T(0), Pi, m, call.st,
-                        call.sum),
-                   worst)) {
-      if (!cuda_ok(launch_combine_complex<T>(Pr, Pi, m, m, n, ar, ai, br, bi, C.ptr, ldc_c, call.st), "combine"))
-        worst = EB2_ERR_CUDA;
-      call.sum.launches += 1;
-    }
-    rc = worst;
-  }
+  const int rc = complex_gemm_device<T>(*call.cx, oa, ob, m, n, k, ar, ai, A.ptr, A.ld / 2, B.ptr, B.ld / 2, br, bi,
+                                        C.ptr, C.ld / 2, call.st, call.sum);
   call.end(rc, A.staged || B.staged || C.staged, C, c, 2 * ldc, 2 * m, n);
+}
+
+// blas/level3_impl.h:507-592 (symm, ISCOMPLEX: the symmetric matrix, no conjugation) and
+// :760-831 (hemm: the Hermitian matrix, the diagonal's real part): C := alpha S B + beta C
+// (left) or alpha B S + beta C (right).  beta scales C first (0: zeros).
+template <typename T>
+void blas_complex_symm(bool hermitian, char side, char uplo, int64_t m, int64_t n, const T* alpha, const T* a,
+                       int64_t lda, const T* b, int64_t ldb, const T* beta, T* c, int64_t ldc) {
+  int info = symm_info(side, uplo, m, n, lda, ldb, ldc);
+  if (info)
+    return xerbla_(hermitian ? prefixed<T>("ZHEMM ", "CHEMM ") : prefixed<T>("ZSYMM ", "CSYMM "), &info, 6);
+  if (m == 0 || n == 0) return;
+  count_call(hermitian ? prefixed<T>("zhemm", "chemm") : prefixed<T>("zsymm", "csymm"));
+  Call call(dtype_of<T>() == 'd' ? 'z' : 'c');
+  if (!call.begin()) return;
+  const bool left = side_code(side) == kLeft;
+  const int64_t size = left ? m : n;
+  const bool need_ab = alpha[0] != T(0) || alpha[1] != T(0);
+  const bool beta_zero = beta[0] == T(0) && beta[1] == T(0);
+  Operand<T> A, B, C;
+  if (!stage(call.cx->stage_a, a, 2 * lda, need_ab ? 2 * size : 0, size, true, call.st, A) ||
+      !stage(call.cx->stage_b, b, 2 * ldb, need_ab ? 2 * m : 0, n, true, call.st, B) ||
+      !stage(call.cx->stage_c, c, 2 * ldc, 2 * m, n, !beta_zero, call.st, C))
+    return call.fail();
+  call.started();
+  const int rc = complex_symm_device<T>(*call.cx, hermitian, left, uplo_code(uplo) == kUp, m, n, alpha[0], alpha[1],
+                                        A.ptr, A.ld / 2, B.ptr, B.ld / 2, beta[0], beta[1], C.ptr, C.ld / 2, call.st,
+                                        call.sum);
+  call.end(rc, A.staged || B.staged || C.staged, C, c, 2 * ldc, 2 * m, n);
+}
+
+// blas/level3_impl.h:230-364 (trsm) and :368-503 (trmm) with Scalar = std::complex; op 'C'
+// is the conjugate transpose.
+template <typename T>
+void blas_complex_trxm(bool solve, char side, char uplo, char op, char diag, int64_t m, int64_t n, const T* alpha,
+                       const T* a, int64_t lda, T* b, int64_t ldb) {
+  int info = trxm_info(side, uplo, op, diag, m, n, lda, ldb);
+  if (info)
+    return xerbla_(solve ? prefixed<T>("ZTRSM ", "CTRSM ") : prefixed<T>("ZTRMM ", "CTRMM "), &info, 6);
+  if (m == 0 || n == 0) return;
+  count_call(solve ? prefixed<T>("ztrsm", "ctrsm") : prefixed<T>("ztrmm", "ctrmm"));
+  Call call(dtype_of<T>() == 'd' ? 'z' : 'c');
+  if (!call.begin()) return;
+  const bool left = side_code(side) == kLeft;
+  const int64_t size = left ? m : n;
+  Operand<T> A, B;
+  if (!stage(call.cx->stage_a, a, 2 * lda, 2 * size, size, true, call.st, A) ||
+      !stage(call.cx->stage_b, b, 2 * ldb, 2 * m, n, true, call.st, B))
+    return call.fail();
+  call.started();
+  const int rc = complex_trxm_device<T>(*call.cx, solve, left, uplo_code(uplo) == kUp, op_code(op),
+                                        diag_code(diag) == kUnit, m, n, alpha[0], alpha[1], A.ptr, A.ld / 2, B.ptr,
+                                        B.ld / 2, call.st, call.sum);
+  call.end(rc, A.staged || B.staged, B, b, 2 * ldb, 2 * m, n);
 }
 
 }  // namespace
 }  // namespace eb2
 
 using eb2::blas_complex_gemm;
+using eb2::blas_complex_symm;
+using eb2::blas_complex_trxm;
 using eb2::blas_gemmtr;
 using eb2::blas_symm;
 using eb2::blas_syr2k;
@@ -745,9 +902,33 @@ using eb2::blas_trxm;
     blas_complex_gemm<float>(*ta, *tb, *m, *n, *k, alpha, a, *lda, b, *ldb, beta, c, *ldc);                          \
   }
 
+// The complex level-3 routines Eigen's external-BLAS hooks bind (?trsm_, ?trmm_, ?hemm_) and
+// ?symm_: alpha, beta and the matrices as interleaved (re, im) pairs of the real type.
+#define EB2_COMPLEX_LEVEL3_SYMBOLS(I, SFX, P, R)                                                                     \
+  void P##symm##SFX(const char* side, const char* uplo, const I* m, const I* n, const R* alpha, const R* a,         \
+                    const I* lda, const R* b, const I* ldb, const R* beta, R* c, const I* ldc) {                     \
+    blas_complex_symm<R>(false, *side, *uplo, *m, *n, alpha, a, *lda, b, *ldb, beta, c, *ldc);                       \
+  }                                                                                                                  \
+  void P##hemm##SFX(const char* side, const char* uplo, const I* m, const I* n, const R* alpha, const R* a,         \
+                    const I* lda, const R* b, const I* ldb, const R* beta, R* c, const I* ldc) {                     \
+    blas_complex_symm<R>(true, *side, *uplo, *m, *n, alpha, a, *lda, b, *ldb, beta, c, *ldc);                        \
+  }                                                                                                                  \
+  void P##trmm##SFX(const char* side, const char* uplo, const char* op, const char* diag, const I* m, const I* n,   \
+                    const R* alpha, const R* a, const I* lda, R* b, const I* ldb) {                                  \
+    blas_complex_trxm<R>(false, *side, *uplo, *op, *diag, *m, *n, alpha, a, *lda, b, *ldb);                          \
+  }                                                                                                                  \
+  void P##trsm##SFX(const char* side, const char* uplo, const char* op, const char* diag, const I* m, const I* n,   \
+                    const R* alpha, const R* a, const I* lda, R* b, const I* ldb) {                                  \
+    blas_complex_trxm<R>(true, *side, *uplo, *op, *diag, *m, *n, alpha, a, *lda, b, *ldb);                           \
+  }
+
 extern "C" {
 EB2_LEVEL3_SYMBOLS(int, _)
 EB2_LEVEL3_SYMBOLS(int64_t, _64_)
 EB2_COMPLEX_GEMM_SYMBOLS(int, _)
 EB2_COMPLEX_GEMM_SYMBOLS(int64_t, _64_)
+EB2_COMPLEX_LEVEL3_SYMBOLS(int, _, z, double)
+EB2_COMPLEX_LEVEL3_SYMBOLS(int64_t, _64_, z, double)
+EB2_COMPLEX_LEVEL3_SYMBOLS(int, _, c, float)
+EB2_COMPLEX_LEVEL3_SYMBOLS(int64_t, _64_, c, float)
 }

@@ -117,6 +117,53 @@ void cgemm_64_(const char* transa, const char* transb, const int64_t* m, const i
                const float* alpha, const float* a, const int64_t* lda, const float* b, const int64_t* ldb,
                const float* beta, float* c, const int64_t* ldc);
 
+/* Complex level-3 routines (Eigen binds ?trsm_, ?trmm_ and ?hemm_ for complex operands under
+ * EIGEN_USE_BLAS: TriangularSolverMatrix_BLAS.h, TriangularMatrixMatrix_BLAS.h,
+ * SelfadjointMatrixMatrix_BLAS.h).  alpha, beta and the matrices hold interleaved (re, im)
+ * pairs; op 'C' is the conjugate transpose.  Replace blas/level3_impl.h's trsm (:230-364),
+ * trmm (:368-503), symm (:507-592) and hemm (:760-831) for std::complex, with their info codes
+ * and xerbla_ names ("ZTRSM ", "CHEMM ", ...); hemm takes the real part of A's diagonal. */
+void ztrsm_(const char* side, const char* uplo, const char* transa, const char* diag, const int* m, const int* n,
+            const double* alpha, const double* a, const int* lda, double* b, const int* ldb);
+void ctrsm_(const char* side, const char* uplo, const char* transa, const char* diag, const int* m, const int* n,
+            const float* alpha, const float* a, const int* lda, float* b, const int* ldb);
+void ztrmm_(const char* side, const char* uplo, const char* transa, const char* diag, const int* m, const int* n,
+            const double* alpha, const double* a, const int* lda, double* b, const int* ldb);
+void ctrmm_(const char* side, const char* uplo, const char* transa, const char* diag, const int* m, const int* n,
+            const float* alpha, const float* a, const int* lda, float* b, const int* ldb);
+void zhemm_(const char* side, const char* uplo, const int* m, const int* n, const double* alpha, const double* a,
+            const int* lda, const double* b, const int* ldb, const double* beta, double* c, const int* ldc);
+void chemm_(const char* side, const char* uplo, const int* m, const int* n, const float* alpha, const float* a,
+            const int* lda, const float* b, const int* ldb, const float* beta, float* c, const int* ldc);
+void zsymm_(const char* side, const char* uplo, const int* m, const int* n, const double* alpha, const double* a,
+            const int* lda, const double* b, const int* ldb, const double* beta, double* c, const int* ldc);
+void csymm_(const char* side, const char* uplo, const int* m, const int* n, const float* alpha, const float* a,
+            const int* lda, const float* b, const int* ldb, const float* beta, float* c, const int* ldc);
+void ztrsm_64_(const char* side, const char* uplo, const char* transa, const char* diag, const int64_t* m,
+               const int64_t* n, const double* alpha, const double* a, const int64_t* lda, double* b,
+               const int64_t* ldb);
+void ctrsm_64_(const char* side, const char* uplo, const char* transa, const char* diag, const int64_t* m,
+               const int64_t* n, const float* alpha, const float* a, const int64_t* lda, float* b,
+               const int64_t* ldb);
+void ztrmm_64_(const char* side, const char* uplo, const char* transa, const char* diag, const int64_t* m,
+               const int64_t* n, const double* alpha, const double* a, const int64_t* lda, double* b,
+               const int64_t* ldb);
+void ctrmm_64_(const char* side, const char* uplo, const char* transa, const char* diag, const int64_t* m,
+               const int64_t* n, const float* alpha, const float* a, const int64_t* lda, float* b,
+               const int64_t* ldb);
+void zhemm_64_(const char* side, const char* uplo, const int64_t* m, const int64_t* n, const double* alpha,
+               const double* a, const int64_t* lda, const double* b, const int64_t* ldb, const double* beta,
+               double* c, const int64_t* ldc);
+void chemm_64_(const char* side, const char* uplo, const int64_t* m, const int64_t* n, const float* alpha,
+               const float* a, const int64_t* lda, const float* b, const int64_t* ldb, const float* beta, float* c,
+               const int64_t* ldc);
+void zsymm_64_(const char* side, const char* uplo, const int64_t* m, const int64_t* n, const double* alpha,
+               const double* a, const int64_t* lda, const double* b, const int64_t* ldb, const double* beta,
+               double* c, const int64_t* ldc);
+void csymm_64_(const char* side, const char* uplo, const int64_t* m, const int64_t* n, const float* alpha,
+               const float* a, const int64_t* lda, const float* b, const int64_t* ldb, const float* beta, float* c,
+               const int64_t* ldc);
+
 void dgemmtr_64_(const char* uplo, const char* transa, const char* transb, const int64_t* n, const int64_t* k,
                  const double* alpha, const double* a, const int64_t* lda, const double* b, const int64_t* ldb,
                  const double* beta, double* c, const int64_t* ldc);

@@ -96,3 +96,28 @@ def test_complex_gemm_argument_errors_match_reference(ilp64, dtype):
         if got:
             assert rec.record_xerbla_last_name().decode() == dtype.upper() + "GEMM "
         assert np.all(sentinel == 7 + 7j)
+
+
+CLEVEL3_GOLDEN = Path(__file__).resolve().parent / "golden" / "complex_level3_golden.npz"
+
+
+@pytest.mark.parametrize("ilp64", [False, True])
+@pytest.mark.parametrize("dtype", ["z", "c"])
+def test_complex_level3_argument_errors_match_reference(ilp64, dtype):
+    """z/c trsm_, trmm_, symm_, hemm_: the reference's info codes and xerbla_ names."""
+    rec = load_xerbla_recorder()
+    errors = json.loads(bytes(np.load(CLEVEL3_GOLDEN)["meta"]).decode())["errors"]
+    sentinel = np.full(256, 7 + 7j, dtype=np.complex128 if dtype == "z" else np.complex64)
+    seen = {}
+    for e in errors:
+        values = [sentinel if v is None else v for v in e["values"]]
+        rec.record_xerbla_reset()
+        eb.level3(dtype + e["routine"], *values, ilp64=ilp64)
+        got = rec.record_xerbla_last_info() if rec.record_xerbla_calls() else 0
+        assert got == e["info"], e
+        if got:
+            assert rec.record_xerbla_last_name().decode() == dtype.upper() + e["name"][1:], e
+        seen.setdefault(e["routine"], set()).add(got)
+        assert np.all(sentinel == 7 + 7j)
+    assert seen["trsm"] == seen["trmm"] == {0, 1, 2, 3, 4, 5, 6, 9, 11}
+    assert seen["hemm"] == seen["symm"] == {0, 1, 2, 3, 4, 7, 9, 12}
