@@ -2,10 +2,10 @@
 // libeigen_b200.so through the external-BLAS seam.
 //
 // Compiled against the Eigen headers with -DEIGEN_USE_BLAS, so the *_BLAS.h headers of
-// Eigen/src/Core/products re-specialise Eigen's triangular solve (dtrsm_), triangular product
-// (dtrmm_), self-adjoint product (dsymm_), rank update (dsyrk_) and complex product (zgemm_)
-// to call the external BLAS symbols; linked with libeigen_b200.so first, they resolve to this
-// project's B200 routines.  Blocked LLT and PartialPivLU reach dtrsm_, dsyrk_ and dgemm_ from
+// Eigen/src/Core/products re-specialise Eigen's triangular solve (dtrsm_, ztrsm_), triangular
+// product (dtrmm_, ztrmm_), self-adjoint product (dsymm_, zhemm_), rank update (dsyrk_) and
+// complex product (zgemm_) to call the external BLAS symbols; linked with libeigen_b200.so
+// first, they resolve to this project's B200 routines.  Blocked LLT and PartialPivLU reach dtrsm_, dsyrk_ and dgemm_ from
 // inside Eigen's own algorithms.
 //
 // Each result is checked against a plain computation (residuals for the solves, an unblocked
@@ -100,19 +100,42 @@ int main(int argc, char** argv) {
   const MatrixXcd Z = Z1 * Z2;
   const double e_zgemm = rel(Z, naive(Z1, Z2));
 
+  // complex: Hermitian positive definite LLT (ztrsm_ inside), a triangular solve (ztrsm_), a
+  // triangular product (ztrmm_) and a self-adjoint product (zhemm_)
+  MatrixXcd ZA = MatrixXcd::Random(n, n);
+  MatrixXcd ZH = ZA * ZA.adjoint();
+  ZH.diagonal().array() += double(n);
+  const MatrixXcd ZB = MatrixXcd::Random(n, r);
+  Eigen::LLT<MatrixXcd> zllt(ZH);
+  const MatrixXcd ZX = zllt.solve(ZB);
+  const double e_zllt_solve = rel(naive(ZH, ZX), ZB);
+  MatrixXcd ZT = ZA.triangularView<Eigen::Upper>();
+  ZT.diagonal().array() += double(n) / 4;
+  const MatrixXcd ZX2 = ZT.triangularView<Eigen::Upper>().solve(ZB);
+  const double e_ztrsm = rel(naive(ZT, ZX2), ZB);
+  const MatrixXcd ZP = ZT.triangularView<Eigen::Upper>() * ZB;
+  const double e_ztrmm = rel(ZP, naive(ZT, ZB));
+  MatrixXcd ZHl = ZH.triangularView<Eigen::Lower>();
+  const MatrixXcd ZQ = ZHl.selfadjointView<Eigen::Lower>() * ZB;
+  const double e_zhemm = rel(ZQ, naive(ZH, ZB));
+
   const long long c_gemm = eb2_routine_calls("dgemm"), c_trsm = eb2_routine_calls("dtrsm"),
                   c_trmm = eb2_routine_calls("dtrmm"), c_symm = eb2_routine_calls("dsymm"),
-                  c_syrk = eb2_routine_calls("dsyrk"), c_zgemm = eb2_routine_calls("zgemm");
+                  c_syrk = eb2_routine_calls("dsyrk"), c_zgemm = eb2_routine_calls("zgemm"),
+                  c_ztrsm = eb2_routine_calls("ztrsm"), c_ztrmm = eb2_routine_calls("ztrmm"),
+                  c_zhemm = eb2_routine_calls("zhemm");
   std::printf(
       "{\"n\": %d, \"rhs\": %d, \"err_llt\": %.3e, \"err_llt_solve\": %.3e, \"err_lu_solve\": %.3e, "
       "\"err_trsm\": %.3e, \"err_trmm\": %.3e, \"err_symm\": %.3e, \"err_syrk\": %.3e, \"err_zgemm\": %.3e, "
+      "\"err_zllt_solve\": %.3e, \"err_ztrsm\": %.3e, \"err_ztrmm\": %.3e, \"err_zhemm\": %.3e, "
       "\"calls\": {\"dgemm\": %lld, \"dtrsm\": %lld, \"dtrmm\": %lld, \"dsymm\": %lld, \"dsyrk\": %lld, "
-      "\"zgemm\": %lld}, \"last_error\": %d}\n",
-      n, r, e_llt, e_llt_solve, e_lu_solve, e_trsm, e_trmm, e_symm, e_syrk, e_zgemm, c_gemm, c_trsm, c_trmm, c_symm,
-      c_syrk, c_zgemm, eb2_last_error());
+      "\"zgemm\": %lld, \"ztrsm\": %lld, \"ztrmm\": %lld, \"zhemm\": %lld}, \"last_error\": %d}\n",
+      n, r, e_llt, e_llt_solve, e_lu_solve, e_trsm, e_trmm, e_symm, e_syrk, e_zgemm, e_zllt_solve, e_ztrsm, e_ztrmm,
+      e_zhemm, c_gemm, c_trsm, c_trmm, c_symm, c_syrk, c_zgemm, c_ztrsm, c_ztrmm, c_zhemm, eb2_last_error());
   const double tol = 1e-13;
   const bool ok = e_llt < tol && e_llt_solve < tol && e_lu_solve < 1e-11 && e_trsm < tol && e_trmm < tol &&
-                  e_symm < tol && e_syrk < tol && e_zgemm < tol && c_gemm > 0 && c_trsm > 0 && c_trmm > 0 &&
-                  c_symm > 0 && c_syrk > 0 && c_zgemm > 0 && eb2_last_error() == 0;
+                  e_symm < tol && e_syrk < tol && e_zgemm < tol && e_zllt_solve < tol && e_ztrsm < tol &&
+                  e_ztrmm < tol && e_zhemm < tol && c_gemm > 0 && c_trsm > 0 && c_trmm > 0 && c_symm > 0 &&
+                  c_syrk > 0 && c_zgemm > 0 && c_ztrsm > 0 && c_ztrmm > 0 && c_zhemm > 0 && eb2_last_error() == 0;
   return ok ? 0 : 1;
 }

@@ -36,9 +36,10 @@ SOLVERS = Path(__file__).resolve().parent / "eigen_seam" / "_bin" / "eigen_seam_
 @pytest.mark.parametrize("n,rhs", [(600, 96), (1500, 300)])
 def test_eigen_decompositions_route_level3_routines_to_library(n, rhs):
     """Eigen's blocked LLT and PartialPivLU, a triangular solve, a triangular product, a
-    self-adjoint product, a rank update and a complex product, compiled with EIGEN_USE_BLAS:
-    each result checks out and dtrsm_, dtrmm_, dsymm_, dsyrk_, dgemm_ and zgemm_ ran in the
-    library (its per-routine counters)."""
+    self-adjoint product, a rank update, a complex product, and complex LLT, triangular solve,
+    triangular product and self-adjoint product, compiled with EIGEN_USE_BLAS: each result
+    checks out and dtrsm_, dtrmm_, dsymm_, dsyrk_, dgemm_, zgemm_, ztrsm_, ztrmm_ and zhemm_ ran
+    in the library (its per-routine counters)."""
     if not SOLVERS.exists():
         pytest.fail(f"{SOLVERS} missing: build it with `make -C tests/eigen_seam if-present`")
     r = subprocess.run([str(SOLVERS), str(n), str(rhs)], capture_output=True, text=True, timeout=600)
@@ -46,7 +47,8 @@ def test_eigen_decompositions_route_level3_routines_to_library(n, rhs):
     assert line, r.stdout + r.stderr
     out = json.loads(line[-1])
     assert r.returncode == 0, out
-    for key in ("err_llt", "err_llt_solve", "err_trsm", "err_trmm", "err_symm", "err_syrk", "err_zgemm"):
+    for key in ("err_llt", "err_llt_solve", "err_trsm", "err_trmm", "err_symm", "err_syrk", "err_zgemm",
+                "err_zllt_solve", "err_ztrsm", "err_ztrmm", "err_zhemm"):
         assert out[key] < 1e-13, (key, out)
     assert out["err_lu_solve"] < 1e-11, out
     assert all(v > 0 for v in out["calls"].values()), out
