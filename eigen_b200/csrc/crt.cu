@@ -191,23 +191,27 @@ __global__ void __launch_bounds__(256) crt_scan_norm_kernel(const double* __rest
     tile[rr][ll] = (r < rows && l < cols) ? X[r * sr + l * sl] : 0.0;
   }
   __syncthreads();
-  // 8 threads per row, 16 columns each, reduced with shuffles inside each 8-lane group
+  // 8 threads per row, reduced with shuffles inside each 8-lane group; thread `sub` takes
+  // columns sub, sub + 8, ..., so that the 8 lanes of a row read 8 consecutive words of the
+  // tile (no shared-memory bank conflicts)
   const int rr = threadIdx.x >> 3;
   const int sub = threadIdx.x & 7;
-  const int cb = sub * 16;
   const int64_t r = r0 + rr;
-  unsigned long long mb = 0;
+  unsigned long long mb = 0, mb64 = 0;
   int esum = 0, ecnt = 0;
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
-    const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(fabs(tile[rr][cb + j])));
+    const unsigned long long bits =
+        static_cast<unsigned long long>(__double_as_longlong(fabs(tile[rr][sub + 8 * j])));
     mb = bits > mb ? bits : mb;
-    if (bits && sub < 4) {  // the first 64 columns, for the spread statistic
-      esum += int(bits >> 52);
-      ++ecnt;
+    if (j < 8) {  // the first 64 columns, for the spread statistic
+      mb64 = bits > mb64 ? bits : mb64;
+      if (bits) {
+        esum += int(bits >> 52);
+        ++ecnt;
+      }
     }
   }
-  unsigned long long mb64 = sub < 4 ? mb : 0ull;
 #pragma unroll
   for (int o = 4; o > 0; o >>= 1) {
     const unsigned long long other = __shfl_xor_sync(0xffffffffu, mb, o);
@@ -223,7 +227,7 @@ __global__ void __launch_bounds__(256) crt_scan_norm_kernel(const double* __rest
     e = frexp_exp(mb);
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-      const double x = tile[rr][cb + j];
+      const double x = tile[rr][sub + 8 * j];
       if (x != 0.0) {
         const double xs = scale2(x, -e);
         s += static_cast<unsigned long long>(ceil(__dmul_rn(__dmul_rn(xs, xs), 4294967296.0))) + 1ull;
@@ -402,9 +406,19 @@ __global__ void __launch_bounds__(kSplitThreadsCrt) crt_split_kernel(
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
     // |v| <= 2^b, an exact integer (0 in zero rows: 2^kCrtZeroRow underflows to 0)
-    const double v = trunc(scale2(tile[rr][cb + j], m));
-    ch[j] = chunks21(fabs(v));
-    neg |= (v < 0.0 ? 1u : 0u) << j;
+    const double x = scale2(tile[rr][cb + j], m);
+    if constexpr (kWide) {
+      const double v = trunc(x);
+      ch[j] = chunks21(fabs(v));
+      neg |= (v < 0.0 ? 1u : 0u) << j;
+    } else {
+      // |v| <= 2^62 fits an int64: one conversion (toward zero, i.e. trunc) and integer
+      // shifts give the same 21-bit chunks as chunks21()
+      const long long v = __double2ll_rz(x);
+      const unsigned long long a = v < 0 ? 0ull - static_cast<unsigned long long>(v) : static_cast<unsigned long long>(v);
+      ch[j] = Chunks21{uint32_t(a & 0x1FFFFFull), uint32_t((a >> 21) & 0x1FFFFFull), uint32_t(a >> 42), 0u};
+      neg |= (v < 0 ? 1u : 0u) << j;
+    }
   }
   int8_t* dst = residues + (size_t(r0 + rr)) * size_t(k_pad) + size_t(l0 + cb);
   const size_t plane = size_t(rows_pad) * size_t(k_pad);
