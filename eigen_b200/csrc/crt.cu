@@ -289,9 +289,11 @@ __global__ void __launch_bounds__(256) crt_mu_kernel(const unsigned long long* _
   mu[r] = m;
 }
 
-// Per-modulus constants: p, floor((2^32 - 1) / p) for mod_small, and 2^21, 2^42, 2^63 mod p.
+// Per-modulus constants: p, floor((2^32 - 1) / p) for mod_small, 2^21, 2^42, 2^63 and 2^32
+// mod p, and RN(1/p).
 struct CrtModConst {
-  uint32_t p, magic, c21, c42, c63;
+  uint32_t p, magic, c21, c42, c63, c32;
+  double inv_p;
 };
 __host__ __device__ constexpr uint32_t pow2_mod_const(int s, uint32_t p) {
   uint32_t v = 1u % p;
@@ -299,9 +301,13 @@ __host__ __device__ constexpr uint32_t pow2_mod_const(int s, uint32_t p) {
   return v;
 }
 __host__ __device__ constexpr CrtModConst crt_mod_const(int l) {
-  return CrtModConst{uint32_t(crt_modulus(l)), 0xFFFFFFFFu / uint32_t(crt_modulus(l)),
-                     pow2_mod_const(21, uint32_t(crt_modulus(l))), pow2_mod_const(42, uint32_t(crt_modulus(l))),
-                     pow2_mod_const(63, uint32_t(crt_modulus(l)))};
+  return CrtModConst{uint32_t(crt_modulus(l)),
+                     0xFFFFFFFFu / uint32_t(crt_modulus(l)),
+                     pow2_mod_const(21, uint32_t(crt_modulus(l))),
+                     pow2_mod_const(42, uint32_t(crt_modulus(l))),
+                     pow2_mod_const(63, uint32_t(crt_modulus(l))),
+                     pow2_mod_const(32, uint32_t(crt_modulus(l))),
+                     1.0 / double(crt_modulus(l))};
 }
 static_assert(kCrtMaxModuli == 20, "constant table below");
 __constant__ CrtModConst kModConst[kCrtMaxModuli] = {
@@ -336,20 +342,15 @@ constexpr int kSplitColsCrt = 128;
 
 constexpr int kSplitThreadsCrt = 512;  // 16 threads per row, 8 entries each
 
-// |t| mod p for |t| < 2^63 (at most 16 moduli: |t| <= 2^62) without the 2^63 chunk
-__device__ __forceinline__ uint32_t residue_of3(const Chunks21& c, const CrtModConst& k) {
-  return mod_small(c.a0 + c.a1 * k.c21 + c.a2 * k.c42, k.p, k.magic);
-}
-
-// The 8 symmetric residues of one thread's entries for one modulus, packed into 8 bytes.
-template <bool kWide>
-__device__ __forceinline__ void store_residues(const CrtModConst& k, const Chunks21 (&ch)[8], uint32_t neg,
-                                               int8_t* dst) {
+// The 8 symmetric residues of one thread's entries for one modulus, from 21-bit chunks of
+// |t| < 2^84 (more than 16 moduli), packed into 8 bytes.
+__device__ __forceinline__ void store_residues_wide(const CrtModConst& k, const Chunks21 (&ch)[8], uint32_t neg,
+                                                    int8_t* dst) {
   const int hi = int(k.p >> 1) - ((k.p & 1u) ? 0 : 1);  // largest representative kept as is
   uint32_t w[2] = {0u, 0u};
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
-    const int res = int(kWide ? residue_of(ch[j], k) : residue_of3(ch[j], k));
+    const int res = int(residue_of(ch[j], k));
     int sres = res > hi ? res - int(k.p) : res;  // symmetric residue of |t|: [-(p/2), (p-1)/2]
     // of -|t|: its negation (for p = 256, 128 packs to the same byte as -128)
     if ((neg >> j) & 1u) sres = -sres;
@@ -358,22 +359,74 @@ __device__ __forceinline__ void store_residues(const CrtModConst& k, const Chunk
   *reinterpret_cast<uint2*>(dst) = make_uint2(w[0], w[1]);
 }
 
+// An entry t = trunc(2^mu x) with |t| <= 2^62 (at most 16 moduli) as hi 2^32 + lo (hi signed,
+// lo unsigned) and as the exact doubles of hi and lo.  1.5 2^52 + k has the bit pattern of
+// 1.5 2^52 plus k for |k| < 2^51, so each conversion is one integer add and one FP64 add.
+struct SplitEntry {
+  int32_t hi;
+  uint32_t lo;
+  double dh, dl;
+};
+__device__ __forceinline__ SplitEntry split_entry(long long t) {
+  SplitEntry e;
+  e.hi = int32_t(t >> 32);
+  e.lo = uint32_t(t);
+  e.dh = __longlong_as_double(0x4338000000000000ll + e.hi) - 0x1.8p52;
+  e.dl = __longlong_as_double(0x4338000000000000ll + e.lo) - 0x1.8p52;
+  return e;
+}
+
+// The symmetric residue of t for an odd modulus p, in [-(p-1)/2, (p-1)/2], as a 32-bit two's
+// complement.  s = hi c32 + lo (c32 = 2^32 mod p) is congruent to t, and |s| < 2^38 + 2^32 is
+// exact in FP64.  One FMA with 1.5 2^52 rounds s/p to the nearest integer q, left in the low
+// word of its result: RN(1/p) moves s/p by less than 2^-21, and for odd p the distance of s/p
+// from a half-integer is at least 1/(2p), so q is the exact rounding.  s - q p, a small
+// integer, is then computed modulo 2^32 from the integer parts.  The division work runs on
+// the FP64 pipe and leaves two integer multiply-adds, where a 32-bit Barrett reduction of
+// chunk sums takes four multiplies and a centring step.
+__device__ __forceinline__ uint32_t symmetric_residue(const SplitEntry& e, const CrtModConst& k, double c32d) {
+  const double s = fma(e.dh, c32d, e.dl);
+  const uint32_t q = uint32_t(__double2loint(fma(s, k.inv_p, 0x1.8p52)));
+  return e.lo + uint32_t(e.hi) * k.c32 - q * k.p;
+}
+
+__device__ __forceinline__ uint32_t pack_low_bytes(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
+}
+
+// The 8 symmetric residues of one thread's entries for one modulus, packed into 8 bytes.  For
+// p = 256 the residue of t is its low byte read as int8 (the representative in [-128, 127]).
+__device__ __forceinline__ void store_residues(const CrtModConst& k, const SplitEntry (&e)[8], int8_t* dst) {
+  uint32_t r[8];
+  if ((k.p & (k.p - 1u)) == 0u) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) r[j] = e[j].lo;
+  } else {
+    const double c32d = double(k.c32);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) r[j] = symmetric_residue(e[j], k, c32d);
+  }
+  *reinterpret_cast<uint2*>(dst) =
+      make_uint2(pack_low_bytes(r[0], r[1], r[2], r[3]), pack_low_bytes(r[4], r[5], r[6], r[7]));
+}
+
 // Moduli L .. NT-1 with their constants as compile-time immediates.
-template <int L, int NT, bool kWide>
-__device__ __forceinline__ void store_residues_static(const Chunks21 (&ch)[8], uint32_t neg, int8_t* dst,
-                                                      size_t plane) {
+template <int L, int NT>
+__device__ __forceinline__ void store_residues_static(const SplitEntry (&e)[8], int8_t* dst, size_t plane) {
   if constexpr (L < NT) {
     constexpr CrtModConst k = crt_mod_const(L);
-    store_residues<kWide>(k, ch, neg, dst + size_t(L) * plane);
-    store_residues_static<L + 1, NT, kWide>(ch, neg, dst, plane);
+    store_residues(k, e, dst + size_t(L) * plane);
+    store_residues_static<L + 1, NT>(e, dst, plane);
   }
 }
 
 // Residues of A' = trunc(2^mu_r x) for moduli [0, n): plane l at residues + l*rows_pad*k_pad,
 // row r contiguous along k; symmetric int8 representatives (mu from crt_mu_kernel).
 // NT > 0: the modulus count is NT (constants as immediates); NT = 0: n, read at run time.
+// Two blocks per SM (64 registers, a few bytes spilled) run faster than one block with the
+// 84 registers the compiler would take otherwise.
 template <bool kWide, int NT>  // kWide: |t| may reach 2^63 (more than 16 moduli)
-__global__ void __launch_bounds__(kSplitThreadsCrt) crt_split_kernel(
+__global__ void __launch_bounds__(kSplitThreadsCrt, 2) crt_split_kernel(
     const double* __restrict__ X, int64_t rows, int64_t cols, int64_t sr, int64_t sl,
     const int32_t* __restrict__ mu, int n, int8_t* __restrict__ residues, int64_t rows_pad, int64_t k_pad) {
   __shared__ double tile[kSplitRowsCrt][kSplitColsCrt + 1];
@@ -401,31 +454,28 @@ __global__ void __launch_bounds__(kSplitThreadsCrt) crt_split_kernel(
   const int rr = threadIdx.x >> 4;
   const int cb = (threadIdx.x & 15) * 8;
   const int m = row_mu_s[rr];
-  Chunks21 ch[8];
-  uint32_t neg = 0;
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    // |v| <= 2^b, an exact integer (0 in zero rows: 2^kCrtZeroRow underflows to 0)
-    const double x = scale2(tile[rr][cb + j], m);
-    if constexpr (kWide) {
-      const double v = trunc(x);
-      ch[j] = chunks21(fabs(v));
-      neg |= (v < 0.0 ? 1u : 0u) << j;
-    } else {
-      // |v| <= 2^62 fits an int64: one conversion (toward zero, i.e. trunc) and integer
-      // shifts give the same 21-bit chunks as chunks21()
-      const long long v = __double2ll_rz(x);
-      const unsigned long long a = v < 0 ? 0ull - static_cast<unsigned long long>(v) : static_cast<unsigned long long>(v);
-      ch[j] = Chunks21{uint32_t(a & 0x1FFFFFull), uint32_t((a >> 21) & 0x1FFFFFull), uint32_t(a >> 42), 0u};
-      neg |= (v < 0 ? 1u : 0u) << j;
-    }
-  }
   int8_t* dst = residues + (size_t(r0 + rr)) * size_t(k_pad) + size_t(l0 + cb);
   const size_t plane = size_t(rows_pad) * size_t(k_pad);
-  if constexpr (NT > 0) {
-    store_residues_static<0, NT, kWide>(ch, neg, dst, plane);
+  if constexpr (kWide) {
+    Chunks21 ch[8];
+    uint32_t neg = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      // |v| <= 2^b, an exact integer (0 in zero rows: 2^kCrtZeroRow underflows to 0)
+      const double v = trunc(scale2(tile[rr][cb + j], m));
+      ch[j] = chunks21(fabs(v));
+      neg |= (v < 0.0 ? 1u : 0u) << j;
+    }
+    for (int l = 0; l < n; ++l) store_residues_wide(kModConst[l], ch, neg, dst + size_t(l) * plane);
   } else {
-    for (int l = 0; l < n; ++l) store_residues<kWide>(kModConst[l], ch, neg, dst + size_t(l) * plane);
+    SplitEntry e[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) e[j] = split_entry(__double2ll_rz(scale2(tile[rr][cb + j], m)));  // trunc
+    if constexpr (NT > 0) {
+      store_residues_static<0, NT>(e, dst, plane);
+    } else {
+      for (int l = 0; l < n; ++l) store_residues(kModConst[l], e, dst + size_t(l) * plane);
+    }
   }
 }
 
