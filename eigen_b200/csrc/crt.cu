@@ -543,6 +543,43 @@ __host__ __device__ constexpr CrtTable make_crt_table() {
 }
 __constant__ CrtTable kCrtTable = make_crt_table();
 
+// Moduli 2g and 2g+1 share the factor Q_g = P / (p_2g p_2g+1) of their weights:
+// W_2g = Q_g X_2g and W_2g+1 = Q_g X_2g+1 with X_2g = p_2g+1 ((P/p_2g)^-1 mod p_2g) and
+// X_2g+1 = p_2g ((P/p_2g+1)^-1 mod p_2g+1), both below p_2g p_2g+1 < 2^16.  A last unpaired
+// modulus has Q = P/p and X = (P/p)^-1 mod p.  Then S = sum_l r_l W_l = sum_g Q_g R_g with
+// R_g = r_2g X_2g + r_2g+1 X_2g+1 < 2^25: the same S, with 32-bit multiply-adds for R_g and
+// half as many 64-bit ones for the 128-bit part.  Up to 16 moduli (P < 2^128).
+struct CrtPairTable {
+  uint32_t X[kCrtMaxModuli + 1][kCrtMaxModuli];
+  uint32_t Q[kCrtMaxModuli + 1][kCrtMaxModuli / 2][4];
+};
+__host__ __device__ constexpr CrtPairTable make_crt_pair_table() {
+  CrtPairTable t{};
+  for (int n = 1; n <= 16; ++n) {
+    uint32_t P[kCrtLimbs] = {1, 0, 0, 0, 0, 0};
+    for (int l = 0; l < n; ++l) ct_mul_small(P, uint32_t(crt_modulus(l)));
+    for (int g = 0; 2 * g < n; ++g) {
+      const bool pair = 2 * g + 1 < n;
+      const uint32_t pa = uint32_t(crt_modulus(2 * g)), pb = pair ? uint32_t(crt_modulus(2 * g + 1)) : 1u;
+      uint32_t Q[kCrtLimbs] = {P[0], P[1], P[2], P[3], P[4], P[5]};
+      (void)ct_div_small(Q, pa);
+      uint32_t Ma[kCrtLimbs] = {Q[0], Q[1], Q[2], Q[3], Q[4], Q[5]};  // P / p_a
+      const uint32_t ma = ct_div_small(Ma, pa);                        // (P / p_a) mod p_a
+      t.X[n][2 * g] = pb * ct_inverse_mod(ma, pa);
+      if (pair) {
+        uint32_t Mb[kCrtLimbs] = {P[0], P[1], P[2], P[3], P[4], P[5]};
+        (void)ct_div_small(Mb, pb);
+        const uint32_t mb = ct_div_small(Mb, pb);  // (P / p_b) mod p_b
+        t.X[n][2 * g + 1] = pa * ct_inverse_mod(mb, pb);
+        (void)ct_div_small(Q, pb);
+      }
+      for (int q = 0; q < 4; ++q) t.Q[n][g][q] = Q[q];
+    }
+  }
+  return t;
+}
+__constant__ CrtPairTable kCrtPairs = make_crt_pair_table();
+
 struct CrtRecParams {
   uint32_t W[kCrtMaxModuli][kCrtLimbs];
   uint32_t P[kCrtLimbs];
@@ -788,11 +825,16 @@ __global__ void __launch_bounds__(256) crt_reconstruct128_kernel(const __grid_co
 #pragma unroll
         for (int l = 0; l < N; ++l) rn[l] = res[(j + 1) * ld_res + i + l * plane];
       }
+      // S = sum_g Q_g R_g in four 32-bit limb columns (each < 8 * 2^25 * 2^32 = 2^60); S itself
+      // (< 2^28 P) may pass 2^128, and the 128-bit arithmetic below works modulo 2^128, which
+      // leaves the small remainder S - q P exact
       unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
 #pragma unroll
-      for (int l = 0; l < N; ++l) {
+      for (int g = 0; 2 * g < N; ++g) {
+        uint32_t Rg = rc[2 * g] * kCrtPairs.X[N][2 * g];
+        if (2 * g + 1 < N) Rg += rc[2 * g + 1] * kCrtPairs.X[N][2 * g + 1];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[q] += static_cast<unsigned long long>(rc[l]) * kCrtTable.W[N][l][q];
+        for (int q = 0; q < 4; ++q) acc[q] += static_cast<unsigned long long>(Rg) * kCrtPairs.Q[N][g][q];
       }
       // q = rint(S / P) from the partial sums in FP64; it may be off by one near a
       // half-integer, which the range fix below absorbs

@@ -55,7 +55,7 @@ SHAPES = [("N", "N", 130, 300, 257), ("T", "N", 64, 64, 1000), ("N", "T", 333, 1
 
 @pytest.mark.parametrize("ta,tb,m,n,k", SHAPES)
 @pytest.mark.parametrize("moduli,tile_n,beta", [(16, 256, 0.0), (16, 512, 0.5), (20, 256, -1.25), (8, 512, 0.0),
-                                                (18, 256, 0.75)])
+                                                (18, 256, 0.75), (11, 256, 0.25), (15, 512, 0.0)])
 def test_crt_bit_exact_vs_oracle_model(ta, tb, m, n, k, moduli, tile_n, beta):
     A, lda, B, ldb, C, ldc = make_operands(m, n, k, ta, tb, pad=3, r=4, seed=m + n + k + moduli)
     eb.set_dgemm_moduli(moduli)
