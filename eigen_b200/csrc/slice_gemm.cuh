@@ -509,6 +509,10 @@ __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull
       if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, true)) continue;
       const uint32_t pm = uint32_t(crt_modulus(t));
       const uint32_t magic = 0xFFFFFFFFu / pm;
+      // |v| <= 1023 * 128 * 128 * 128 = 2^31 - 2^21 for an accumulation unit, so with bias a
+      // multiple of p in [2^31 - 2^21, 2^31 - 2^21 + p), v + bias lies in [0, 2^32) and
+      // (v + bias) mod p = v mod p: one reduction of an unsigned word, no sign handling
+      const uint32_t bias = (0x7FE00000u + pm - 1u) / pm * pm;
       uint8_t* rp = P.residues + int64_t(t) * plane + grow;
       for (int u0 = 0; u0 < total && ok; u0 += kMaxUnitKbCrt) {
         if (!mbar_wait(&tfull[buf], (ephase >> buf) & 1u, abort_flag, P.status)) {
@@ -523,12 +527,10 @@ __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull
           tmem_ld_32x32b_x32(taddr + uint32_t(c * 32), r);
           tmem_ld_wait();
           if (grow < P.ld_res) {
+            uint8_t* dst = rp + (n0 + c * 32) * P.ld_res;
 #pragma unroll
-            for (int jj = 0; jj < 32; ++jj) {
-              const int32_t v = static_cast<int32_t>(r[jj]);
-              uint32_t res = mod_small(v < 0 ? 0u - uint32_t(v) : uint32_t(v), pm, magic);
-              if (v < 0 && res) res = pm - res;
-              uint8_t* dst = rp + (n0 + c * 32 + jj) * P.ld_res;
+            for (int jj = 0; jj < 32; ++jj, dst += P.ld_res) {
+              uint32_t res = mod_small(r[jj] + bias, pm, magic);
               if (u0 > 0) {
                 res += *dst;
                 if (res >= pm) res -= pm;
