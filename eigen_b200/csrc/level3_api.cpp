@@ -381,7 +381,9 @@ int complex_gemm_device(Context& cx, int oa, int ob, int64_t m, int64_t n, int64
                ? EB2_OK
                : EB2_ERR_CUDA;
   }
-  // workspace: A' (m x 2k), B1 and B2 (2k x n), Pr and Pi (m x n)
+  // workspace: A' (m x 2k), B1 and B2 (2k x n), Pr and Pi (m x n); B1 | B2 and Pr | Pi are
+  // adjacent, so the two real products are one product of width 2n, and A' is scanned and
+  // split once
   const size_t e_a = size_t(m) * 2 * k, e_b = size_t(2 * k) * n, e_p = size_t(m) * n;
   if (!cx.cplx.ensure((e_a + 2 * e_b + 2 * e_p) * sizeof(T))) {
     set_error(EB2_ERR_ALLOC, "could not allocate the complex-product workspace");
@@ -401,8 +403,7 @@ int complex_gemm_device(Context& cx, int oa, int ob, int64_t m, int64_t n, int64
   if (!ok) return EB2_ERR_CUDA;
   sum.launches += 2;
   int worst = EB2_OK;
-  if (keep_going(gemm(cx, false, false, m, n, 2 * k, T(1), Ap, m, B1, 2 * k, T(0), Pr, m, st, sum), worst) &&
-      keep_going(gemm(cx, false, false, m, n, 2 * k, T(1), Ap, m, B2, 2 * k, T(0), Pi, m, st, sum), worst)) {
+  if (keep_going(gemm(cx, false, false, m, 2 * n, 2 * k, T(1), Ap, m, B1, 2 * k, T(0), Pr, m, st, sum), worst)) {
     if (!cuda_ok(launch_combine_complex<T>(Pr, Pi, m, m, n, ar, ai, br, bi, C, ldc, st), "combine"))
       worst = EB2_ERR_CUDA;
     sum.launches += 1;
