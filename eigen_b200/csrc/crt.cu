@@ -597,6 +597,8 @@ struct CrtRecParams {
   double* err_sq;  // [0] += estimated squared error, [1] += squared alpha*A*B entries
   const int* skip_if_flag;
   int write_c;
+  double* save;
+  int64_t ld_save;
   int cols_per_block;  // columns one block handles per pass (fewer when the grid would be small)
   int uplo;            // 0: all of C; 1: i <= j only; 2: i >= j only
 };
@@ -642,6 +644,8 @@ struct CrtStoreCtx {
   double alpha, beta;
   double* C;
   int64_t ldc;
+  double* save;
+  int64_t ld_save;
   const int32_t* mu_a;
   const int32_t* mu_b;
   int b;
@@ -649,7 +653,8 @@ struct CrtStoreCtx {
 };
 
 __device__ __forceinline__ CrtStoreCtx store_ctx(const CrtRecParams& R) {
-  return CrtStoreCtx{R.alpha, R.beta, R.C, R.ldc, R.mu_a, R.mu_b, R.b, R.write_c != 0, R.err_sq != nullptr};
+  return CrtStoreCtx{R.alpha, R.beta, R.C,       R.ldc,          R.save,
+                     R.ld_save, R.mu_a, R.mu_b, R.b, R.write_c != 0, R.err_sq != nullptr};
 }
 
 // C_ij from RN(C'_ij) = d 2^shift (signed d): scale by 2^-(mu_i + nu_j), apply alpha and
@@ -662,10 +667,13 @@ __device__ __forceinline__ void crt_store(const CrtStoreCtx& S, int64_t i, int64
   const double v = __dmul_rn(S.alpha, val);
   if (S.write_c) {
     double* c = S.C + j * S.ldc + i;
-    if (S.beta == 0.0)
+    if (S.beta == 0.0) {
       *c = v;
-    else
-      *c = __fma_rn(S.beta, *c, v);
+    } else {
+      const double old = *c;
+      if (S.save) S.save[j * S.ld_save + i] = old;
+      *c = __fma_rn(S.beta, old, v);
+    }
   }
   if (S.estimate) {
     // truncation errors need a nonzero row on both sides
@@ -1006,6 +1014,8 @@ cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t 
   R.err_sq = args.err_sq;
   R.skip_if_flag = args.skip_if_flag;
   R.write_c = args.write_c ? 1 : 0;
+  R.save = args.save;
+  R.ld_save = args.ld_save;
   R.uplo = args.uplo;
   const unsigned gx = unsigned((args.m + 255) / 256);
   // up to kRecCols columns per block, fewer while the grid is under ~4 blocks per SM

@@ -100,7 +100,8 @@ namespace {
 
 // CRT-form emulation (Ozaki scheme II): scan, norm bounds, residue split, one INT8 GEMM
 // per modulus, exact reconstruction.  The a-posteriori check adds two moduli at a time;
-// with beta != 0 the estimate is taken before C is written, so C is read only once.
+// with beta != 0 the reconstruction keeps the old C as it writes the new one, and a product
+// redone with more moduli starts again from it.
 int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
               int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc, cudaStream_t st,
               const DgemmOptions& opt, eb2_call_info& info) {
@@ -152,6 +153,12 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   off = align256(off + (tri ? size_t(max_tiles) * 4 : 0));
   const size_t o_full = off;
   off = align256(off + (tri ? size_t(m) * n * 8 : 0));
+  // beta != 0 with the check: the old C, kept as the reconstruction overwrites it, in case the
+  // product must be redone with more moduli (a triangle keeps it in the fallback buffer, which
+  // only a non-finite input uses, and then no reconstruction runs)
+  const bool keep_old = check && beta != 0.0;
+  const size_t o_save = off;
+  off = align256(off + (keep_old && !tri ? size_t(m) * n * 8 : 0));
   if (!cx.ws.ensure(off)) {
     set_error(EB2_ERR_ALLOC, "could not allocate %zu bytes of emulation workspace", off);
     return EB2_ERR_ALLOC;
@@ -222,8 +229,10 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   r.err_sq = df->err_sq;
   r.skip_if_flag = &df->nonfinite;
   r.uplo = tri ? opt.uplo : 0;
-  // with beta != 0 and the check on, C is written only once the estimate has passed
-  const bool deferred = check && beta != 0.0;
+  r.write_c = true;
+  double* const saved = keep_old ? reinterpret_cast<double*>(ws + (tri ? o_full : o_save)) : nullptr;
+  r.save = saved;
+  r.ld_save = m;
   auto product = [&](bool first) -> bool {
     bool good = check_cuda(launch_crt_split(va, oa, nmod, st), "residues A");
     if (!same) good = good && check_cuda(launch_crt_split(vb, ob, nmod, st), "residues B");
@@ -231,7 +240,6 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
     if (first && opt.timed) cudaEventRecord(cx.ev_gemm0, st);
     good = good && check_cuda(launch_crt_gemm(oa, ob, g, st), "CRT GEMM");
     if (first && opt.timed) cudaEventRecord(cx.ev_gemm1, st);
-    r.write_c = !deferred;
     good = good && check_cuda(launch_crt_reconstruct(r, st), "CRT reconstruction");
     info.launches += 6;
     return good;
@@ -292,19 +300,22 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
     if (!check || !known || est <= tol || nmod + 2 > nmax) {
       if (check && est > tol)
         set_error(EB2_ERR_ACCURACY, "emulated DGEMM estimate %.3g above target %.3g with %d moduli", est, tol, nmod);
-      if (deferred) {
-        r.write_c = true;
-        r.err_sq = nullptr;
-        if (!check_cuda(launch_crt_reconstruct(r, st), "CRT reconstruction")) return EB2_ERR_CUDA;
-        info.launches += 1;
-        if (opt.sync && !check_cuda(cudaStreamSynchronize(st), "DGEMM")) return EB2_ERR_CUDA;
-      }
       break;
     }
-    // two more moduli: b grows by 4 bits, so every residue is recomputed
+    // two more moduli: b grows by 4 bits, so every residue is recomputed, from the old C
     nmod += 2;
     ++info.escalations;
     info.slices = nmod;
+    if (keep_old) {
+      const bool restored =
+          tri ? check_cuda(launch_merge_triangle<double>(saved, m, n, opt.uplo == 1, 0.0, C, ldc, st, nullptr),
+                           "restore C")
+              : check_cuda(cudaMemcpy2DAsync(C, size_t(ldc) * 8, saved, size_t(m) * 8, size_t(m) * 8, size_t(n),
+                                             cudaMemcpyDeviceToDevice, st),
+                           "restore C");
+      if (!restored) return EB2_ERR_CUDA;
+      info.launches += 1;
+    }
     if (!check_cuda(cudaMemsetAsync(df->err_sq, 0, sizeof(df->err_sq), st), "reset estimate") || !product(false))
       return EB2_ERR_CUDA;
   }

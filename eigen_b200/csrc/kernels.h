@@ -155,6 +155,10 @@ struct CrtReconstructArgs {
   double* err_sq;  // [2]: += estimated squared error, += squared alpha*A*B entries (may be null)
   const int* skip_if_flag;
   bool write_c;    // false: only the estimate
+  // beta != 0: where the old C goes as the new one is written (ld_save), so that a product
+  // that must be redone with more moduli can start again from it (null: not kept)
+  double* save = nullptr;
+  int64_t ld_save = 0;
   int uplo = 0;    // 0: all of C; 1: only i <= j (upper triangle); 2: only i >= j (lower)
 };
 cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t stream);
