@@ -550,6 +550,10 @@ def our_arm(a, world, rank, local):
     gemm_ms_avg = rank_max(sum(gemm_ms) / len(gemm_ms)) if gemm_ms else None
     slices = infos[-1]["slices"]
     launches = sum(i["launches"] for i in infos)
+    # device time of one call's kernels (events around them inside the library), against which
+    # ms_per_step also holds the host side of each synchronous, checked call
+    call_ms = sorted(i["kernel_ms"] for i in infos if i["kernel_ms"] > 0)
+    kernel_ms_per_call = round(call_ms[len(call_ms) // 2], 3) if call_ms else None
 
     native = None
     if not a.no_native:
@@ -638,7 +642,8 @@ def our_arm(a, world, rank, local):
             "warmup": a.warmup, "ms_per_step": round(ms_emu_max, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int8 residues (s32 accumulate) -> f64", "data": "synthetic",
             "config": dict(workload_config(a), method=method, moduli_or_slices=slices, tile_n=infos[-1]["tile_n"],
-                           err_estimate=infos[-1]["err_estimate"], escalations=infos[-1]["escalations"]),
+                           err_estimate=infos[-1]["err_estimate"], escalations=infos[-1]["escalations"],
+                           kernel_ms_per_call=kernel_ms_per_call),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "native_fp64": native, "accuracy": accuracy, "grouped_batch": grouped,
             "level3_routines": level3,
