@@ -135,6 +135,7 @@ void blas_gemm(char transa, char transb, int64_t m, int64_t n, int64_t k, T alph
   eb2_call_info& ci = call_info();
   ci = eb2_call_info{};
   cudaStream_t st = cx->stream;
+  StreamFence fence(*cx, st);
 
   const bool a_dev = !need_ab || device_usable(a);
   const bool b_dev = !need_ab || device_usable(b);
@@ -319,6 +320,7 @@ int eb2_dgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, 
   eb2::Context* cx = eb2::current_context();
   if (!cx) return EB2_ERR_NO_DEVICE;
   std::lock_guard<std::mutex> lock(cx->mu);
+  eb2::StreamFence fence(*cx, static_cast<cudaStream_t>(stream));
   eb2::DgemmOptions o;
   o.sync = check_accuracy != 0;
   o.check_accuracy = check_accuracy != 0;
@@ -339,6 +341,7 @@ int eb2_sgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, 
   eb2::Context* cx = eb2::current_context();
   if (!cx) return EB2_ERR_NO_DEVICE;
   std::lock_guard<std::mutex> lock(cx->mu);
+  eb2::StreamFence fence(*cx, static_cast<cudaStream_t>(stream));
   eb2::SgemmOptions o;
   o.sync = false;
   o.timed = eb2::settings().timing.load() != 0;

@@ -82,6 +82,24 @@ bool DeviceBuffer::ensure(size_t bytes) {
   return true;
 }
 
+StreamFence::StreamFence(Context& cx, cudaStream_t st) : cx_(cx), st_(st), active_(false) {
+  cudaStreamCaptureStatus status = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &status) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return;
+  }
+  active_ = status == cudaStreamCaptureStatusNone;
+  if (active_ && cx_.fence_armed) (void)cudaStreamWaitEvent(st_, cx_.ev_fence, 0);
+}
+
+StreamFence::~StreamFence() {
+  if (!active_) return;
+  if (cudaEventRecord(cx_.ev_fence, st_) == cudaSuccess)
+    cx_.fence_armed = true;
+  else
+    (void)cudaGetLastError();
+}
+
 Context* current_context() {
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
@@ -123,6 +141,7 @@ Context* current_context() {
   ok = ok && cudaStreamCreateWithFlags(&c->copy_in, cudaStreamNonBlocking) == cudaSuccess;
   ok = ok && cudaStreamCreateWithFlags(&c->copy_out, cudaStreamNonBlocking) == cudaSuccess;
   ok = ok && cudaEventCreateWithFlags(&c->ev_a, cudaEventDisableTiming) == cudaSuccess;
+  ok = ok && cudaEventCreateWithFlags(&c->ev_fence, cudaEventDisableTiming) == cudaSuccess;
   for (int i = 0; i < Context::kPipeChunks && ok; ++i) {
     ok = cudaEventCreateWithFlags(&c->ev_in[i], cudaEventDisableTiming) == cudaSuccess;
     ok = ok && cudaEventCreateWithFlags(&c->ev_done[i], cudaEventDisableTiming) == cudaSuccess;

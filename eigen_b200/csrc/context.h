@@ -51,6 +51,29 @@ struct Context {
   cudaEvent_t ev_in[kPipeChunks] = {};
   cudaEvent_t ev_done[kPipeChunks] = {};
   double* hchunk = nullptr;  // pinned [kPipeChunks][2]: per-block error-estimate energies
+  // End of the last call's work on its stream (fence_armed: recorded since the last call);
+  // see StreamFence.
+  cudaEvent_t ev_fence = nullptr;
+  bool fence_armed = false;
+};
+
+// The workspaces and the flag block of a context pass from one call to the next in stream
+// order.  A stream-ordered call (eb2_dgemm_device without the check, eb2_sgemm_device) may
+// return with its kernels still running, and the next call may come on another stream or from
+// another host thread: so every call's stream first waits for the previous call's end event,
+// and records its own when it is done.  Construct it with the context's mutex held.  Nothing
+// is waited for or recorded on a stream that is being captured into a graph.
+class StreamFence {
+ public:
+  StreamFence(Context& cx, cudaStream_t st);
+  ~StreamFence();
+  StreamFence(const StreamFence&) = delete;
+  StreamFence& operator=(const StreamFence&) = delete;
+
+ private:
+  Context& cx_;
+  cudaStream_t st_;
+  bool active_;
 };
 
 // Context of the calling thread's current device, created on first use.

@@ -33,6 +33,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <functional>
+#include <optional>
 
 #include "blas_common.h"
 #include "context.h"
@@ -541,11 +542,13 @@ bool stage(DeviceBuffer& buf, const T* p, int64_t ld, int64_t rows, int64_t cols
 struct Call {
   Context* cx = nullptr;
   std::unique_lock<std::mutex> lock;
+  std::optional<StreamFence> fence;  // constructed under the lock, destroyed before it
   cudaStream_t st = nullptr;
   Summary sum;
   char dtype = 'd';
 
   explicit Call(char dt) : dtype(dt) {}
+  ~Call() { fence.reset(); }
 
   bool begin() {
     cx = current_context();
@@ -555,6 +558,7 @@ struct Call {
     }
     lock = std::unique_lock<std::mutex>(cx->mu);
     st = cx->stream;
+    fence.emplace(*cx, st);
     call_info() = eb2_call_info{};
     set_pending_timing(nullptr, false);
     return true;
