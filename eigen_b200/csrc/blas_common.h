@@ -24,9 +24,21 @@ inline int op_code(char c) {
   if (c == 'C' || c == 'c') return kAdj;
   return kInvalid;
 }
-inline int side_code(char c) { return (c == 'L' || c == 'l') ? kLeft : (c == 'R' || c == 'r') ? kRight : kInvalid; }
-inline int uplo_code(char c) { return (c == 'U' || c == 'u') ? kUp : (c == 'L' || c == 'l') ? kLo : kInvalid; }
-inline int diag_code(char c) { return (c == 'N' || c == 'n') ? kNonUnit : (c == 'U' || c == 'u') ? kUnit : kInvalid; }
+inline int side_code(char c) {
+  if (c == 'L' || c == 'l') return kLeft;
+  if (c == 'R' || c == 'r') return kRight;
+  return kInvalid;
+}
+inline int uplo_code(char c) {
+  if (c == 'U' || c == 'u') return kUp;
+  if (c == 'L' || c == 'l') return kLo;
+  return kInvalid;
+}
+inline int diag_code(char c) {
+  if (c == 'N' || c == 'n') return kNonUnit;
+  if (c == 'U' || c == 'u') return kUnit;
+  return kInvalid;
+}
 
 // Per-routine call counters behind eb2_routine_calls: a routine counts once per call that
 // gets past its argument checks and quick returns (name lower-case without the trailing
