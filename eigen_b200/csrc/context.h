@@ -48,6 +48,7 @@ struct Context {
   static constexpr int kPipeChunks = 16;
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   cudaEvent_t ev_a = nullptr;
+  cudaEvent_t ev_scan = nullptr;  // the scans' statistics have reached the host (picker stage 2)
   cudaEvent_t ev_in[kPipeChunks] = {};
   cudaEvent_t ev_done[kPipeChunks] = {};
   double* hchunk = nullptr;  // pinned [kPipeChunks][2]: per-block error-estimate energies

@@ -179,9 +179,22 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   if (!same) ok = ok && check_cuda(launch_crt_scan_norms(vb, ob, &df->nonfinite, &df->spread[0], st), "scan B");
   if (!ok) return EB2_ERR_CUDA;
   info.launches = same ? 1 : 2;
+  // Stage 2 reads the scans' statistics on the host.  The residue split for the current
+  // modulus count is launched first, so the GPU works while the host waits and decides; it is
+  // redone only if the picker changes the count (both tile configurations use the same
+  // residue layout).
+  int split_moduli = 0;  // modulus count of the residues already launched (0: none)
+  auto split = [&]() -> bool {
+    bool good = check_cuda(launch_crt_split(va, oa, nmod, st), "residues A");
+    if (!same) good = good && check_cuda(launch_crt_split(vb, ob, nmod, st), "residues B");
+    info.launches += same ? 2 : 4;
+    split_moduli = nmod;
+    return good;
+  };
   if (stage2) {
     if (!check_cuda(cudaMemcpyAsync(cx.hflags, df, sizeof(DeviceFlags), cudaMemcpyDeviceToHost, st), "read scan") ||
-        !check_cuda(cudaStreamSynchronize(st), "scan"))
+        !check_cuda(cudaEventRecord(cx.ev_scan, st), "scan event") || !split() ||
+        !check_cuda(cudaEventSynchronize(cx.ev_scan), "scan"))
       return EB2_ERR_CUDA;
     const double spread = cx.hflags->spread[1] > 0 ? cx.hflags->spread[0] / cx.hflags->spread[1] : 0.0;
     int cfg = -1, cls = 0;
@@ -234,14 +247,14 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   r.save = saved;
   r.ld_save = m;
   auto product = [&](bool first) -> bool {
-    bool good = check_cuda(launch_crt_split(va, oa, nmod, st), "residues A");
-    if (!same) good = good && check_cuda(launch_crt_split(vb, ob, nmod, st), "residues B");
+    bool good = split_moduli == nmod || split();
+    split_moduli = 0;  // a product redone with more moduli splits again
     g.moduli = r.moduli = nmod;
     if (first && opt.timed) cudaEventRecord(cx.ev_gemm0, st);
     good = good && check_cuda(launch_crt_gemm(oa, ob, g, st), "CRT GEMM");
     if (first && opt.timed) cudaEventRecord(cx.ev_gemm1, st);
     good = good && check_cuda(launch_crt_reconstruct(r, st), "CRT reconstruction");
-    info.launches += 6;
+    info.launches += 2;
     return good;
   };
   ok = product(true);
