@@ -228,10 +228,13 @@ __global__ void __launch_bounds__(256) crt_scan_norm_kernel(const double* __rest
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const double x = tile[rr][sub + 8 * j];
-      if (x != 0.0) {
-        const double xs = scale2(x, -e);
-        s += static_cast<unsigned long long>(ceil(__dmul_rn(__dmul_rn(xs, xs), 4294967296.0))) + 1ull;
-      }
+      const double xs = scale2(x, -e);
+      // ceil(v) for v = rn(x'^2) 2^32 in [0, 2^32]: v + 2^52 rounded up is 2^52 + ceil(v)
+      // exactly, read from its bits (no rounding or conversion instruction)
+      const double v = __dmul_rn(__dmul_rn(xs, xs), 4294967296.0);
+      const unsigned long long c = static_cast<unsigned long long>(__double_as_longlong(__dadd_ru(v, 0x1p52)) -
+                                                                   __double_as_longlong(0x1p52));
+      s += x != 0.0 ? c + 1ull : 0ull;
     }
   }
 #pragma unroll
