@@ -374,7 +374,8 @@ def _exact_block(Ar, Bc):
 
 def accuracy_leg(eb, torch, dev, S, r_values, seed=99, sample=24):
     """Normwise error of the automatic (emulated) and the native DGEMM against an exactly
-    rounded reference on a sampled sub-block, for entries u*2^e with e in [-r, r]."""
+    rounded reference on a sampled sub-block, for entries u*2^e with e in [-r, r]:
+    ||dC||_F / ||C||_F, ||dC||_F / || |A||B| ||_F and max |dC| on the block."""
     import numpy as np
 
     out = {}
@@ -393,6 +394,7 @@ def accuracy_leg(eb, torch, dev, S, r_values, seed=99, sample=24):
         Ar = A[:, rows].T.cpu().numpy().astype(np.float64)
         Bc = B[cols, :].T.cpu().numpy().astype(np.float64)
         ref = _exact_block(Ar, Bc)
+        absprod = np.abs(Ar) @ np.abs(Bc)  # |A||B| on the block (rounding here is immaterial)
         res = {}
         for name, method in (("emulated", eb.METHOD_AUTO), ("native", eb.METHOD_NATIVE)):
             eb.set_dgemm_method(method)
@@ -402,7 +404,10 @@ def accuracy_leg(eb, torch, dev, S, r_values, seed=99, sample=24):
             info = eb.last_call_info()
             got = C[cols][:, rows].T.cpu().numpy()
             err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
-            res[name] = {"rel_error": err, "rc": rc, "method": info["method"], "moduli_or_slices": info["slices"],
+            res[name] = {"rel_error": err,
+                         "rel_to_abs_product": float(np.linalg.norm(got - ref) / np.linalg.norm(absprod)),
+                         "max_abs_error": float(np.max(np.abs(got - ref))),
+                         "rc": rc, "method": info["method"], "moduli_or_slices": info["slices"],
                          "escalations": info["escalations"], "err_estimate": info["err_estimate"]}
         eb.set_dgemm_method(eb.METHOD_AUTO)
         res["sample"] = f"{sample}x{sample} block of C, exactly rounded reference"
