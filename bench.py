@@ -58,6 +58,7 @@ def parse_args():
     ap.add_argument("--no-native", action="store_true")
     ap.add_argument("--no-grouped", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-sgemm", action="store_true", help="skip the split-BF16 / native FP32 SGEMM leg")
     ap.add_argument("--no-level3", action="store_true", help="skip the level-3 routine and complex GEMM leg")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
@@ -372,6 +373,48 @@ def _exact_block(Ar, Bc):
     return out
 
 
+def sgemm_leg(eb, torch, dev, S, steps, rank_max, seed=123, sample=24):
+    """Split-BF16 SGEMM (the default FP32 method) and the native FP32 kernel at S^3 on device
+    operands: CUDA-event time over `steps` calls (max over ranks), and the normwise error of a
+    sampled block against the FP64 product of the same FP32 inputs."""
+    import numpy as np
+
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    A = torch.rand((S, S), dtype=torch.float32, device=dev, generator=g) * 2 - 1
+    B = torch.rand((S, S), dtype=torch.float32, device=dev, generator=g) * 2 - 1
+    rng = np.random.default_rng(seed)
+    rows = np.sort(rng.choice(S, sample, replace=False))
+    cols = np.sort(rng.choice(S, sample, replace=False))
+    # column-major: A(i, l) is A_t[l, i]; the FP64 product of FP32 inputs is exact to ~1e-16
+    ref = A[:, rows].T.cpu().double().numpy() @ B[cols, :].T.cpu().double().numpy()
+    out = {}
+    stream = torch.cuda.Stream(device=dev)
+    for name, method, n in (("split_bf16", eb.METHOD_EMULATED, steps), ("native_fp32", eb.METHOD_NATIVE, min(steps, 3))):
+        eb.set_sgemm_method(method)
+        C = torch.zeros((S, S), dtype=torch.float32, device=dev)
+        for _ in range(2):
+            assert eb.sgemm_device("N", "N", S, S, S, 1.0, A, S, B, S, 0.0, C, S, stream=stream.cuda_stream) == eb.EB2_OK
+        stream.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(n):
+            rc = eb.sgemm_device("N", "N", S, S, S, 1.0, A, S, B, S, 0.0, C, S, stream=stream.cuda_stream)
+            assert rc == eb.EB2_OK, eb.last_error()
+        ev1.record(stream)
+        stream.synchronize()
+        info = eb.last_call_info()
+        ms = rank_max(ev0.elapsed_time(ev1) / n)
+        got = C[cols][:, rows].T.cpu().double().numpy()
+        out[name] = {"tflops": round(2.0 * S**3 / ms / 1e9, 3), "ms_per_step": round(ms, 3), "steps": n,
+                     "rel_error": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+                     "method": info["method"], "bf16_products": info["slices"]}
+    eb.set_sgemm_method(eb.METHOD_AUTO)
+    out["sample"] = f"{sample}x{sample} block of C against the FP64 product of the FP32 inputs"
+    del A, B, C
+    return out
+
+
 def accuracy_leg(eb, torch, dev, S, r_values, seed=99, sample=24):
     """Normwise error of the automatic (emulated) and the native DGEMM against an exactly
     rounded reference on a sampled sub-block, for entries u*2^e with e in [-r, r]:
@@ -597,6 +640,10 @@ def our_arm(a, world, rank, local):
     if not a.no_accuracy:
         accuracy = accuracy_leg(eb, torch, dev, S, (0, 8, 32))
 
+    sgemm = None
+    if not a.no_sgemm:
+        sgemm = sgemm_leg(eb, torch, dev, S, min(a.steps, 5), rank_max)
+
     grouped = None
     if not a.no_grouped:
         grouped = grouped_bench(eb, torch, dev, stream, a.steps, a.warmup)
@@ -650,7 +697,7 @@ def our_arm(a, world, rank, local):
                            err_estimate=infos[-1]["err_estimate"], escalations=infos[-1]["escalations"],
                            kernel_ms_per_call=kernel_ms_per_call),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk, "native_fp64": native, "accuracy": accuracy, "grouped_batch": grouped,
+            "clocks": clk, "native_fp64": native, "accuracy": accuracy, "sgemm": sgemm, "grouped_batch": grouped,
             "level3_routines": level3,
             "emulated_over_native": round(value / native["tflops"], 3) if native else None,
         }
