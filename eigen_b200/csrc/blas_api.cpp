@@ -319,6 +319,17 @@ int eb2_dgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, 
   }
   eb2::Context* cx = eb2::current_context();
   if (!cx) return EB2_ERR_NO_DEVICE;
+  if (check_accuracy) {
+    // the a-posteriori check reads the estimate on the host between kernels
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &capture) == cudaSuccess &&
+        capture != cudaStreamCaptureStatusNone) {
+      eb2::set_error(EB2_ERR_ARG, "a DGEMM with the accuracy check cannot be captured into a graph; "
+                                  "capture it with check_accuracy = 0");
+      return EB2_ERR_ARG;
+    }
+    (void)cudaGetLastError();
+  }
   std::lock_guard<std::mutex> lock(cx->mu);
   eb2::StreamFence fence(*cx, static_cast<cudaStream_t>(stream));
   eb2::DgemmOptions o;

@@ -111,8 +111,15 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   int nmod = forced ? forced : kCrtDefaultModuli;
   const bool auto_tile = opt.tile_n != kTilePair && opt.tile_n != 256 && settings().tile_n.load() == 0;
   // Stage 2 of the learned picker: tile configuration and modulus count, once the scan
-  // has measured the inputs' exponent spread.
-  const bool stage2 = picker_weights() != nullptr && (auto_tile || forced == 0);
+  // has measured the inputs' exponent spread.  It needs the host to read the scan's result,
+  // so a call captured into a graph keeps the stage-1 choice.
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &capture) != cudaSuccess) {
+    (void)cudaGetLastError();
+    capture = cudaStreamCaptureStatusNone;
+  }
+  const bool stage2 =
+      picker_weights() != nullptr && (auto_tile || forced == 0) && capture == cudaStreamCaptureStatusNone;
   const int nmax = (check || stage2) ? std::max(nmod, kCrtMaxModuli) : nmod;
   int tile = (opt.tile_n == kTilePair || opt.tile_n == 256) ? opt.tile_n : choose_crt_tile(cx, m, n);
   const StridedView<double> va = view_a(ta, A, lda, m, k);

@@ -285,7 +285,9 @@ int eb2_set_timing(int on);
 
 /* Stream-ordered product on device pointers; no host synchronisation unless the
  * a-posteriori check of the emulated DGEMM needs one (check_accuracy != 0).
- * `stream` is a cudaStream_t (NULL = the legacy default stream).  Returns EB2_*. */
+ * `stream` is a cudaStream_t (NULL = the legacy default stream).  Returns EB2_*.
+ * Both can be captured into a CUDA graph once a first call of the same size has sized the
+ * workspace; a DGEMM with check_accuracy != 0 refuses capture (EB2_ERR_ARG). */
 int eb2_dgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, double alpha, const double* a,
                      int64_t lda, const double* b, int64_t ldb, double beta, double* c, int64_t ldc, void* stream,
                      int check_accuracy);
