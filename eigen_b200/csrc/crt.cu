@@ -918,6 +918,7 @@ cudaError_t launch_gemm_config(const CrtOperand& a, const CrtOperand& b, const C
   P.ld_res = args.ld_res;
   P.tile_list = args.tile_list;
   P.num_listed = args.num_listed;
+  P.tri_k = args.tri_k;
   if (P.tile_list) {
     if (P.num_listed < 1 || P.num_listed > P.tiles_m * P.tiles_n) return cudaErrorInvalidValue;
     return launch_slice_gemm<kModeCrtI8Listed, BN, STAGES, 4, PAIR>(tmA, tmB, P, args.num_sms, stream);

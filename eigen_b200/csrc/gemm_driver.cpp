@@ -222,6 +222,7 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   g.num_sms = cx.num_sms;
   g.cres = ws + o_res_c;
   g.ld_res = m_pad;
+  g.tri_k = opt.tri_operand;
   if (tri) {
     // the tiles meeting the triangle, in the kernel's raster order
     std::vector<int> tiles(static_cast<size_t>(max_tiles));

@@ -19,6 +19,8 @@ struct DgemmOptions {
   bool timed = false;    // record kernel time in call_info
   int uplo = 0;          // CRT only, m == n: 1 = compute and write only C's upper triangle
                          // (i <= j), 2 = only the lower (i >= j); the other is not touched
+  int tri_operand = 0;   // CRT only: op(A) (1 lower, 2 upper) or op(B) (3 lower, 4 upper) is
+                         // triangular with zeros outside; its zero K blocks are skipped (same C)
 };
 
 struct SgemmOptions {

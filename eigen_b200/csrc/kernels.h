@@ -139,6 +139,8 @@ struct CrtGemmArgs {
   int64_t ld_res;  // = a.rows_pad
   const int* tile_list = nullptr;  // device: the output tiles to compute (null: all)
   int num_listed = 0;
+  int tri_k = 0;  // triangular operand whose zero K blocks are skipped: 1/2 = op(A) lower/upper,
+                  // 3/4 = op(B) lower/upper (0: dense)
 };
 cudaError_t launch_crt_gemm(const CrtOperand& a, const CrtOperand& b, const CrtGemmArgs& args, cudaStream_t stream);
 

@@ -132,7 +132,7 @@ bool cuda_ok(cudaError_t e, const char* what) {
 // uplo != 0: the CRT product of only C's upper (1) or lower (2) triangle (m == n).
 int gemm(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
          int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc, cudaStream_t st,
-         Summary& sum, int uplo = 0) {
+         Summary& sum, int uplo = 0, int tri = 0) {
   if (m == 0 || n == 0) return EB2_OK;
   DgemmOptions o;
   o.sync = false;
@@ -142,6 +142,7 @@ int gemm(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double 
     o.method = EB2_METHOD_CRT;
     o.uplo = uplo;
   }
+  o.tri_operand = tri;
   eb2_call_info ci{};
   const int rc = dgemm_on_device(cx, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, st, o, ci);
   const int64_t flops = m * n * k;
@@ -297,8 +298,17 @@ int trxm_device(Context& cx, bool solve, bool left, bool upper, bool trans, bool
     T* P = Tf + size_t(size) * size;
     if (!cuda_ok(launch_expand_triangular<T>(A, lda, size, upper, unit, Tf, size, st), "expand")) return EB2_ERR_CUDA;
     sum.launches += 1;
-    const int rc = left ? gemm(cx, trans, false, m, n, m, alpha, Tf, size, B, ldb, T(0), P, m, st, sum)
-                        : gemm(cx, false, trans, m, n, n, alpha, B, ldb, Tf, size, T(0), P, m, st, sum);
+    int rc;
+    if constexpr (sizeof(T) == 8) {
+      // op(triangle) is lower when the stored triangle is lower and not transposed, or upper
+      // and transposed; the CRT product then skips the K blocks that are zero in it
+      const bool op_lower = upper == trans;
+      rc = left ? gemm(cx, trans, false, m, n, m, alpha, Tf, size, B, ldb, T(0), P, m, st, sum, 0, op_lower ? 1 : 2)
+                : gemm(cx, false, trans, m, n, n, alpha, B, ldb, Tf, size, T(0), P, m, st, sum, 0, op_lower ? 3 : 4);
+    } else {
+      rc = left ? gemm(cx, trans, false, m, n, m, alpha, Tf, size, B, ldb, T(0), P, m, st, sum)
+                : gemm(cx, false, trans, m, n, n, alpha, B, ldb, Tf, size, T(0), P, m, st, sum);
+    }
     if (rc != EB2_OK && rc != EB2_ERR_ACCURACY) return rc;
     if (!cuda_ok(cudaMemcpy2DAsync(B, size_t(ldb) * sizeof(T), P, size_t(m) * sizeof(T), size_t(m) * sizeof(T),
                                    size_t(n), cudaMemcpyDeviceToDevice, st),

@@ -84,6 +84,8 @@ struct SliceGemmParams {
   int64_t ld_res;        // CRT: rows of one residue plane (padded m)
   const int* tile_list;  // CRT: the tiles to compute (indices of the full raster), or null for all
   int num_listed;        // CRT: entries of tile_list
+  int tri_k;             // CRT: 1 = op(A) lower, 2 = op(A) upper, 3 = op(B) lower, 4 = op(B) upper
+                         // triangular (zero blocks of K skipped per tile); 0 = dense
 };
 
 // Pair range of diagonal t: p = p_lo .. p_lo + total/num_kb - 1 (q = t - p).
@@ -110,6 +112,28 @@ __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, 
   const int r = tile % group_size;
   tm = first_m + r % gm;
   tn = r / gm;
+}
+
+// CRT with a triangular operand (P.tri_k): the 128-byte K blocks [kb_lo, kb_hi) that can be
+// nonzero for the output tile of `rows` x `cols` at raster index `tile`.  A triangle's zero
+// blocks have zero residues and add exact zeros, so leaving them out changes no bit.  A tile
+// wholly in the padding keeps one block (its operand rows are zero), so every role walks at
+// least one block per item.
+__device__ __forceinline__ void tile_k_range(const SliceGemmParams& P, int tile, int rows, int cols, int& kb_lo,
+                                             int& kb_hi) {
+  kb_lo = 0;
+  kb_hi = P.num_kb;
+  if (P.tri_k == 0) return;
+  int tm, tn;
+  tile_coords(tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
+  const int r0 = tm * rows, c0 = tn * cols;
+  if (P.tri_k == 1) kb_hi = (r0 + rows + kSliceKBytes - 1) / kSliceKBytes;  // op(A)(r, k) = 0 for k > r
+  if (P.tri_k == 2) kb_lo = r0 / kSliceKBytes;                              // ... for k < r
+  if (P.tri_k == 3) kb_lo = c0 / kSliceKBytes;                              // op(B)(k, c) = 0 for k < c
+  if (P.tri_k == 4) kb_hi = (c0 + cols + kSliceKBytes - 1) / kSliceKBytes;  // ... for k > c
+  kb_hi = min(kb_hi, P.num_kb);
+  kb_lo = min(kb_lo, P.num_kb - 1);
+  if (kb_hi <= kb_lo) kb_hi = kb_lo + 1;
 }
 
 // Work items: one per output tile, or in CRT mode one per (tile, modulus): the moduli are
@@ -141,12 +165,14 @@ __device__ __forceinline__ void work_item(const SliceGemmParams& P, int w, int& 
 template <bool LISTED>
 struct BlockIter {
   int work, tile, t, t_lo, f, p_lo, total, stride;
+  int rows, cols, kb_lo, kb_hi;  // tile shape; CRT: the item's K blocks
   bool valid;
   __device__ __forceinline__ void load(const SliceGemmParams& P) {
     int t_hi;
     work_item<LISTED>(P, work, tile, t_hi, t_lo);
     t = t_hi;
     f = 0;
+    tile_k_range(P, tile, rows, cols, kb_lo, kb_hi);
   }
   __device__ __forceinline__ void settle(const SliceGemmParams& P, int nwork) {
     valid = false;
@@ -156,7 +182,9 @@ struct BlockIter {
         if (work < nwork) load(P);
         continue;
       }
-      if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, P.crt != 0) || f >= total) {
+      const bool some = diag_bounds(t, P.slices, P.num_kb, p_lo, total, P.crt != 0);
+      if (P.crt) total = kb_hi - kb_lo;
+      if (!some || f >= total) {
         --t;
         f = 0;
         continue;
@@ -165,9 +193,12 @@ struct BlockIter {
       return;
     }
   }
-  __device__ __forceinline__ void start(const SliceGemmParams& P, int nwork, int first, int step) {
+  __device__ __forceinline__ void start(const SliceGemmParams& P, int nwork, int first, int step, int tile_rows,
+                                        int tile_cols) {
     work = first;
     stride = step;
+    rows = tile_rows;
+    cols = tile_cols;
     if (work < nwork) load(P);
     settle(P, nwork);
   }
@@ -222,13 +253,13 @@ __device__ __forceinline__ void slice_producer(const CUtensorMap* tmA, const CUt
   const int a_row_off = PAIR ? int(rank) * kSliceBM : 0;
   const int b_row_off = PAIR ? int(rank) * L::kBRows : 0;
   BlockIter<kListed> it;
-  it.start(P, nwork, first_tile<PAIR>(), tile_step<PAIR>());
+  it.start(P, nwork, first_tile<PAIR>(), tile_step<PAIR>(), PAIR ? 2 * kSliceBM : kSliceBM, BN);
   uint32_t issued = 0;  // stage = issued % STAGES, phase = (issued / STAGES) & 1
   bool ok = true;
   while (it.valid) {
     int tm, tn;
     tile_coords(it.tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
-    const int p = it.p_lo + it.f / P.num_kb, kb = it.f % P.num_kb;
+    const int p = it.p_lo + it.f / P.num_kb, kb = P.crt ? it.kb_lo + it.f : it.f % P.num_kb;
     const int stage = int(issued % STAGES);
     if (!mbar_wait(&empty[stage], ((issued / STAGES) & 1u) ^ 1u, abort_flag, P.status)) {
       ok = false;
@@ -298,6 +329,11 @@ __device__ __forceinline__ void slice_mma(uint8_t* smem, uint64_t* full, uint64_
     for (int t = t_hi; t >= t_lo && ok; --t) {
       int p_lo, total;
       if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, is_crt_mode(MODE))) continue;
+      if constexpr (is_crt_mode(MODE)) {
+        int kb_lo, kb_hi;
+        tile_k_range(P, tile, PAIR ? 2 * kSliceBM : kSliceBM, BN, kb_lo, kb_hi);
+        total = kb_hi - kb_lo;
+      }
       constexpr int kUnit = SliceTraits<MODE, BN, PAIR>::kUnitKb;
       for (int u0 = 0; u0 < total && ok;) {
         const int u1 = (kTileUnit || total - u0 <= kUnit) ? total : u0 + kUnit;
@@ -507,6 +543,11 @@ __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull
     for (int t = t_hi; t >= t_lo && ok; --t) {
       int p_lo, total;
       if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, true)) continue;
+      {
+        int kb_lo, kb_hi;
+        tile_k_range(P, tile, PAIR ? 2 * kSliceBM : kSliceBM, BN, kb_lo, kb_hi);
+        total = kb_hi - kb_lo;
+      }
       const uint32_t pm = uint32_t(crt_modulus(t));
       const uint32_t magic = 0xFFFFFFFFu / pm;
       // |v| <= 1023 * 128 * 128 * 128 = 2^31 - 2^21 for an accumulation unit, so with bias a
