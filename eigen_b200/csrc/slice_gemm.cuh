@@ -162,17 +162,20 @@ __device__ __forceinline__ void work_item(const SliceGemmParams& P, int w, int& 
 }
 
 // Walks the (work item, diagonal, pair, k-block) schedule in issue order.
-template <bool LISTED>
+// CRT: each item walks the K blocks [kb_lo, kb_hi) of its tile (a compile-time branch: the
+// producer's per-block path stays as short as the dense one).
+template <bool LISTED, bool CRT>
 struct BlockIter {
   int work, tile, t, t_lo, f, p_lo, total, stride;
   int rows, cols, kb_lo, kb_hi;  // tile shape; CRT: the item's K blocks
+  int kbi, pi;                   // f as (K block, pair offset): f = pi * num_kb + kbi, kept by adds
   bool valid;
   __device__ __forceinline__ void load(const SliceGemmParams& P) {
     int t_hi;
     work_item<LISTED>(P, work, tile, t_hi, t_lo);
     t = t_hi;
-    f = 0;
-    tile_k_range(P, tile, rows, cols, kb_lo, kb_hi);
+    f = kbi = pi = 0;
+    if constexpr (CRT) tile_k_range(P, tile, rows, cols, kb_lo, kb_hi);
   }
   __device__ __forceinline__ void settle(const SliceGemmParams& P, int nwork) {
     valid = false;
@@ -182,11 +185,9 @@ struct BlockIter {
         if (work < nwork) load(P);
         continue;
       }
-      const bool some = diag_bounds(t, P.slices, P.num_kb, p_lo, total, P.crt != 0);
-      if (P.crt) total = kb_hi - kb_lo;
-      if (!some || f >= total) {
+      if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, CRT) || f >= (CRT ? kb_hi - kb_lo : total)) {
         --t;
-        f = 0;
+        f = kbi = pi = 0;
         continue;
       }
       valid = true;
@@ -204,6 +205,10 @@ struct BlockIter {
   }
   __device__ __forceinline__ void next(const SliceGemmParams& P, int nwork) {
     ++f;
+    if (++kbi == P.num_kb) {
+      kbi = 0;
+      ++pi;
+    }
     settle(P, nwork);
   }
 };
@@ -252,14 +257,21 @@ __device__ __forceinline__ void slice_producer(const CUtensorMap* tmA, const CUt
   const int nwork = num_work<kListed>(P);
   const int a_row_off = PAIR ? int(rank) * kSliceBM : 0;
   const int b_row_off = PAIR ? int(rank) * L::kBRows : 0;
-  BlockIter<kListed> it;
+  BlockIter<kListed, is_crt_mode(MODE)> it;
   it.start(P, nwork, first_tile<PAIR>(), tile_step<PAIR>(), PAIR ? 2 * kSliceBM : kSliceBM, BN);
   uint32_t issued = 0;  // stage = issued % STAGES, phase = (issued / STAGES) & 1
   bool ok = true;
   while (it.valid) {
     int tm, tn;
     tile_coords(it.tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
-    const int p = it.p_lo + it.f / P.num_kb, kb = P.crt ? it.kb_lo + it.f : it.f % P.num_kb;
+    int p, kb;
+    if constexpr (is_crt_mode(MODE)) {
+      p = it.p_lo;
+      kb = it.kb_lo + it.f;
+    } else {
+      p = it.p_lo + it.pi;
+      kb = it.kbi;
+    }
     const int stage = int(issued % STAGES);
     if (!mbar_wait(&empty[stage], ((issued / STAGES) & 1u) ^ 1u, abort_flag, P.status)) {
       ok = false;
