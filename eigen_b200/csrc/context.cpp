@@ -76,10 +76,40 @@ bool DeviceBuffer::ensure(size_t bytes) {
       return false;
     }
   }
-  if (ptr) cudaFree(ptr);  // implicitly waits for work still using the old buffer
+  if (ptr) {
+    if (held_by_graph)
+      retired.push_back(ptr);  // a captured graph still replays into it
+    else
+      cudaFree(ptr);  // implicitly waits for work still using the old buffer
+  }
   ptr = p;
   cap = want;
+  held_by_graph = false;
   return true;
+}
+
+int reserve_buffer(DeviceBuffer& buf, size_t bytes, cudaStream_t st, const char* what) {
+  cudaStreamCaptureStatus status = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &status) != cudaSuccess) {
+    (void)cudaGetLastError();
+    status = cudaStreamCaptureStatusNone;
+  }
+  if (status != cudaStreamCaptureStatusNone) {
+    if (bytes > buf.cap) {
+      set_error(EB2_ERR_ARG,
+                "a captured call needs %zu bytes of %s, more than the %zu sized so far; make a direct call of this "
+                "size first",
+                bytes, what, buf.cap);
+      return EB2_ERR_ARG;
+    }
+    buf.held_by_graph = true;
+    return EB2_OK;
+  }
+  if (!buf.ensure(bytes)) {
+    set_error(EB2_ERR_ALLOC, "could not allocate %zu bytes of %s", bytes, what);
+    return EB2_ERR_ALLOC;
+  }
+  return EB2_OK;
 }
 
 StreamFence::StreamFence(Context& cx, cudaStream_t st) : cx_(cx), st_(st), active_(false) {

@@ -8,6 +8,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <mutex>
+#include <vector>
 
 #include "eigen_b200/blas.h"
 
@@ -17,9 +18,21 @@ namespace eb2 {
 struct DeviceBuffer {
   void* ptr = nullptr;
   size_t cap = 0;
+  // A CUDA graph captured a call that used `ptr`: its replays read and write that address,
+  // so a later growth keeps the old allocation alive (in `retired`) instead of freeing it.
+  bool held_by_graph = false;
+  std::vector<void*> retired;
   // Returns false (and leaves the old buffer) if the allocation fails.
   bool ensure(size_t bytes);
 };
+
+// Sizes `buf` to at least `bytes` for a call on stream `st`.  Outside a capture it grows the
+// buffer as needed (EB2_ERR_ALLOC if that fails).  In a stream capture an allocation would
+// invalidate the caller's graph, so a buffer that is too small gives EB2_ERR_ARG ("make a
+// direct call of this size first") before anything is enqueued, and a buffer that is large
+// enough becomes held by the graph.  Sets the thread's error on failure; `what` names the
+// buffer in the message.
+int reserve_buffer(DeviceBuffer& buf, size_t bytes, cudaStream_t st, const char* what);
 
 // Flags the kernels write; mirrored into pinned host memory after a call.
 struct DeviceFlags {

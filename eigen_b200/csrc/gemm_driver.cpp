@@ -166,10 +166,7 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   const bool keep_old = check && beta != 0.0;
   const size_t o_save = off;
   off = align256(off + (keep_old && !tri ? size_t(m) * n * 8 : 0));
-  if (!cx.ws.ensure(off)) {
-    set_error(EB2_ERR_ALLOC, "could not allocate %zu bytes of emulation workspace", off);
-    return EB2_ERR_ALLOC;
-  }
+  if (const int rc = reserve_buffer(cx.ws, off, st, "emulation workspace"); rc != EB2_OK) return rc;
   uint8_t* ws = static_cast<uint8_t*>(cx.ws.ptr);
   DeviceFlags* df = cx.dflags;
   CrtOperand oa{reinterpret_cast<int8_t*>(ws + o_res_a), reinterpret_cast<int32_t*>(ws + o_mu_a),
@@ -426,10 +423,7 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   off = align256(off + size_t(smax) * m_cap * k_pad);
   const size_t o_dig_b = off;
   off = align256(off + size_t(smax) * n_cap * k_pad);
-  if (!cx.ws.ensure(off)) {
-    set_error(EB2_ERR_ALLOC, "could not allocate %zu bytes of emulation workspace", off);
-    return EB2_ERR_ALLOC;
-  }
+  if (const int rc = reserve_buffer(cx.ws, off, st, "emulation workspace"); rc != EB2_OK) return rc;
   uint8_t* ws = static_cast<uint8_t*>(cx.ws.ptr);
   const StridedView<double> va = view_a(ta, A, lda, m, k);
   const StridedView<double> vb = view_bt(tb, B, ldb, n, k);
@@ -598,10 +592,7 @@ int sgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   off = align256(off + size_t(3) * m_pad * k_pad * 2);
   const size_t o_b = off;
   off = align256(off + size_t(3) * n_pad * k_pad * 2);
-  if (!cx.ws.ensure(off)) {
-    set_error(EB2_ERR_ALLOC, "could not allocate %zu bytes of emulation workspace", off);
-    return EB2_ERR_ALLOC;
-  }
+  if (const int rc = reserve_buffer(cx.ws, off, st, "emulation workspace"); rc != EB2_OK) return rc;
   uint8_t* ws = static_cast<uint8_t*>(cx.ws.ptr);
   Bf16Operand oa{ws + o_a, m, m_pad, k, k_pad};
   Bf16Operand ob{ws + o_b, n, n_pad, k, k_pad};

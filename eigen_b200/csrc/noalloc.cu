@@ -25,6 +25,7 @@ namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(64) << 20;  // 64 MiB
 constexpr int kNoAllocModuli = kCrtDefaultModuli;
+constexpr int64_t kNoAllocMaxDim = int64_t(1) << 20;  // larger m, n or k never fits the scratch
 constexpr int kMaxDevices = 64;
 
 // The scratch.  Host code must not use this name as an address: on the host it denotes a
@@ -111,6 +112,16 @@ extern "C" int eb2_dgemm_device_noalloc(char transa, char transb, int64_t m, int
     return EB2_ERR_ARG;
   }
   if (m == 0 || n == 0) return EB2_OK;
+  // Every operand keeps 16 residue planes of at least one 128-byte K block per row, so a
+  // dimension above 2^20 needs more than 2 GiB of scratch: refuse it before the layout
+  // arithmetic below, whose products could otherwise wrap for absurd (BLAS-valid) sizes.
+  if (m > kNoAllocMaxDim || n > kNoAllocMaxDim || k > kNoAllocMaxDim) {
+    set_error(EB2_ERR_ARG,
+              "eb2_dgemm_device_noalloc: a %lld x %lld x %lld product cannot fit the fixed %zu bytes of scratch; "
+              "use eb2_dgemm_device for it",
+              static_cast<long long>(m), static_cast<long long>(n), static_cast<long long>(k), kNoAllocScratchBytes);
+    return EB2_ERR_ARG;
+  }
   const DeviceSetup* ds = setup_device();
   if (!ds) return last_error();
   cudaStream_t st = static_cast<cudaStream_t>(stream);

@@ -286,8 +286,12 @@ int eb2_set_timing(int on);
 /* Stream-ordered product on device pointers; no host synchronisation unless the
  * a-posteriori check of the emulated DGEMM needs one (check_accuracy != 0).
  * `stream` is a cudaStream_t (NULL = the legacy default stream).  Returns EB2_*.
- * Both can be captured into a CUDA graph once a first call of the same size has sized the
- * workspace; a DGEMM with check_accuracy != 0 refuses capture (EB2_ERR_ARG). */
+ * Both can be captured into a CUDA graph once a direct call of the same size has sized the
+ * workspace; a captured call that would need a larger workspace returns EB2_ERR_ARG without
+ * enqueueing anything (the capture stays valid), and a DGEMM with check_accuracy != 0 refuses
+ * capture (EB2_ERR_ARG).  A workspace a graph captured is never freed (later growth keeps it),
+ * but replays are not fenced against other calls: do not let a replay overlap another product
+ * on the same GPU. */
 int eb2_dgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, double alpha, const double* a,
                      int64_t lda, const double* b, int64_t ldb, double beta, double* c, int64_t ldc, void* stream,
                      int check_accuracy);

@@ -96,6 +96,14 @@ def test_noalloc_rejects_products_beyond_its_scratch_and_allocates_nothing():
     code, msg = eb.last_error()
     assert code == eb.EB2_ERR_ARG and "scratch" in msg
     assert bool(torch.all(y == 3.0))
+    # dimensions whose scratch size would wrap the layout arithmetic are refused before it
+    # (nothing is read: the refusal comes before any launch, so the small buffers suffice)
+    eb.clear_error()
+    huge = 1 << 31
+    rc = eb.dgemm_device_noalloc("N", "N", huge, 8, huge, 1.0, x, huge, x, huge, 0.0, y, huge)
+    assert rc == eb.EB2_ERR_ARG
+    assert "scratch" in eb.last_error()[1]
+    assert bool(torch.all(y == 3.0))
     # BLAS argument rules
     eb.clear_error()
     assert eb.dgemm_device_noalloc("X", "N", m, n, k, 1.0, dA, lda, dB, ldb, 0.0, dC, ldc) == eb.EB2_ERR_ARG
