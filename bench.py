@@ -60,6 +60,7 @@ def parse_args():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-sgemm", action="store_true", help="skip the split-BF16 / native FP32 SGEMM leg")
     ap.add_argument("--no-level3", action="store_true", help="skip the level-3 routine and complex GEMM leg")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the native-precision sweep (C2) leg")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     a.steps = max(a.steps, 1)
@@ -259,18 +260,75 @@ def peaks():
         return FALLBACK_BF16_TFLOPS, 1400.0, FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic(size: int):
-    """DRAM bytes per launch of the main GEMM kernel from the committed ncu summary
-    (profiles/crt_gemm_i8_8192.md: 'dram_bytes_per_launch: <bytes> at <size>')."""
-    f = ROOT / "profiles" / "crt_gemm_i8_8192.md"
-    try:
-        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)\s*at\s*(\d+)", f.read_text())
-    except OSError:
-        return None
-    if not m:
-        return None
-    b, at = float(m.group(1)), int(m.group(2))
-    return b if at == size else None
+# The main GEMM kernel's instantiation for a method and tile configuration (tile 512 = CTA pair).
+def gemm_instantiation(method_crt: bool, tile: int) -> str:
+    if method_crt:
+        return "slice_gemm_kernel<2, 256, 6, 4, true>" if tile == 512 else "slice_gemm_kernel<2, 256, 4, 4, false>"
+    return "slice_gemm_kernel<0, 128, 8, 8, true>" if tile == 512 else "slice_gemm_kernel<0, 128, 6, 8, false>"
+
+
+def profiled_traffic(size: int, instantiation: str):
+    """DRAM bytes per launch of `instantiation` at `size`^3 from the committed ncu summaries
+    (a line 'dram_bytes_per_launch: <bytes> at <size> for <instantiation>' in profiles/*.md),
+    with the file it came from; (None, None) when no summary covers that kernel and size."""
+    pat = re.compile(r"dram_bytes_per_launch:\s*([0-9.eE+]+)\s*at\s*(\d+)\s*for\s*(\S.*\S)\s*$", re.M)
+    for f in sorted((ROOT / "profiles").glob("*.md")):
+        for m in pat.finditer(f.read_text()):
+            if int(m.group(2)) == size and m.group(3).strip("` ") == instantiation:
+                return float(m.group(1)), f"profiles/{f.name}"
+    return None, None
+
+
+# ------------------------------------------------------------------------ native sweep
+def native_sweep_leg(eb, torch, dev, rank_max, sizes=(1024, 2048, 4096, 8192), reps=3):
+    """The native-precision sweep: DGEMM and SGEMM at M = N = K in `sizes`, NN / NT / TN,
+    alpha = 1.5, beta = 0.5, A, B, C ~ U[-1,1], leading dimensions + 8, through the device entry
+    points with the native kernels (FP64 DMMA, FP32 FFMA) and with the default method (CRT
+    emulation / split-BF16): TFLOP/s (2MNK over the CUDA-event time of one call, best of
+    `reps` after a warm-up), max over ranks."""
+    out = []
+    stream = torch.cuda.Stream(device=dev)
+    g = torch.Generator(device=dev)
+    for dtype, tdt in (("d", torch.float64), ("s", torch.float32)):
+        for S in sizes:
+            ld = S + 8
+            g.manual_seed(S)
+            A = (torch.rand((S, ld), dtype=torch.float64, device=dev, generator=g) * 2 - 1).to(tdt)
+            B = (torch.rand((S, ld), dtype=torch.float64, device=dev, generator=g) * 2 - 1).to(tdt)
+            C0 = (torch.rand((S, ld), dtype=torch.float64, device=dev, generator=g) * 2 - 1).to(tdt)
+            C = C0.clone()
+            for ta, tb in (("N", "N"), ("N", "T"), ("T", "N")):
+                row = {"dtype": dtype, "size": S, "trans": ta + tb}
+                for name, method in (("native", eb.METHOD_NATIVE), ("default", eb.METHOD_AUTO)):
+                    if dtype == "d":
+                        eb.set_dgemm_method(method)
+                        call = lambda: eb.dgemm_device(ta, tb, S, S, S, 1.5, A, ld, B, ld, 0.5, C, ld,  # noqa: E731
+                                                       stream=stream.cuda_stream, check_accuracy=True)
+                    else:
+                        eb.set_sgemm_method(method)
+                        call = lambda: eb.sgemm_device(ta, tb, S, S, S, 1.5, A, ld, B, ld, 0.5, C, ld,  # noqa: E731
+                                                       stream=stream.cuda_stream)
+                    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    best = None
+                    for i in range(reps + 1):
+                        C.copy_(C0)
+                        torch.cuda.synchronize()
+                        ev0.record(stream)
+                        rc = call()
+                        ev1.record(stream)
+                        stream.synchronize()
+                        assert rc == eb.EB2_OK, eb.last_error()
+                        if i:
+                            t = ev0.elapsed_time(ev1)
+                            best = t if best is None else min(best, t)
+                    ms = rank_max(best)
+                    row[name] = {"tflops": round(2.0 * S ** 3 / (ms * 1e-3) / 1e12, 3), "ms": round(ms, 4),
+                                 "method": eb.last_call_info()["method"]}
+                out.append(row)
+            del A, B, C0, C
+    eb.set_dgemm_method(eb.METHOD_AUTO)
+    eb.set_sgemm_method(eb.METHOD_AUTO)
+    return out
 
 
 # ------------------------------------------------------------------------ grouped batch
@@ -652,6 +710,10 @@ def our_arm(a, world, rank, local):
     if not a.no_level3:
         level3 = level3_leg(torch, S)
 
+    sweep = None
+    if not a.no_sweep:
+        sweep = native_sweep_leg(eb, torch, dev, rank_max)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         model, _ = host_cpu_info()
@@ -673,18 +735,25 @@ def our_arm(a, world, rank, local):
     roof = None
     if gemm_ms_avg and method != eb.METHOD_NATIVE:
         achieved = flops / (gemm_ms_avg * 1e-3) / 1e12  # FP64-equivalent TFLOP/s of the GEMM kernel
-        # dense int8 rate = 2 x dense bf16 on sm_100; the GEMM kernel runs inside a seconds-long
-        # loop of back-to-back products under the power cap, so the sustained figure applies
-        int8_peak = 2.0 * bf16_sus
+        # dense int8 rate = 2 x dense bf16 on sm_100.  The burst figure applies to a timed loop
+        # shorter than 2 s (the power cap has not settled the clocks yet), the sustained one above
+        timed_s = ms_emu_max * a.steps * 1e-3
+        sustained = timed_s >= 2.0
+        int8_peak = 2.0 * (bf16_sus if sustained else bf16)
         peak = int8_peak / products  # the FP64-equivalent ceiling of an int8 kernel doing `products` GEMMs
         shape = "CTA pair, 256x256 tiles, cta_group::2" if tile == 512 else "one CTA, 128x256 tiles"
-        kname = "slice_gemm_kernel<CRT>" if method == eb.METHOD_CRT else "slice_gemm_kernel<Ozaki>"
+        inst = gemm_instantiation(method == eb.METHOD_CRT, tile)
+        traffic, traffic_src = profiled_traffic(S, inst)
         roof = {"bound": "tensor", "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": UNIT,
-                "frac": round(achieved / peak, 4), "traffic": profiled_traffic(S),
-                "kernel": f"{kname} (tcgen05.mma kind::i8, {shape}), {gemm_ms_avg:.3f} ms/launch",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "kernel": f"{inst} (tcgen05.mma kind::i8, {shape}), {gemm_ms_avg:.3f} ms/launch",
+                "traffic_source": traffic_src,
                 "pipe": {"achieved_tops": round(achieved * products, 1), "peak_tops": round(int8_peak, 1),
-                         "basis": f"peak = 2 x {basis} sustained dense bf16 ({bf16_sus} TFLOP/s; burst {bf16}), "
-                                  f"of {basis}; {products} int8 products of 2*M*N*K each",
+                         "basis": f"peak = 2 x {basis} {'sustained' if sustained else 'burst'} dense bf16 "
+                                  f"({bf16_sus if sustained else bf16} TFLOP/s), of {basis}; timed region "
+                                  f"{timed_s:.2f} s ({'>=' if sustained else '<'} 2 s); {products} int8 products "
+                                  f"of 2*M*N*K each",
+                         "sustained_frac": round(achieved * products / (2.0 * bf16_sus), 4),
                          "burst_frac": round(achieved * products / (2.0 * bf16), 4)}}
 
     value = whole_job_tflops(world, flops, ms_emu_max)
@@ -698,7 +767,7 @@ def our_arm(a, world, rank, local):
                            kernel_ms_per_call=kernel_ms_per_call),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "native_fp64": native, "accuracy": accuracy, "sgemm": sgemm, "grouped_batch": grouped,
-            "level3_routines": level3,
+            "level3_routines": level3, "native_sweep": sweep,
             "emulated_over_native": round(value / native["tflops"], 3) if native else None,
         }
         print(json.dumps(line))

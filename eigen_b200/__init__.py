@@ -105,6 +105,7 @@ def load(path: str | os.PathLike | None = None, mode: int = ctypes.RTLD_GLOBAL) 
     lib.eb2_set_sgemm_pieces.argtypes = [ctypes.c_int]
     lib.eb2_set_timing.argtypes = [ctypes.c_int]
     lib.eb2_set_slice_tuning.argtypes = [ctypes.c_int, ctypes.c_int]
+    lib.eb2_set_wait_limit_ns.argtypes = [ctypes.c_longlong]
     lib.eb2_last_error_string.restype = ctypes.c_char_p
     lib.eb2_last_call_info.argtypes = [ctypes.POINTER(CallInfo)]
     lib.eb2_version.restype = ctypes.c_char_p
@@ -288,6 +289,11 @@ def set_tile_n(tile_n: int) -> int:
 
 def set_slice_tuning(group_m: int, prefetch: int) -> int:
     return load().eb2_set_slice_tuning(group_m, prefetch)
+
+
+def set_wait_limit_ns(ns: int) -> int:
+    """Wall-time bound (ns) of the tcgen05 GEMM's pipeline waits; 0 = the default (2 s)."""
+    return load().eb2_set_wait_limit_ns(int(ns))
 
 
 def set_picker(weights) -> int:

@@ -297,6 +297,12 @@ int eb2_set_slice_tuning(int group_m, int prefetch) {
   return EB2_OK;
 }
 
+int eb2_set_wait_limit_ns(long long ns) {
+  if (ns < 0) return EB2_ERR_ARG;
+  eb2::tuning().wait_limit_ns = static_cast<uint64_t>(ns);
+  return EB2_OK;
+}
+
 int eb2_set_timing(int on) {
   eb2::settings().timing = on ? 1 : 0;
   return EB2_OK;
@@ -317,8 +323,8 @@ int eb2_dgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, 
                    eb2::gemm_info(transa, transb, m, n, k, lda, ldb, ldc));
     return EB2_ERR_ARG;
   }
-  eb2::Context* cx = eb2::current_context();
-  if (!cx) return EB2_ERR_NO_DEVICE;
+  eb2::Context* cx = eb2::context_for_stream(static_cast<cudaStream_t>(stream));
+  if (!cx) return eb2::last_error();
   if (check_accuracy) {
     // the a-posteriori check reads the estimate on the host between kernels
     cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
@@ -349,8 +355,8 @@ int eb2_sgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, 
                    eb2::gemm_info(transa, transb, m, n, k, lda, ldb, ldc));
     return EB2_ERR_ARG;
   }
-  eb2::Context* cx = eb2::current_context();
-  if (!cx) return EB2_ERR_NO_DEVICE;
+  eb2::Context* cx = eb2::context_for_stream(static_cast<cudaStream_t>(stream));
+  if (!cx) return eb2::last_error();
   std::lock_guard<std::mutex> lock(cx->mu);
   eb2::StreamFence fence(*cx, static_cast<cudaStream_t>(stream));
   eb2::SgemmOptions o;

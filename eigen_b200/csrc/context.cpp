@@ -191,6 +191,31 @@ Context* current_context() {
   return c;
 }
 
+Context* context_for_stream(cudaStream_t st) {
+  cudaStreamCaptureStatus status = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &status) != cudaSuccess) {
+    (void)cudaGetLastError();
+    status = cudaStreamCaptureStatusNone;
+  }
+  if (status != cudaStreamCaptureStatusNone) {
+    int dev = -1;
+    bool exists = false;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices) {
+      std::lock_guard<std::mutex> lock(g_ctx_mu);
+      exists = g_ctx[dev] != nullptr;
+    } else {
+      (void)cudaGetLastError();
+    }
+    if (!exists) {
+      set_error(EB2_ERR_ARG,
+                "the first call on a device creates its context (allocations) and cannot be captured; make a "
+                "direct call first");
+      return nullptr;
+    }
+  }
+  return current_context();
+}
+
 }  // namespace eb2
 
 extern "C" const char* eb2_last_error_string(void) { return eb2::last_error_string(); }

@@ -93,6 +93,10 @@ class StreamFence {
 // Context of the calling thread's current device, created on first use.
 // Returns nullptr (and sets the thread's error) when no usable device exists.
 Context* current_context();
+// current_context() for a call enqueued on `st`: creating a device's context allocates, which
+// would invalidate a stream capture, so a capture on a device that has no context yet gets
+// nullptr with EB2_ERR_ARG ("make a direct call first") and nothing enqueued.
+Context* context_for_stream(cudaStream_t st);
 
 struct Settings {
   std::atomic<int> dgemm_method{EB2_METHOD_AUTO};

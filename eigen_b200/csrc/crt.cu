@@ -913,6 +913,7 @@ cudaError_t launch_gemm_config(const CrtOperand& a, const CrtOperand& b, const C
   P.skip_if_flag = args.skip_if_flag;
   P.status = args.status;
   P.group_m = tuning().group_m > 0 ? tuning().group_m : P.tiles_m;
+  P.wait_limit_ns = tuning().wait_limit_ns ? tuning().wait_limit_ns : kWaitLimitNs;
   P.crt = 1;
   P.residues = args.cres;
   P.ld_res = args.ld_res;

@@ -26,6 +26,10 @@ enum : uint32_t {
 // Wall-time limit for one mbarrier wait (ns).  The longest legitimate wait in
 // these kernels is one accumulation unit of one tile (well under 10 ms).
 constexpr uint64_t kWaitLimitNs = 2000000000ull;
+// Limits below this poll with the non-blocking test_wait and read the clock on every spin,
+// so that a short limit is measured from the first failed test, not after a blocking
+// try_wait that may itself last until the phase completes.
+constexpr uint64_t kShortWaitNs = 1000000ull;
 
 __device__ __forceinline__ uint64_t globaltimer_ns() {
   uint64_t t;
@@ -68,13 +72,34 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 // Bounded wait for the phase with the given parity to complete.  `abort_flag`
 // (shared memory) lets one role that gave up release the others quickly.
-// Returns false when the wait was abandoned.
+// Returns false when the wait was abandoned.  `limit_ns` is the wall-time bound.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
-                                          uint32_t* status) {
+                                          uint32_t* status, uint64_t limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   uint64_t t0 = globaltimer_ns();
+  if (limit_ns < kShortWaitNs) {
+    while (!mbar_test_wait(bar, parity)) {
+      if ((abort_flag && *abort_flag) || globaltimer_ns() - t0 > limit_ns) {
+        const bool aborted = abort_flag && *abort_flag;
+        atomicOr(status, aborted ? EB2_DEV_ERR_ABORTED : EB2_DEV_ERR_TIMEOUT);
+        if (abort_flag) *abort_flag = 1;
+        return false;
+      }
+    }
+    return true;
+  }
   uint32_t spins = 0;
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
@@ -83,7 +108,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
         atomicOr(status, EB2_DEV_ERR_ABORTED);
         return false;
       }
-      if (globaltimer_ns() - t0 > kWaitLimitNs) {
+      if (globaltimer_ns() - t0 > limit_ns) {
         atomicOr(status, EB2_DEV_ERR_TIMEOUT);
         if (abort_flag) *abort_flag = 1;
         return false;

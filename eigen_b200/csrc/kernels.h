@@ -12,6 +12,9 @@ namespace eb2 {
 struct SliceTuning {
   int group_m = 0;   // row-tiles per raster group; 0 = all (column-major tile order)
   int prefetch = 0;  // L2 prefetch distance in K blocks; 0 = off
+  // wall-time limit (ns) of the GEMM's pipeline waits; 0 = the default (2 s).  The waits
+  // that drain copies and MMAs already issued keep the default.
+  uint64_t wait_limit_ns = 0;
 };
 SliceTuning& tuning();
 

@@ -212,6 +212,7 @@ cudaError_t launch_config(const OzakiOperand& a, const OzakiOperand& b, const Oz
   P.err_sq = args.err_sq;
   P.status = args.status;
   P.group_m = tuning().group_m > 0 ? tuning().group_m : P.tiles_m;
+  P.wait_limit_ns = tuning().wait_limit_ns ? tuning().wait_limit_ns : kWaitLimitNs;
   return launch_slice_gemm<kModeOzakiI8, BN, STAGES, 8, PAIR>(tmA, tmB, P, args.num_sms, stream);
 }
 

@@ -7,8 +7,9 @@
 //     the epilogue scales it exactly to FP64 and adds it into a per-thread FP64 register
 //     accumulator, writing C once per tile: C = alpha * sum_t D_t 2^(e_i+f_j+w_t) (+ beta C);
 //   * split-BF16 SGEMM: A_p, B_q are the hi/mid/lo BF16 pieces of the FP32 inputs;
-//     the pieces carry their own exponents, so the whole triangle accumulates into one
-//     FP32 TMEM accumulator and the epilogue applies alpha/beta once.
+//     the pieces carry their own exponents, so all of the triangle's products over a chunk
+//     of K accumulate into one FP32 TMEM accumulator; the epilogue adds the chunks into
+//     FP32 registers (round to nearest) and applies alpha/beta once per tile.
 //
 // Roles: warp 0 = TMA producer, warp 1 = MMA issuer + TMEM owner, warps 2.. = epilogue
 // (NW warps; warp w may read TMEM lanes 32*(w%4)..+31, one output row per thread).
@@ -44,6 +45,12 @@ constexpr int kSliceKBytes = 128;  // bytes of K per pipeline stage
 constexpr int kMaxUnitKb = 4095;
 // CRT residues lie in [-128, 127]: 1023 * 128 * 128 * 128 < 2^31.
 constexpr int kMaxUnitKbCrt = 1023;
+// Split-BF16: K blocks (64 bf16 each) per FP32 accumulation unit.  The tensor core's FP32
+// accumulation is not a round-to-nearest sum: its error grows with the number of MMAs that
+// add into one accumulator and with the accumulator's magnitude.  So every 256 elements of K
+// the unit's sum (all pieces' products over those K) leaves TMEM and is added, rounded to
+// nearest, into FP32 registers of the epilogue; the accumulator restarts from zero.
+constexpr int kBf16ChunkKb = 4;
 
 template <int BN, int STAGES, bool PAIR>
 struct SliceLayout {
@@ -86,6 +93,7 @@ struct SliceGemmParams {
   int num_listed;        // CRT: entries of tile_list
   int tri_k;             // CRT: 1 = op(A) lower, 2 = op(A) upper, 3 = op(B) lower, 4 = op(B) upper
                          // triangular (zero blocks of K skipped per tile); 0 = dense
+  uint64_t wait_limit_ns;  // wall-time bound of the pipeline waits (the drain waits keep kWaitLimitNs)
 };
 
 // Pair range of diagonal t: p = p_lo .. p_lo + total/num_kb - 1 (q = t - p).
@@ -257,26 +265,12 @@ __device__ __forceinline__ void slice_producer(const CUtensorMap* tmA, const CUt
   const int nwork = num_work<kListed>(P);
   const int a_row_off = PAIR ? int(rank) * kSliceBM : 0;
   const int b_row_off = PAIR ? int(rank) * L::kBRows : 0;
-  BlockIter<kListed, is_crt_mode(MODE)> it;
-  it.start(P, nwork, first_tile<PAIR>(), tile_step<PAIR>(), PAIR ? 2 * kSliceBM : kSliceBM, BN);
   uint32_t issued = 0;  // stage = issued % STAGES, phase = (issued / STAGES) & 1
   bool ok = true;
-  while (it.valid) {
-    int tm, tn;
-    tile_coords(it.tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
-    int p, kb;
-    if constexpr (is_crt_mode(MODE)) {
-      p = it.p_lo;
-      kb = it.kb_lo + it.f;
-    } else {
-      p = it.p_lo + it.pi;
-      kb = it.kbi;
-    }
+  // one stage: A piece p - 1 and B piece q_slice at K block kb of the tile (tm, tn)
+  auto issue = [&](int tm, int tn, int p, int q_slice, int kb) -> bool {
     const int stage = int(issued % STAGES);
-    if (!mbar_wait(&empty[stage], ((issued / STAGES) & 1u) ^ 1u, abort_flag, P.status)) {
-      ok = false;
-      break;
-    }
+    if (!mbar_wait(&empty[stage], ((issued / STAGES) & 1u) ^ 1u, abort_flag, P.status, P.wait_limit_ns)) return false;
     const int a_row = tm * (PAIR ? 2 * kSliceBM : kSliceBM) + a_row_off;
     const int b_row = tn * BN + b_row_off;
     if (PAIR) {
@@ -284,19 +278,58 @@ __device__ __forceinline__ void slice_producer(const CUtensorMap* tmA, const CUt
       const uint32_t leader_full = mapa_shared(smem_u32(&full[stage]), 0);
       if (rank == 0) mbar_arrive_expect_tx(&full[stage], kTx);
       tma_load_3d_pair(smem + L::kAOff + stage * L::kABytes, tmA, leader_full, kb * ke, a_row, p - 1);
-      tma_load_3d_pair(smem + L::kBOff + stage * L::kBBytes, tmB, leader_full, kb * ke, b_row,
-                       b_slice(it.t, p, P.crt != 0));
+      tma_load_3d_pair(smem + L::kBOff + stage * L::kBBytes, tmB, leader_full, kb * ke, b_row, q_slice);
     } else {
       mbar_arrive_expect_tx(&full[stage], kTx);
       tma_load_3d(smem + L::kAOff + stage * L::kABytes, tmA, &full[stage], kb * ke, a_row, p - 1);
-      tma_load_3d(smem + L::kBOff + stage * L::kBBytes, tmB, &full[stage], kb * ke, b_row, b_slice(it.t, p, P.crt != 0));
+      tma_load_3d(smem + L::kBOff + stage * L::kBBytes, tmB, &full[stage], kb * ke, b_row, q_slice);
     }
     ++issued;
-    it.next(P, nwork);
+    return true;
+  };
+  if constexpr (MODE == kModeSplitBF16) {
+    // chunks of kBf16ChunkKb K blocks; in each, the diagonals (smallest weight first), their
+    // pairs and the chunk's K blocks -- the order slice_mma consumes them in
+    for (int w = first_tile<PAIR>(); w < nwork && ok; w += tile_step<PAIR>()) {
+      int tm, tn;
+      tile_coords(w, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
+      for (int kc = 0; kc < P.num_kb && ok; kc += kBf16ChunkKb) {
+        const int kend = min(P.num_kb, kc + kBf16ChunkKb);
+        for (int t = P.diag_hi; t >= P.diag_lo && ok; --t) {
+          int p_lo, total;
+          if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total)) continue;
+          const int p_hi = p_lo + total / P.num_kb;
+          for (int p = p_lo; p < p_hi && ok; ++p)
+            for (int kb = kc; kb < kend && ok; ++kb) ok = issue(tm, tn, p, b_slice(t, p, false), kb);
+        }
+      }
+    }
+  } else {
+    BlockIter<kListed, is_crt_mode(MODE)> it;
+    it.start(P, nwork, first_tile<PAIR>(), tile_step<PAIR>(), PAIR ? 2 * kSliceBM : kSliceBM, BN);
+    while (it.valid) {
+      int tm, tn;
+      tile_coords(it.tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
+      int p, kb;
+      if constexpr (is_crt_mode(MODE)) {
+        p = it.p_lo;
+        kb = it.kb_lo + it.f;
+      } else {
+        p = it.p_lo + it.pi;
+        kb = it.kbi;
+      }
+      if (!issue(tm, tn, p, b_slice(it.t, p, P.crt != 0), kb)) {
+        ok = false;
+        break;
+      }
+      it.next(P, nwork);
   }
-  if (!ok && !PAIR) {
-    // let the copies still in flight land before the CTA can exit (bounded); a pair's
-    // copies complete on the leader, and the final cluster barrier keeps both CTAs alive
+  }
+  if (!PAIR) {
+    // let the copies still in flight land before the CTA can exit (bounded).  Also when this
+    // loop finished: the MMA issuer may have given up before consuming the last stages.  On
+    // the normal path their phases are complete and each wait returns at once.  A pair's
+    // copies complete on the leader, and the final cluster barrier keeps both CTAs alive.
     volatile int no_abort = 0;
     for (uint32_t i = issued > STAGES ? issued - STAGES : 0; i < issued; ++i)
       (void)mbar_wait(&full[i % STAGES], (i / STAGES) & 1u, &no_abort, P.status);
@@ -304,8 +337,9 @@ __device__ __forceinline__ void slice_producer(const CUtensorMap* tmA, const CUt
 }
 
 // ------------------------------------------------------------------ MMA issuer (warp 1, one lane; leader only)
-// Ozaki: one accumulation unit per diagonal chunk (exact INT32).  Split-BF16: the whole
-// triangle of a tile is one unit (FP32 accumulation in a single accumulator).
+// Ozaki / CRT: one accumulation unit per diagonal or modulus (exact INT32, cut into chunks
+// where K is too long).  Split-BF16: one unit per kBf16ChunkKb K blocks of a tile, covering
+// every piece product over those K (FP32 accumulation, drained by the epilogue).
 template <bool PAIR>
 __device__ __forceinline__ void commit_to(uint64_t* bar) {
   if (PAIR) {
@@ -323,83 +357,98 @@ __device__ __forceinline__ void slice_mma(uint8_t* smem, uint64_t* full, uint64_
                                           volatile int* abort_flag, const SliceGemmParams& P) {
   using L = SliceLayout<BN, STAGES, PAIR>;
   constexpr uint32_t idesc = SliceTraits<MODE, BN, PAIR>::kIdesc;
-  constexpr bool kTileUnit = (MODE == kModeSplitBF16);
   constexpr bool kListed = MODE == kModeCrtI8Listed;
   const int nwork = num_work<kListed>(P);
   uint32_t consumed = 0;  // stage = consumed % STAGES, phase = (consumed / STAGES) & 1
   int buf = 0;
   uint32_t tphase = 0u;  // bit b: phase of accumulator buffer b
   bool ok = true;
-  for (int w = first_tile<PAIR>(); w < nwork && ok; w += tile_step<PAIR>()) {
-    int tile, t_hi, t_lo;
-    work_item<kListed>(P, w, tile, t_hi, t_lo);
-    bool fresh = true;  // the next MMA overwrites the accumulator
-    if (kTileUnit) {
-      if (!mbar_wait(&tempty[buf], ((tphase >> buf) & 1u) ^ 1u, abort_flag, P.status)) break;
-      tc_fence_after();
-    }
-    for (int t = t_hi; t >= t_lo && ok; --t) {
-      int p_lo, total;
-      if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, is_crt_mode(MODE))) continue;
-      if constexpr (is_crt_mode(MODE)) {
-        int kb_lo, kb_hi;
-        tile_k_range(P, tile, PAIR ? 2 * kSliceBM : kSliceBM, BN, kb_lo, kb_hi);
-        total = kb_hi - kb_lo;
-      }
-      constexpr int kUnit = SliceTraits<MODE, BN, PAIR>::kUnitKb;
-      for (int u0 = 0; u0 < total && ok;) {
-        const int u1 = (kTileUnit || total - u0 <= kUnit) ? total : u0 + kUnit;
-        if (!kTileUnit) {
-          if (!mbar_wait(&tempty[buf], ((tphase >> buf) & 1u) ^ 1u, abort_flag, P.status)) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-          fresh = true;
-        }
-        const uint32_t d_tmem = tmem_base + uint32_t(buf * BN);
-        for (int f = u0; f < u1; ++f) {
-          const int stage = int(consumed % STAGES);
-          if (!mbar_wait(&full[stage], (consumed / STAGES) & 1u, abort_flag, P.status)) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-          const uint64_t adesc = make_sw128_kmajor_desc(smem_u32(smem + L::kAOff + stage * L::kABytes));
-          const uint64_t bdesc = make_sw128_kmajor_desc(smem_u32(smem + L::kBOff + stage * L::kBBytes));
+  // the MMAs of one stage into accumulator d_tmem (fresh: the first overwrites it)
+  auto consume = [&](uint32_t d_tmem, bool fresh) -> bool {
+    const int stage = int(consumed % STAGES);
+    if (!mbar_wait(&full[stage], (consumed / STAGES) & 1u, abort_flag, P.status, P.wait_limit_ns)) return false;
+    tc_fence_after();
+    const uint64_t adesc = make_sw128_kmajor_desc(smem_u32(smem + L::kAOff + stage * L::kABytes));
+    const uint64_t bdesc = make_sw128_kmajor_desc(smem_u32(smem + L::kBOff + stage * L::kBBytes));
 #pragma unroll
-          for (int kk = 0; kk < kSliceKBytes / 32; ++kk) {
-            const uint32_t acc = (fresh && kk == 0) ? 0u : 1u;
-            const uint64_t ad = adesc + uint64_t(2 * kk), bd = bdesc + uint64_t(2 * kk);
-            if (PAIR) {
-              if (MODE != kModeSplitBF16)
-                mma_i8_pair(d_tmem, ad, bd, idesc, acc);
-              else
-                mma_f16_pair(d_tmem, ad, bd, idesc, acc);
-            } else {
-              if (MODE != kModeSplitBF16)
-                mma_i8(d_tmem, ad, bd, idesc, acc);
-              else
-                mma_f16(d_tmem, ad, bd, idesc, acc);
+    for (int kk = 0; kk < kSliceKBytes / 32; ++kk) {
+      const uint32_t acc = (fresh && kk == 0) ? 0u : 1u;
+      const uint64_t ad = adesc + uint64_t(2 * kk), bd = bdesc + uint64_t(2 * kk);
+      if (PAIR) {
+        if (MODE != kModeSplitBF16)
+          mma_i8_pair(d_tmem, ad, bd, idesc, acc);
+        else
+          mma_f16_pair(d_tmem, ad, bd, idesc, acc);
+      } else {
+        if (MODE != kModeSplitBF16)
+          mma_i8(d_tmem, ad, bd, idesc, acc);
+        else
+          mma_f16(d_tmem, ad, bd, idesc, acc);
+      }
+    }
+    commit_to<PAIR>(&empty[stage]);
+    ++consumed;
+    return true;
+  };
+  if constexpr (MODE == kModeSplitBF16) {
+    // one accumulation unit per chunk of kBf16ChunkKb K blocks (order as in slice_producer)
+    for (int w = first_tile<PAIR>(); w < nwork && ok; w += tile_step<PAIR>()) {
+      for (int kc = 0; kc < P.num_kb && ok; kc += kBf16ChunkKb) {
+        const int kend = min(P.num_kb, kc + kBf16ChunkKb);
+        if (!mbar_wait(&tempty[buf], ((tphase >> buf) & 1u) ^ 1u, abort_flag, P.status, P.wait_limit_ns)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d_tmem = tmem_base + uint32_t(buf * BN);
+        bool fresh = true;
+        for (int t = P.diag_hi; t >= P.diag_lo && ok; --t) {
+          int p_lo, total;
+          if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total)) continue;
+          const int p_hi = p_lo + total / P.num_kb;
+          for (int p = p_lo; p < p_hi && ok; ++p)
+            for (int kb = kc; kb < kend && ok; ++kb) {
+              ok = consume(d_tmem, fresh);
+              fresh = false;
             }
-          }
-          fresh = false;
-          commit_to<PAIR>(&empty[stage]);
-          ++consumed;
         }
         if (!ok) break;
-        if (!kTileUnit) {
+        commit_to<PAIR>(&tfull[buf]);
+        tphase ^= 1u << buf;
+        buf ^= 1;
+      }
+    }
+  } else {
+    // one accumulation unit per diagonal (Ozaki) or modulus (CRT), cut where K exceeds what
+    // the INT32 accumulator holds exactly
+    for (int w = first_tile<PAIR>(); w < nwork && ok; w += tile_step<PAIR>()) {
+      int tile, t_hi, t_lo;
+      work_item<kListed>(P, w, tile, t_hi, t_lo);
+      for (int t = t_hi; t >= t_lo && ok; --t) {
+        int p_lo, total;
+        if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, is_crt_mode(MODE))) continue;
+        if constexpr (is_crt_mode(MODE)) {
+          int kb_lo, kb_hi;
+          tile_k_range(P, tile, PAIR ? 2 * kSliceBM : kSliceBM, BN, kb_lo, kb_hi);
+          total = kb_hi - kb_lo;
+        }
+        constexpr int kUnit = SliceTraits<MODE, BN, PAIR>::kUnitKb;
+        for (int u0 = 0; u0 < total && ok;) {
+          const int u1 = total - u0 <= kUnit ? total : u0 + kUnit;
+          if (!mbar_wait(&tempty[buf], ((tphase >> buf) & 1u) ^ 1u, abort_flag, P.status, P.wait_limit_ns)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d_tmem = tmem_base + uint32_t(buf * BN);
+          for (int f = u0; f < u1 && ok; ++f) ok = consume(d_tmem, f == u0);
+          if (!ok) break;
           commit_to<PAIR>(&tfull[buf]);
           tphase ^= 1u << buf;
           buf ^= 1;
+          u0 = u1;
         }
-        u0 = u1;
       }
-    }
-    if (kTileUnit && ok) {
-      commit_to<PAIR>(&tfull[buf]);
-      tphase ^= 1u << buf;
-      buf ^= 1;
     }
   }
   // every issued MMA must finish before TMEM is released
@@ -466,7 +515,7 @@ __device__ __forceinline__ void ozaki_epilogue(uint32_t tmem_base, uint64_t* tfu
       const bool est_hi = P.err_sq != nullptr && t == P.diag_hi;
       const bool est_lo = P.err_sq != nullptr && t == 2;
       for (int u0 = 0; u0 < total && ok; u0 += kMaxUnitKb) {
-        if (!mbar_wait(&tfull[buf], (ephase >> buf) & 1u, abort_flag, P.status)) {
+        if (!mbar_wait(&tfull[buf], (ephase >> buf) & 1u, abort_flag, P.status, P.wait_limit_ns)) {
           ok = false;
           break;
         }
@@ -568,7 +617,7 @@ __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull
       const uint32_t bias = (0x7FE00000u + pm - 1u) / pm * pm;
       uint8_t* rp = P.residues + int64_t(t) * plane + grow;
       for (int u0 = 0; u0 < total && ok; u0 += kMaxUnitKbCrt) {
-        if (!mbar_wait(&tfull[buf], (ephase >> buf) & 1u, abort_flag, P.status)) {
+        if (!mbar_wait(&tfull[buf], (ephase >> buf) & 1u, abort_flag, P.status, P.wait_limit_ns)) {
           ok = false;
           break;
         }
@@ -601,12 +650,14 @@ __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull
   }
 }
 
-// Split-BF16: C = alpha * acc + beta * C in FP32, one unit per tile.
+// Split-BF16: each thread owns one row and kCols columns of the tile.  The units of a tile
+// (one per kBf16ChunkKb K blocks) are added, rounded to nearest, into FP32 registers; after
+// the last one C = alpha * acc + beta * C in FP32.
 template <int BN, int NW, bool PAIR>
 __device__ __forceinline__ void bf16_epilogue(uint32_t tmem_base, uint64_t* tfull, uint64_t* tempty,
                                               volatile int* abort_flag, const SliceGemmParams& P) {
   constexpr int kCols = BN * 4 / NW;
-  static_assert(kCols % 32 == 0, "column slice");
+  static_assert(kCols % 32 == 0 && kCols <= 128, "register budget of the FP32 accumulator");
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int quad = warp & 3;
   const int col_base = ((warp - 2) >> 2) * kCols;
@@ -616,36 +667,47 @@ __device__ __forceinline__ void bf16_epilogue(uint32_t tmem_base, uint64_t* tful
   float* C = static_cast<float*>(P.C);
   int buf = 0;
   uint32_t ephase = 0u;
-  for (int tile = first_tile<PAIR>(); tile < num_tiles; tile += tile_step<PAIR>()) {
+  bool ok = true;
+  for (int tile = first_tile<PAIR>(); tile < num_tiles && ok; tile += tile_step<PAIR>()) {
     int tm, tn;
     tile_coords(tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
     const int64_t m0 = int64_t(tm) * (PAIR ? 2 * kSliceBM : kSliceBM) + row_base;
     const int64_t n0 = int64_t(tn) * BN + col_base;
-    if (!mbar_wait(&tfull[buf], (ephase >> buf) & 1u, abort_flag, P.status)) break;
-    tc_fence_after();
-    const uint32_t taddr = tmem_base + uint32_t(buf * BN + col_base) + (uint32_t(quad * 32) << 16);
-    const int64_t grow = m0 + row;
-#pragma unroll 1
-    for (int c = 0; c < kCols / 32; ++c) {
-      uint32_t r[32];
-      tmem_ld_32x32b_x32(taddr + uint32_t(c * 32), r);
-      tmem_ld_wait();
-      if (grow < P.m) {
-        float* cp = C + grow + (n0 + c * 32) * P.ldc;
+    float acc[kCols];
 #pragma unroll
-        for (int jj = 0; jj < 32; ++jj) {
-          if (n0 + c * 32 + jj < P.n) {
-            float* dst = cp + int64_t(jj) * P.ldc;
-            const float v = __fmul_rn(P.alpha_f, __uint_as_float(r[jj]));
-            *dst = (P.beta_f == 0.0f) ? v : __fmaf_rn(P.beta_f, *dst, v);
-          }
+    for (int j = 0; j < kCols; ++j) acc[j] = 0.0f;
+    for (int kc = 0; kc < P.num_kb; kc += kBf16ChunkKb) {
+      if (!mbar_wait(&tfull[buf], (ephase >> buf) & 1u, abort_flag, P.status, P.wait_limit_ns)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t taddr = tmem_base + uint32_t(buf * BN + col_base) + (uint32_t(quad * 32) << 16);
+#pragma unroll
+      for (int c = 0; c < kCols / 16; ++c) {
+        uint32_t r[16];
+        tmem_ld_32x32b_x16(taddr + uint32_t(c * 16), r);
+        tmem_ld_wait();
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) acc[c * 16 + jj] = __fadd_rn(acc[c * 16 + jj], __uint_as_float(r[jj]));
+      }
+      tc_fence_before();
+      acc_release<PAIR>(&tempty[buf]);
+      ephase ^= 1u << buf;
+      buf ^= 1;
+    }
+    const int64_t grow = m0 + row;
+    if (ok && grow < P.m) {
+      float* cp = C + grow + n0 * P.ldc;
+#pragma unroll
+      for (int j = 0; j < kCols; ++j) {
+        if (n0 + j < P.n) {
+          float* dst = cp + int64_t(j) * P.ldc;
+          const float v = __fmul_rn(P.alpha_f, acc[j]);
+          *dst = (P.beta_f == 0.0f) ? v : __fmaf_rn(P.beta_f, *dst, v);
         }
       }
     }
-    tc_fence_before();
-    acc_release<PAIR>(&tempty[buf]);
-    ephase ^= 1u << buf;
-    buf ^= 1;
   }
 }
 

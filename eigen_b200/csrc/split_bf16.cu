@@ -102,7 +102,9 @@ cudaError_t launch_config(const Bf16Operand& a, const Bf16Operand& b, const Sgem
   P.skip_if_flag = args.skip_if_flag;
   P.status = args.status;
   P.group_m = tuning().group_m > 0 ? tuning().group_m : P.tiles_m;
-  return launch_slice_gemm<kModeSplitBF16, BN, STAGES, 4, PAIR>(tmA, tmB, P, args.num_sms, stream);
+  P.wait_limit_ns = tuning().wait_limit_ns ? tuning().wait_limit_ns : kWaitLimitNs;
+  // 128 accumulator columns per epilogue thread: 4 epilogue warps for 128-wide tiles, 8 for 256
+  return launch_slice_gemm<kModeSplitBF16, BN, STAGES, BN / 32, PAIR>(tmA, tmB, P, args.num_sms, stream);
 }
 
 }  // namespace

@@ -249,6 +249,13 @@ int eb2_set_tile_n(int tile_n);
  * (0 = off). */
 int eb2_set_slice_tuning(int group_m, int prefetch);
 
+/* Wall-time bound, in nanoseconds, of each pipeline wait inside the tcgen05 GEMM kernels
+ * (0 = the default, 2 s).  No counterpart in the reference: a kernel whose wait runs out
+ * stops issuing work, lets the copies and MMAs already in flight finish, releases its tensor
+ * memory and returns; the call then reports EB2_ERR_TIMEOUT and C is invalid.  The device
+ * stays usable.  Values below 1 ms are meant for testing that path.  Process-wide. */
+int eb2_set_wait_limit_ns(long long ns);
+
 /* Sticky last error of this thread (EB2_OK if none) and its message. */
 int eb2_last_error(void);
 const char* eb2_last_error_string(void);

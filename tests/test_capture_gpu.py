@@ -140,22 +140,36 @@ def test_replay_after_workspace_growth(dtype):
 _FIRST_CAPTURE = r"""
 import torch, eigen_b200 as eb
 eb.load()
-eb.set_dgemm_method(eb.METHOD_CRT)
-eb.set_dgemm_moduli(16)
 S = 1024
 A = torch.rand((S, S), dtype=torch.float64, device="cuda")
 C = torch.zeros((S, S), dtype=torch.float64, device="cuda")
 s = torch.cuda.Stream()
-graph = torch.cuda.CUDAGraph()
-with torch.cuda.graph(graph, stream=s):
-    rc = eb.dgemm_device("N", "N", S, S, S, 1.0, A, S, A, S, 0.0, C, S, stream=s.cuda_stream, check_accuracy=False)
-    C.add_(1.0)
-assert rc == eb.EB2_ERR_ARG, rc
-assert "direct call of this size first" in eb.last_error()[1], eb.last_error()
-eb.clear_error()
-graph.replay()
-torch.cuda.synchronize()
-assert torch.all(C == 1.0)
+
+def captured(expect):
+    C.zero_()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s):
+        rc = eb.dgemm_device("N", "N", S, S, S, 1.0, A, S, A, S, 0.0, C, S, stream=s.cuda_stream,
+                             check_accuracy=False)
+        C.add_(1.0)  # the capture itself stays valid
+    assert rc == eb.EB2_ERR_ARG, rc
+    assert expect in eb.last_error()[1], eb.last_error()
+    eb.clear_error()
+    graph.replay()
+    torch.cuda.synchronize()
+    assert torch.all(C == 1.0)
+
+# no context on the device yet: creating it would allocate inside the capture
+captured("direct call first")
+# a context, but no workspace yet (the native method needs none)
+eb.set_dgemm_method(eb.METHOD_NATIVE)
+with torch.cuda.stream(s):
+    assert eb.dgemm_device("N", "N", 64, 64, 64, 1.0, A, S, A, S, 0.0, C, S, stream=s.cuda_stream,
+                           check_accuracy=False) == eb.EB2_OK
+s.synchronize()
+eb.set_dgemm_method(eb.METHOD_CRT)
+eb.set_dgemm_moduli(16)
+captured("direct call of this size first")
 with torch.cuda.stream(s):
     assert eb.dgemm_device("N", "N", S, S, S, 1.0, A, S, A, S, 0.0, C, S, stream=s.cuda_stream,
                            check_accuracy=False) == eb.EB2_OK
@@ -174,9 +188,10 @@ print("ok")
 
 
 def test_capture_before_any_direct_call_refuses():
-    """In a fresh process the workspace is empty: a captured call must not allocate inside the
-    capture (that would invalidate it) and returns EB2_ERR_ARG instead; after a direct call of
-    the same size the capture works."""
+    """In a fresh process neither the device context nor the workspace exists: a captured call
+    must not create them inside the capture (the allocations would invalidate it) and returns
+    EB2_ERR_ARG instead, leaving the capture valid; after a direct call of the same size the
+    capture works."""
     import subprocess
     import sys
     from pathlib import Path

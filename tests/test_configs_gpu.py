@@ -99,3 +99,62 @@ def test_native_precision_sweep(size, ta, tb, dtype):
     limit = 1.5 if dtype == "d" else 4.0
     for method in methods[1:]:
         assert errs[method] <= limit * errs[eb.METHOD_NATIVE] + 1e-300, errs
+
+
+def _dev_operand(rows, cols, pad, gen, tdt):
+    """Column-major rows x cols matrix with leading dimension rows + pad, entries U[-1,1], on
+    the device: a (cols, ld) row-major tensor holds the column-major bytes."""
+    ld = rows + pad
+    return (torch.rand((cols, ld), dtype=torch.float64, device="cuda", generator=gen) * 2 - 1).to(tdt), ld
+
+
+def _op_rows(X, trans, idx, k):
+    """Rows idx of op(X) (op(X) is len x k) as a host float64 array, from the device tensor."""
+    if trans == "N":  # op(X)(i, l) = X[i + l*ld]: element (i, l) is X_t[l, i]
+        return X[:k, idx].T.double().cpu().numpy()
+    return X[idx, :k].double().cpu().numpy()  # op(X)(i, l) = X[l + i*ld] = X_t[i, l]
+
+
+@pytest.mark.parametrize("size", [4096, 8192])
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("N", "T"), ("T", "N")])
+@pytest.mark.parametrize("dtype", ["d", "s"])
+def test_native_precision_sweep_large(size, ta, tb, dtype):
+    """The sweep's 4096 and 8192 cases with device operands through dgemm_ / sgemm_ (alpha = 1.5,
+    beta = 0.5, leading dimensions + 8): each method within the error bound on a sampled 32 x 32
+    block against the double-double oracle, the DGEMM emulations at least as accurate as the FP64
+    kernel there and split-BF16 SGEMM within 4x of the FP32 FFMA kernel's error."""
+    m = n = k = size
+    tdt = torch.float64 if dtype == "d" else torch.float32
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(size + ord(ta) + 3 * ord(tb))
+    A, lda = _dev_operand(*((m, k) if ta == "N" else (k, m)), 8, gen, tdt)
+    B, ldb = _dev_operand(*((k, n) if tb == "N" else (n, k)), 8, gen, tdt)
+    C0, ldc = _dev_operand(m, n, 8, gen, tdt)
+    rng = np.random.default_rng(size)
+    rows = np.sort(rng.choice(m, 32, replace=False))
+    cols = np.sort(rng.choice(n, 32, replace=False))
+    ti = torch.from_numpy(rows).cuda()
+    tj = torch.from_numpy(cols).cuda()
+    As = np.asfortranarray(_op_rows(A, ta, ti, k))            # 32 x k: rows of op(A)
+    Bs = np.asfortranarray(_op_rows(B, "T" if tb == "N" else "N", tj, k).T)  # k x 32: columns of op(B)
+    Cs = np.asfortranarray(C0[tj][:, ti].T.double().cpu().numpy())  # C(rows, cols)
+    hi, lo = dd_reference("N", "N", 32, 32, k, 1.5, As, 32, Bs, k, 0.5, Cs, 32)
+    eps = U64 if dtype == "d" else U32
+    bound = gemm_error_bound(As, "N", Bs, "N", 32, 32, k, 1.5, 0.5, Cs, eps)
+    methods = (eb.METHOD_NATIVE, eb.METHOD_CRT, eb.METHOD_EMULATED) if dtype == "d" else (eb.METHOD_NATIVE,
+                                                                                          eb.METHOD_EMULATED)
+    errs = {}
+    for method in methods:
+        (eb.set_dgemm_method if dtype == "d" else eb.set_sgemm_method)(method)
+        C = C0.clone()
+        (eb.dgemm if dtype == "d" else eb.sgemm)(ta, tb, m, n, k, 1.5, A, lda, B, ldb, 0.5, C, ldc)
+        torch.cuda.synchronize()
+        assert eb.last_error()[0] == eb.EB2_OK, eb.last_error()
+        blk = C[tj][:, ti].T.double().cpu().numpy()
+        assert np.all(np.abs(blk - hi) <= bound), method
+        errs[method] = np.linalg.norm((blk - hi) - lo)
+        assert torch.equal(C[:, m:], C0[:, m:])  # padding rows of C untouched
+        del C
+    limit = 1.5 if dtype == "d" else 4.0
+    for method in methods[1:]:
+        assert errs[method] <= limit * errs[eb.METHOD_NATIVE] + 1e-300, errs
