@@ -404,6 +404,25 @@ def grouped_bench(eb, torch, dev, stream, steps, warmup, count=10000, seed=7):
     return res
 
 
+def grouped_cpu_reference(count=10000):
+    """The reference's CPU path for the same batch law (oracle/_ref/eigen_ref_bench --mode batch):
+    an OpenMP parallel for over the products on all host threads, each C = A * B through Eigen's
+    operator*, with fixed-size Matrix<Scalar,N,N> types (unrolled coefficient-based products)
+    for the products drawn from {3,4,6,8}; median of 3 repetitions after a warm-up."""
+    out = {}
+    for dtype, key in (("d", "fp64"), ("s", "fp32")):
+        res, err = run_ref_bench(["--mode", "batch", "--dtype", dtype, "--count", str(count), "--reps", "3",
+                                  "--warmup", "1", "--max-seconds", "20"])
+        if res is None:
+            out[key] = {"error": err}
+            continue
+        out[key] = {"gflops": round(res["gflops"], 2), "ms": round(res["seconds_median"] * 1e3, 3),
+                    "threads": res["threads"], "problems": res["count"],
+                    "sample": "same size law (m, n, k log-uniform in [3, 256], 20% from {3,4,6,8} cubes), "
+                              "its own seeded draw; Eigen operator* per product, OpenMP over products"}
+    return out
+
+
 # ------------------------------------------------------------------------ accuracy
 def _exact_block(Ar, Bc):
     """alpha*A*B on a sampled block, rounded once from the exact sum: every product a*b is
@@ -705,6 +724,8 @@ def our_arm(a, world, rank, local):
     grouped = None
     if not a.no_grouped:
         grouped = grouped_bench(eb, torch, dev, stream, a.steps, a.warmup)
+        if rank == 0 and world == 1 and not a.no_cpu_baseline:
+            grouped["cpu"] = grouped_cpu_reference()
 
     level3 = None
     if not a.no_level3:

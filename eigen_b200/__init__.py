@@ -124,6 +124,7 @@ def load(path: str | os.PathLike | None = None, mode: int = ctypes.RTLD_GLOBAL) 
     lib.eb2_grouped_plan_destroy.argtypes = [ctypes.c_void_p]
     lib.eb2_gemm_grouped.argtypes = [ctypes.c_char, ctypes.c_int64, pp, ctypes.c_void_p]
     lib.eb2_gemm_each.argtypes = [ctypes.c_char, ctypes.c_int64, pp, ctypes.c_void_p]
+    lib.eb2_set_grouped_classes.argtypes = [ctypes.c_int, ctypes.c_int]
     fp = ctypes.POINTER(ctypes.c_float)
     ip = ctypes.POINTER(ctypes.c_int)
     lib.eb2_picker_set_weights.argtypes = [vp, ctypes.c_int]
@@ -375,8 +376,13 @@ def gemm_grouped(dtype: str, problems, stream=0) -> int:
     return load().eb2_gemm_grouped(dtype.encode(), len(arr), arr, stream or None)
 
 
+def set_grouped_classes(small_max: int = 8, mid_max: int = 16) -> int:
+    """Size classes of later grouped plans (eb2_set_grouped_classes)."""
+    return load().eb2_set_grouped_classes(small_max, mid_max)
+
+
 def gemm_each(dtype: str, problems, stream=0) -> int:
-    """One plain native launch per product (the per-call baseline of the grouped path)."""
+    """One launch per product of the same arithmetic (the per-call baseline of the grouped path)."""
     arr = problems if isinstance(problems, ctypes.Array) else problems_array(problems)
     return load().eb2_gemm_each(dtype.encode(), len(arr), arr, stream or None)
 

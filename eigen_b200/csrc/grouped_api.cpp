@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <vector>
 
 #include "context.h"
@@ -16,7 +17,6 @@ struct eb2_grouped_plan {
   int64_t count = 0, num_items = 0;
   eb2::GroupedProblem* d_problems = nullptr;
   eb2::GroupedItem* d_items = nullptr;
-  unsigned long long* d_counter = nullptr;
   cudaStream_t capture_stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -38,7 +38,6 @@ void release(eb2_grouped_plan* p) {
   if (p->capture_stream) cudaStreamDestroy(p->capture_stream);
   if (p->d_problems) cudaFree(p->d_problems);
   if (p->d_items) cudaFree(p->d_items);
-  if (p->d_counter) cudaFree(p->d_counter);
   delete p;
 }
 
@@ -49,11 +48,15 @@ bool cuda_ok(cudaError_t e, const char* what) {
   return false;
 }
 
-// Validates and converts the problems; builds the work items in schedule order.
+// Validates and converts the problems; builds the work items in schedule order: products of
+// at most small_max x small_max four to a warp, of at most mid_max two to a warp (each group
+// of similar K), larger ones cut into 32 x 32 tiles; then all items longest-K first.
 int build(char dtype, int64_t count, const eb2_gemm_problem* ps, std::vector<GroupedProblem>& out,
           std::vector<GroupedItem>& items) {
   out.resize(size_t(count));
   std::vector<std::pair<int64_t, GroupedItem>> keyed;
+  std::vector<std::pair<int64_t, uint32_t>> small, mid;  // (k, problem) of the shared-warp classes
+  const GroupedClasses cls = grouped_classes();
   for (int64_t i = 0; i < count; ++i) {
     const eb2_gemm_problem& q = ps[i];
     const int oa = op_code(q.transa), ob = op_code(q.transb);
@@ -92,11 +95,40 @@ int build(char dtype, int64_t count, const eb2_gemm_problem* ps, std::vector<Gro
     g.pad_ = 0;
     if (q.m == 0 || q.n == 0) continue;
     if (g.k == 0 && q.beta == 1.0) continue;  // nothing to do
-    const int tm = int((q.m + 31) / 32), tn = int((q.n + 31) / 32);
-    for (int a = 0; a < tm; ++a)
-      for (int b = 0; b < tn; ++b)
-        keyed.push_back({g.k, GroupedItem{uint32_t(i), uint16_t(a), uint16_t(b)}});
+    const int64_t side = std::max(q.m, q.n);
+    if (side <= cls.small_max) {
+      small.push_back({g.k, uint32_t(i)});
+    } else if (side <= cls.mid_max) {
+      mid.push_back({g.k, uint32_t(i)});
+    } else {
+      const int tm = int((q.m + 31) / 32), tn = int((q.n + 31) / 32);
+      for (int a = 0; a < tn; ++a)
+        for (int b = 0; b < tm; ++b) {
+          GroupedItem it{};
+          it.problem[0] = uint32_t(i);
+          it.problem[1] = it.problem[2] = it.problem[3] = kNoProblem;
+          it.k = int32_t(std::min<int64_t>(g.k, INT32_MAX));
+          it.tile_m = uint16_t(b);
+          it.tile_n = uint16_t(a);
+          it.cls = 32;
+          keyed.push_back({g.k, it});
+        }
+    }
   }
+  // products that share a warp: similar K together (each item walks its largest K)
+  auto pack = [&](std::vector<std::pair<int64_t, uint32_t>>& v, int per_item, uint8_t c) {
+    std::stable_sort(v.begin(), v.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    for (size_t s = 0; s < v.size(); s += size_t(per_item)) {
+      GroupedItem it{};
+      for (int q = 0; q < 4; ++q) it.problem[q] = kNoProblem;
+      for (int q = 0; q < per_item && s + size_t(q) < v.size(); ++q) it.problem[q] = v[s + size_t(q)].second;
+      it.k = int32_t(std::min<int64_t>(v[s].first, INT32_MAX));
+      it.cls = c;
+      keyed.push_back({v[s].first, it});
+    }
+  };
+  pack(small, 4, 8);
+  pack(mid, 2, 16);
   // longest K first: a greedy balance of the uneven work over the persistent warps
   std::stable_sort(keyed.begin(), keyed.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
   items.resize(keyed.size());
@@ -105,6 +137,12 @@ int build(char dtype, int64_t count, const eb2_gemm_problem* ps, std::vector<Gro
 }
 
 }  // namespace
+
+GroupedClasses& grouped_classes() {
+  static GroupedClasses c;
+  return c;
+}
+
 }  // namespace eb2
 
 extern "C" {
@@ -130,7 +168,6 @@ int eb2_grouped_plan_create(char dtype, int64_t count, const eb2_gemm_problem* p
                          "grouped descriptors");
   ok = ok && eb2::cuda_ok(cudaMalloc(&p->d_items, std::max<size_t>(1, items.size()) * sizeof(eb2::GroupedItem)),
                           "grouped schedule");
-  ok = ok && eb2::cuda_ok(cudaMalloc(&p->d_counter, sizeof(unsigned long long)), "grouped counter");
   ok = ok && eb2::cuda_ok(cudaStreamCreateWithFlags(&p->capture_stream, cudaStreamNonBlocking), "capture stream");
   if (ok && !ps.empty())
     ok = eb2::cuda_ok(cudaMemcpy(p->d_problems, ps.data(), ps.size() * sizeof(eb2::GroupedProblem),
@@ -140,11 +177,13 @@ int eb2_grouped_plan_create(char dtype, int64_t count, const eb2_gemm_problem* p
     ok = eb2::cuda_ok(cudaMemcpy(p->d_items, items.data(), items.size() * sizeof(eb2::GroupedItem),
                                  cudaMemcpyHostToDevice),
                       "upload schedule");
+  unsigned blocks = 0;
+  ok = ok && eb2::cuda_ok(eb2::grouped_grid(p->f64, p->num_items, cx->num_sms, &blocks), "grouped grid");
   if (ok) {
     ok = eb2::cuda_ok(cudaStreamBeginCapture(p->capture_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     if (ok) {
-      cudaError_t le = eb2::launch_grouped_gemm(p->f64, p->d_problems, p->d_items, p->num_items, p->d_counter,
-                                               cx->num_sms, p->capture_stream);
+      cudaError_t le = eb2::launch_grouped_gemm(p->f64, p->d_problems, p->d_items, p->num_items, blocks,
+                                               p->capture_stream);
       cudaError_t ee = cudaStreamEndCapture(p->capture_stream, &p->graph);
       ok = eb2::cuda_ok(le, "grouped launch (capture)") && eb2::cuda_ok(ee, "end capture");
     }
@@ -210,6 +249,8 @@ int eb2_gemm_each(char dtype, int64_t count, const eb2_gemm_problem* problems, v
     const bool ta = eb2::op_code(q.transa) != 0, tb = eb2::op_code(q.transb) != 0;
     cudaError_t e;
     if (dtype == 'd') {
+      // the FP64 kernel of the grouped launch walks K in the native kernel's order: the plain
+      // native DGEMM gives the same bits
       if (q.k == 0 || q.alpha == 0.0)
         e = q.beta == 1.0 ? cudaSuccess : eb2::launch_scale_matrix_d(q.m, q.n, q.beta, static_cast<double*>(q.c), q.ldc, st);
       else
@@ -217,16 +258,22 @@ int eb2_gemm_each(char dtype, int64_t count, const eb2_gemm_problem* problems, v
                                      static_cast<const double*>(q.b), q.ldb, q.beta, static_cast<double*>(q.c), q.ldc,
                                      nullptr, st);
     } else {
-      const float al = float(q.alpha), be = float(q.beta);
-      if (q.k == 0 || al == 0.0f)
-        e = be == 1.0f ? cudaSuccess : eb2::launch_scale_matrix_s(q.m, q.n, be, static_cast<float*>(q.c), q.ldc, st);
-      else
-        e = eb2::launch_sgemm_native(ta, tb, q.m, q.n, q.k, al, static_cast<const float*>(q.a), q.lda,
-                                     static_cast<const float*>(q.b), q.ldb, be, static_cast<float*>(q.c), q.ldc,
-                                     nullptr, st);
+      // FP32: the split-BF16 tile arithmetic of the grouped launch, one launch per product
+      const eb2::GroupedProblem& g = ps[size_t(i)];
+      e = (g.k == 0 && g.beta == 1.0) ? cudaSuccess : eb2::launch_grouped_one(false, g, st);
     }
     if (!eb2::cuda_ok(e, "per-product launch")) return EB2_ERR_CUDA;
   }
+  return EB2_OK;
+}
+
+int eb2_set_grouped_classes(int small_max, int mid_max) {
+  if (small_max < 0 || small_max > 8 || mid_max < 0 || mid_max > 16) {
+    eb2::set_error(EB2_ERR_ARG, "eb2_set_grouped_classes: small_max in [0, 8], mid_max in [0, 16]");
+    return EB2_ERR_ARG;
+  }
+  eb2::grouped_classes().small_max = small_max;
+  eb2::grouped_classes().mid_max = mid_max;
   return EB2_OK;
 }
 

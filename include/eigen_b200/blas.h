@@ -326,9 +326,13 @@ int eb2_dgemm_device_noalloc(char transa, char transb, int64_t m, int64_t n, int
  * Thousands of independent products C_i = alpha_i*op(A_i)op(B_i) + beta_i*C_i (device
  * pointers, column-major) in ONE persistent launch.  Eigen has no batch entry point;
  * this is the batched counterpart of its fixed-size coefficient-based products
- * (Eigen/src/Core/GeneralProduct.h:76-80) and of per-product GEMM calls.  The math is
- * native FP64 (DMMA) for dtype 'd' and FP32 (FFMA) for 's', i.e. the same accuracy class
- * as one plain call per product. */
+ * (Eigen/src/Core/GeneralProduct.h:76-80) and of per-product GEMM calls.  Products of at
+ * most 8 x 8 share a warp four at a time, of at most 16 x 16 two at a time; larger ones are
+ * cut into 32 x 32 tiles.  The math is native FP64 (DMMA, the native DGEMM's order, so each
+ * product equals a plain native dgemm bit for bit) for dtype 'd', and split-BF16 on the
+ * tensor cores for 's' (x = h + m + l in bf16 pieces, six piece products per 16-deep chunk
+ * with FP32 accumulation, chunk sums added in FP32 with round-to-nearest): at least the
+ * accuracy of an FP32 FMA loop. */
 typedef struct eb2_gemm_problem {
   char transa, transb;   /* 'N', 'T' or 'C' */
   int64_t m, n, k;
@@ -353,10 +357,17 @@ int eb2_grouped_plan_destroy(eb2_grouped_plan_t plan);
 /* One-shot: plan, launch on `stream`, wait, release. */
 int eb2_gemm_grouped(char dtype, int64_t count, const eb2_gemm_problem* problems, void* stream);
 
-/* The same products as separate plain launches of the native kernels, one per product,
- * stream-ordered: what a caller looping over dgemm_/sgemm_ gets, without the host
- * synchronisation.  The baseline the grouped launch is measured against. */
+/* The same products as separate launches, one per product, of the same arithmetic (dtype
+ * 'd': the native DGEMM kernel; 's': the grouped split-BF16 tile code on that product alone),
+ * stream-ordered: what a caller looping over per-product calls gets, without the host
+ * synchronisation.  The baseline the grouped launch is measured against; same bits. */
 int eb2_gemm_each(char dtype, int64_t count, const eb2_gemm_problem* problems, void* stream);
+
+/* Size classes of later plans (process-wide): products with max(m, n) <= small_max go four
+ * to a warp, those <= mid_max two to a warp, the rest as 32 x 32 tiles.  small_max in
+ * [0, 8], mid_max in [0, 16]; 0 disables a class.  Defaults 8 and 16.  The tuner times the
+ * alternatives.  No counterpart in the reference. */
+int eb2_set_grouped_classes(int small_max, int mid_max);
 
 /* ---------------------------------------------------------------- learned picker
  * A 3-layer MLP (8 features -> 64 -> 64 -> 11, ReLU, FP32) that plays the role of Eigen's

@@ -1,6 +1,10 @@
 """Grouped (batched) GEMM: one persistent, graph-captured launch for many uneven
-products, checked against the oracle and bit for bit against one plain native call per
-product (same arithmetic, same order)."""
+products, checked against the oracle; FP64 bit for bit against one plain native DGEMM call
+per product (same arithmetic, same order), FP32 (split-BF16 on the tensor cores) bit for bit
+against the per-product launches of the same arithmetic and no less accurate than the FP32
+FFMA kernel.  Small products share a warp (four of at most 8 x 8, two of at most 16 x 16);
+the arithmetic of each output does not depend on that, so every class setting gives the
+same bits."""
 from __future__ import annotations
 
 import numpy as np
@@ -24,6 +28,7 @@ def _defaults():
     yield
     eb.set_dgemm_method(eb.METHOD_AUTO)
     eb.set_sgemm_method(eb.METHOD_AUTO)
+    eb.set_grouped_classes(8, 16)
 
 
 def batch_sizes(count, seed, lo=3, hi=256):
@@ -99,11 +104,11 @@ def test_grouped_matches_oracle_and_plain_calls(dtype):
                                  h["C"], eps)
         assert np.all(np.abs(got[:m, :n] - ref[:m, :n]) <= bound)
         np.testing.assert_array_equal(got[m:, :], h["C"][m:, :])
-        # one plain call of the native kernel gives the same bits
-        plain = h["C"].copy(order="F")
-        f_native(h["transa"], h["transb"], m, n, h["k"], h["alpha"], h["A"], h["lda"], h["B"], h["ldb"], h["beta"],
-                 plain, h["ldc"])
-        np.testing.assert_array_equal(got, plain)
+        if dtype == "d":  # one plain call of the native kernel gives the same bits
+            plain = h["C"].copy(order="F")
+            f_native(h["transa"], h["transb"], m, n, h["k"], h["alpha"], h["A"], h["lda"], h["B"], h["ldb"],
+                     h["beta"], plain, h["ldc"])
+            np.testing.assert_array_equal(got, plain)
 
 
 def test_grouped_plan_replays_and_accumulates():
@@ -162,3 +167,44 @@ def test_gemm_each_equals_grouped(dtype):
     torch.cuda.synchronize()
     for (a1, b1, c1), (a2, b2, c2) in zip(dev1, dev2):
         assert torch.equal(c1, c2)
+
+
+@pytest.mark.parametrize("dtype", ["d", "s"])
+def test_grouped_classes_give_the_same_bits(dtype):
+    """Four products of <= 8 x 8 per warp, two of <= 16 x 16, or every product as 32 x 32
+    tiles: each output sees the same operations in the same order."""
+    sizes = batch_sizes(200, seed=21, lo=2, hi=40) + [(8, 8, 200), (3, 16, 5), (16, 2, 300), (1, 1, 1), (9, 8, 7)]
+    host = make_batch(sizes, dtype, seed=22)
+    results = []
+    for small, mid in ((8, 16), (0, 0), (8, 0), (0, 16), (4, 12)):
+        assert eb.set_grouped_classes(small, mid) == eb.EB2_OK
+        dev, probs = to_device(host)
+        assert eb.gemm_grouped(dtype, probs) == eb.EB2_OK
+        torch.cuda.synchronize()
+        results.append([back(c) for (_, _, c) in dev])
+    for other in results[1:]:
+        for a, b in zip(results[0], other):
+            np.testing.assert_array_equal(a, b)
+    assert eb.set_grouped_classes(9, 16) == eb.EB2_ERR_ARG
+
+
+def test_grouped_fp32_no_less_accurate_than_ffma():
+    """Normwise error over the batch against the FP64 product of the same FP32 inputs: the
+    split-BF16 grouped result against one FFMA SGEMM call per product."""
+    sizes = batch_sizes(150, seed=31)
+    host = make_batch(sizes, "s", seed=32, mixed=False)
+    dev, probs = to_device(host)
+    assert eb.gemm_grouped("s", probs) == eb.EB2_OK
+    torch.cuda.synchronize()
+    eb.set_sgemm_method(eb.METHOD_NATIVE)
+    err_g = err_f = norm = 0.0
+    for h, (_, _, tC) in zip(host, dev):
+        m, n, k = h["m"], h["n"], h["k"]
+        A64, B64 = h["A"].astype(np.float64), h["B"].astype(np.float64)
+        exact = h["alpha"] * (A64[:m, :k] @ B64[:k, :n])
+        ffma = h["C"].copy(order="F")
+        eb.sgemm("N", "N", m, n, k, h["alpha"], h["A"], h["lda"], h["B"], h["ldb"], 0.0, ffma, h["ldc"])
+        err_g += float(np.sum((back(tC)[:m, :n] - exact) ** 2))
+        err_f += float(np.sum((ffma[:m, :n] - exact) ** 2))
+        norm += float(np.sum(exact ** 2))
+    assert np.sqrt(err_g / norm) <= np.sqrt(err_f / norm), (np.sqrt(err_g / norm), np.sqrt(err_f / norm))
