@@ -52,6 +52,8 @@ class CallInfo(ctypes.Structure):
         ("gemm_kernel_ms", ctypes.c_double),
         ("launches", ctypes.c_int),
         ("spread", ctypes.c_double),
+        ("config", ctypes.c_int),
+        ("splits", ctypes.c_int),
     ]
 
     def as_dict(self) -> dict:
@@ -129,10 +131,11 @@ def load(path: str | os.PathLike | None = None, mode: int = ctypes.RTLD_GLOBAL) 
     ip = ctypes.POINTER(ctypes.c_int)
     lib.eb2_picker_set_weights.argtypes = [vp, ctypes.c_int]
     lib.eb2_picker_features.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_char, ctypes.c_double,
-                                        ctypes.c_int64, vp]
+                                        ctypes.c_int64, ctypes.c_double, vp]
     lib.eb2_picker_forward_host.argtypes = [vp, vp, vp]
     lib.eb2_picker_predict.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_char, ctypes.c_double,
-                                       ctypes.c_int64, ip, ip]
+                                       ctypes.c_int64, ctypes.c_double, ip, ip]
+    lib.eb2_set_config.argtypes = [ctypes.c_int]
     lib.eb2_mlp_forward.argtypes = [vp, vp, ctypes.c_int, vp, vp]
     lib.eb2_mlp_backward.argtypes = [vp, vp, vp, vp, ctypes.c_int, vp, vp, vp]
     lib.eb2_mlp_adam.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_float, vp]
@@ -295,6 +298,11 @@ def set_slice_tuning(group_m: int, prefetch: int) -> int:
 def set_wait_limit_ns(ns: int) -> int:
     """Wall-time bound (ns) of the tcgen05 GEMM's pipeline waits; 0 = the default (2 s)."""
     return load().eb2_set_wait_limit_ns(int(ns))
+
+
+def set_config(config: int) -> int:
+    """Force a configuration class of the picker's first head (-1: automatic); see blas.h."""
+    return load().eb2_set_config(int(config))
 
 
 def set_picker(weights) -> int:

@@ -12,7 +12,7 @@ namespace eb2 {
 namespace {
 thread_local int t_error = EB2_OK;
 thread_local char t_message[512] = "";
-thread_local eb2_call_info t_info = {0, 0, 0, 0, 0, 0, 0, -1.0, -1.0, -1.0, 0, 0.0};
+thread_local eb2_call_info t_info = {0, 0, 0, 0, 0, 0, 0, -1.0, -1.0, -1.0, 0, 0.0, -1, 1};
 thread_local Context* t_pending = nullptr;
 thread_local bool t_pending_gemm = false;
 

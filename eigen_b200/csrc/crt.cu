@@ -880,6 +880,31 @@ __global__ void __launch_bounds__(256, 4) crt_reconstruct128_kernel(const __grid
   if (EST) crt_reduce_energies(R, e_acc, v_acc);
 }
 
+// Split-K: residue planes (l, s), s = 0 .. splits-1, of modulus l added modulo p_l into
+// plane (l, 0); 16 bytes per thread, one modulus per grid row.
+__global__ void __launch_bounds__(256) crt_merge_splits_kernel(uint8_t* __restrict__ cres, int64_t plane, int splits) {
+  const int l = int(blockIdx.y);
+  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v * 16 >= plane) return;
+  const uint32_t p = uint32_t(crt_modulus(l));
+  uint8_t* base = cres + int64_t(l) * splits * plane + v * 16;
+  uint32_t sum[16];
+  const uint4 first = *reinterpret_cast<const uint4*>(base);
+  const uint32_t w0[4] = {first.x, first.y, first.z, first.w};
+#pragma unroll
+  for (int b = 0; b < 16; ++b) sum[b] = (w0[b >> 2] >> (8 * (b & 3))) & 0xFFu;
+  for (int s = 1; s < splits; ++s) {
+    const uint4 q = *reinterpret_cast<const uint4*>(base + int64_t(s) * plane);
+    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int b = 0; b < 16; ++b) sum[b] += (w[b >> 2] >> (8 * (b & 3))) & 0xFFu;
+  }
+  uint32_t out[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+  for (int b = 0; b < 16; ++b) out[b >> 2] |= (sum[b] % p) << (8 * (b & 3));
+  *reinterpret_cast<uint4*>(base) = make_uint4(out[0], out[1], out[2], out[3]);
+}
+
 template <int N>
 void launch_rec128(bool est, dim3 grid, cudaStream_t stream, const CrtRecParams& R) {
   if (est)
@@ -912,9 +937,13 @@ cudaError_t launch_gemm_config(const CrtOperand& a, const CrtOperand& b, const C
   P.diag_hi = args.moduli - 1;
   P.skip_if_flag = args.skip_if_flag;
   P.status = args.status;
-  P.group_m = tuning().group_m > 0 ? tuning().group_m : P.tiles_m;
+  const int gm = args.group_m > 0 ? args.group_m : tuning().group_m;
+  P.group_m = gm > 0 ? gm : P.tiles_m;
   P.wait_limit_ns = tuning().wait_limit_ns ? tuning().wait_limit_ns : kWaitLimitNs;
   P.crt = 1;
+  P.splits = args.splits > 1 ? args.splits : 1;
+  if (P.splits > 1 && (args.tile_list != nullptr || args.tri_k != 0 || P.splits > P.num_kb))
+    return cudaErrorInvalidValue;
   P.residues = args.cres;
   P.ld_res = args.ld_res;
   P.tile_list = args.tile_list;
@@ -993,6 +1022,16 @@ cudaError_t launch_crt_gemm(const CrtOperand& a, const CrtOperand& b, const CrtG
   if (args.tile_n == kTilePair) return launch_gemm_config<256, 6, true>(a, b, args, stream);
   if (args.tile_n == 256) return launch_gemm_config<256, 4, false>(a, b, args, stream);
   return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_crt_merge_splits(uint8_t* cres, int64_t plane, int moduli, int splits, cudaStream_t stream) {
+  if (splits <= 1) return cudaSuccess;
+  if (moduli < 1 || moduli > kCrtMaxModuli || splits > kCrtMaxSplits || plane % 16 != 0) return cudaErrorInvalidValue;
+  const int64_t vecs = plane / 16;
+  dim3 grid(unsigned((vecs + 255) / 256), unsigned(moduli));
+  if (grid.x == 0) return cudaSuccess;
+  crt_merge_splits_kernel<<<grid, 256, 0, stream>>>(cres, plane, splits);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t stream) {

@@ -20,6 +20,9 @@ namespace eb2 {
 
 namespace {
 
+// The accuracy target of an FP32 product as a picker feature (FP32 unit roundoff).
+constexpr double kSgemmTolFeature = 5.9604644775390625e-08;
+
 // Rows / columns of C covered by one tile of a tile configuration.  The Ozaki GEMM keeps
 // its FP64 accumulator in registers, so its tiles are 128 columns wide (128 and 256
 // select one CTA / a CTA pair); the split-BF16 GEMM uses 128 / 256 wide single-CTA tiles
@@ -81,10 +84,21 @@ int auto_method_rule(int64_t m, int64_t n, int64_t k) {
 int resolve_dgemm_method(int64_t m, int64_t n, int64_t k) {
   const int method = settings().dgemm_method.load();
   if (method != EB2_METHOD_AUTO) return method;
+  const int fc = forced_config();
+  if (fc >= kCfgNative && fc <= kCfgCrtSplitK) return fc == kCfgNative ? EB2_METHOD_NATIVE : EB2_METHOD_CRT;
   int cfg = -1, cls = 0;
-  if (picker_weights() != nullptr && picker_predict(m, n, k, 'd', 0.0, 1, &cfg, &cls))
-    return cfg == 0 ? EB2_METHOD_NATIVE : EB2_METHOD_CRT;
+  if (picker_weights() != nullptr && picker_predict(m, n, k, 'd', 0.0, 1, settings().dgemm_tol.load(), &cfg, &cls))
+    return cfg == kCfgNative ? EB2_METHOD_NATIVE : EB2_METHOD_CRT;
   return auto_method_rule(m, n, k);
+}
+
+int crt_split_rule(const Context& cx, int64_t m_pad, int64_t n_pad, int64_t k_pad, int moduli) {
+  // one-CTA tiles; about two waves of work items over the SMs, each split at least two K blocks
+  const int64_t items = (m_pad / 128) * ((n_pad + 255) / 256) * moduli;
+  const int64_t kb = k_pad / kOzakiKBlock;
+  int64_t s = items > 0 ? (2 * int64_t(cx.num_sms)) / items : 1;
+  s = std::min<int64_t>(s, std::min<int64_t>(kCrtMaxSplits, kb / 2));
+  return int(std::max<int64_t>(s, 1));
 }
 
 int choose_crt_tile(const Context& cx, int64_t m, int64_t n) {
@@ -118,19 +132,35 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
     (void)cudaGetLastError();
     capture = cudaStreamCaptureStatusNone;
   }
-  const bool stage2 =
-      picker_weights() != nullptr && (auto_tile || forced == 0) && capture == cudaStreamCaptureStatusNone;
+  const int fc = forced_config();
+  const bool forced_cfg = fc >= kCfgCrtCta && fc <= kCfgCrtSplitK;
+  const bool stage2 = picker_weights() != nullptr && !forced_cfg && (auto_tile || forced == 0) &&
+                      capture == cudaStreamCaptureStatusNone;
   const int nmax = (check || stage2) ? std::max(nmod, kCrtMaxModuli) : nmod;
   int tile = (opt.tile_n == kTilePair || opt.tile_n == 256) ? opt.tile_n : choose_crt_tile(cx, m, n);
+  int group_m = 0, splits = 1;
   const StridedView<double> va = view_a(ta, A, lda, m, k);
   const StridedView<double> vb = view_bt(tb, B, ldb, n, k);
   // op(B)^T == op(A) (a product A A^T, as in syrk): one scan and one split serve both
   const bool same = m == n && va.ptr == vb.ptr && va.sr == vb.sr && va.sl == vb.sl;
   // rows padded for the pair tile whenever the picker may still choose it
-  const int64_t m_pad = round_up(m, (stage2 || same) ? 256 : crt_tile_rows(tile)),
+  // (a forced pair class switches the tile to a CTA pair below)
+  const bool pair_rows = stage2 || same || (auto_tile && (fc == kCfgCrtPair || fc == kCfgCrtPairGroup));
+  const int64_t m_pad = round_up(m, pair_rows ? 256 : crt_tile_rows(tile)),
                 n_pad = round_up(n, crt_tile_cols(tile)), k_pad = round_up(k, kOzakiKBlock);
   const bool tri = opt.uplo == 1 || opt.uplo == 2;
   const int64_t max_tiles = (m_pad / 128) * (n_pad / 256);
+  // a configuration class: tile shape, raster order, K splits (dense products only)
+  const bool may_split = auto_tile && !tri && opt.tri_operand == 0;
+  auto apply_config = [&](int c) {
+    tile = (c == kCfgCrtPair || c == kCfgCrtPairGroup) ? kTilePair : 256;
+    group_m = (c == kCfgCrtCtaGroup || c == kCfgCrtPairGroup) ? kCfgGroupM : 0;
+    splits = (c == kCfgCrtSplitK && may_split) ? crt_split_rule(cx, m_pad, n_pad, k_pad, nmod) : 1;
+  };
+  if (auto_tile && forced_cfg) apply_config(fc);
+  // planes of the product residues per modulus: the most K splits a decision can still pick
+  const int max_splits =
+      splits > 1 ? splits : ((stage2 && may_split) ? crt_split_rule(cx, m_pad, n_pad, k_pad, kCrtMinModuli) : 1);
   size_t off = 0;
   const size_t o_mb_a = off;
   off = align256(off + size_t(m) * 8);
@@ -154,7 +184,7 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   const size_t o_res_b = off;
   off = align256(off + size_t(nmax) * n_pad * k_pad);
   const size_t o_res_c = off;
-  off = align256(off + size_t(nmax) * m_pad * n_pad);
+  off = align256(off + size_t(nmax) * max_splits * m_pad * n_pad);
   // triangle only: the tile list, and the non-finite fallback's full product
   const size_t o_tiles = off;
   off = align256(off + (tri ? size_t(max_tiles) * 4 : 0));
@@ -202,11 +232,14 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
       return EB2_ERR_CUDA;
     const double spread = cx.hflags->spread[1] > 0 ? cx.hflags->spread[0] / cx.hflags->spread[1] : 0.0;
     int cfg = -1, cls = 0;
-    if (picker_predict(m, n, k, 'd', spread, 1, &cfg, &cls)) {
-      // DGEMM configurations: 1 = one CTA per 128 x 256 tile, 2 = CTA pair per 256 x 256 tile;
-      // precision class c -> 8 + 2c moduli
-      if (auto_tile && (cfg == 1 || cfg == 2)) tile = cfg == 1 ? 256 : kTilePair;
-      if (forced == 0) nmod = std::min(kCrtMaxModuli, std::max(8, 8 + 2 * (cls - kMlpSliceBase)));
+    if (picker_predict(m, n, k, 'd', spread, 1, opt.tol > 0 ? opt.tol : settings().dgemm_tol.load(), &cfg, &cls)) {
+      // precision class c -> 8 + 2c moduli; then the configuration class (the split rule needs
+      // the modulus count)
+      if (forced == 0) nmod = std::min(kCrtMaxModuli, std::max(kCrtMinModuli, 8 + 2 * (cls - kMlpSliceBase)));
+      if (auto_tile && cfg >= kCfgCrtCta && cfg <= kCfgCrtSplitK) {
+        apply_config(cfg);
+        splits = std::min(splits, max_splits);
+      }
     }
   }
 
@@ -220,6 +253,8 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   g.cres = ws + o_res_c;
   g.ld_res = m_pad;
   g.tri_k = opt.tri_operand;
+  g.group_m = group_m;
+  g.splits = splits;
   if (tri) {
     // the tiles meeting the triangle, in the kernel's raster order
     std::vector<int> tiles(static_cast<size_t>(max_tiles));
@@ -241,7 +276,7 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   r.ldc = ldc;
   r.cres = ws + o_res_c;
   r.ld_res = m_pad;
-  r.plane = m_pad * n_pad;
+  r.plane = int64_t(splits) * m_pad * n_pad;  // the merged residues of modulus l: plane l*splits
   r.mu_a = oa.mu;
   r.mu_b = ob.mu;
   r.err_sq = df->err_sq;
@@ -258,6 +293,10 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
     if (first && opt.timed) cudaEventRecord(cx.ev_gemm0, st);
     good = good && check_cuda(launch_crt_gemm(oa, ob, g, st), "CRT GEMM");
     if (first && opt.timed) cudaEventRecord(cx.ev_gemm1, st);
+    if (splits > 1) {
+      good = good && check_cuda(launch_crt_merge_splits(g.cres, m_pad * n_pad, nmod, splits, st), "merge K splits");
+      info.launches += 1;
+    }
     good = good && check_cuda(launch_crt_reconstruct(r, st), "CRT reconstruction");
     info.launches += 2;
     return good;
@@ -282,6 +321,10 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   if (!ok) return EB2_ERR_CUDA;
   info.slices = nmod;
   info.tile_n = tile;
+  info.splits = splits;
+  info.config = splits > 1 ? kCfgCrtSplitK
+                           : (tile == kTilePair ? (group_m ? kCfgCrtPairGroup : kCfgCrtPair)
+                                                : (group_m ? kCfgCrtCtaGroup : kCfgCrtCta));
   auto finish_timing = [&](bool gemm_timed) {
     if (opt.timed) {
       cudaEventRecord(cx.ev_stop, st);
@@ -356,6 +399,8 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   info.gemm_kernel_ms = -1.0;
   info.launches = 0;
   info.spread = 0.0;
+  info.config = -1;
+  info.splits = 1;
   set_pending_timing(nullptr, false);
   if (m == 0 || n == 0) return EB2_OK;
   if (opt.uplo != 0 && (m != n || opt.method != EB2_METHOD_CRT || k == 0 || alpha == 0.0)) {
@@ -369,20 +414,26 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
     return check_cuda(launch_scale_matrix_d(m, n, beta, C, ldc, st), "scale C") ? EB2_OK : EB2_ERR_CUDA;
   }
   int method = opt.method ? opt.method : settings().dgemm_method.load();
-  // The learned picker decides what is left automatic: method (when AUTO), tile
-  // configuration and slice count.  Stage 1 uses the shape only.
-  const bool auto_method = (method == EB2_METHOD_AUTO);
-  const bool auto_tile = !opt.tile_n && settings().tile_n.load() == 0;
-  const bool auto_slices = !opt.slices && settings().dgemm_slices.load() == 0;
-  const bool use_picker = picker_weights() != nullptr && (auto_method || auto_tile || auto_slices);
-  int pick_cfg = -1, pick_s = 0;
-  if (use_picker && picker_predict(m, n, k, 'd', 0.0, 1, &pick_cfg, &pick_s) && auto_method && pick_cfg == 0)
-    method = EB2_METHOD_NATIVE;
-  if (method == EB2_METHOD_AUTO) method = use_picker ? EB2_METHOD_CRT : auto_method_rule(m, n, k);
+  // What is left automatic is decided by a forced configuration class (the tuner), else the
+  // learned picker, else the size rule.  Stage 1 here uses the shape only; the CRT path
+  // consults the picker again once the scan has measured the data.
+  if (method == EB2_METHOD_AUTO) {
+    const int fc = forced_config();
+    int pick_cfg = -1, pick_s = 0;
+    if (fc >= kCfgNative && fc <= kCfgCrtSplitK)
+      method = fc == kCfgNative ? EB2_METHOD_NATIVE : EB2_METHOD_CRT;
+    else if (picker_weights() != nullptr &&
+             picker_predict(m, n, k, 'd', 0.0, 1, opt.tol > 0 ? opt.tol : settings().dgemm_tol.load(), &pick_cfg,
+                            &pick_s))
+      method = pick_cfg == kCfgNative ? EB2_METHOD_NATIVE : EB2_METHOD_CRT;
+    else
+      method = auto_method_rule(m, n, k);
+  }
   info.method = method;
 
   auto run_native = [&](bool from_auto) -> int {
     info.method = EB2_METHOD_NATIVE;
+    info.config = kCfgNative;
     if (opt.timed && !from_auto) cudaEventRecord(cx.ev_start, st);
     if (opt.timed) cudaEventRecord(cx.ev_gemm0, st);
     if (!check_cuda(launch_dgemm_native(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, st),
@@ -407,8 +458,8 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   // exponents and digit panels, sized for the largest tile padding and slice count the
   // decision can pick.
   const bool check = opt.check_accuracy;
-  const int s_fixed = opt.slices ? opt.slices : (auto_slices ? 0 : choose_slices(m, n, k));
-  const int smax = (use_picker && s_fixed == 0) || check ? kOzakiMaxSlices : std::max(s_fixed, 8);
+  const int s_fixed = opt.slices ? opt.slices : choose_slices(m, n, k);
+  const int smax = check ? kOzakiMaxSlices : std::max(s_fixed, 8);
   const int64_t m_cap = round_up(m, 256), n_cap = round_up(n, 256), k_pad = round_up(k, kOzakiKBlock);
   size_t off = 0;
   const size_t o_mb_a = off;
@@ -441,21 +492,10 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   if (!ok) return EB2_ERR_CUDA;
   info.launches = 2;
 
-  // Stage 2: with the inputs' exponent spread known, pick tile and slices.
-  int tile_n = opt.tile_n ? opt.tile_n : choose_tile_n(cx, m, n, true);
-  int s = s_fixed ? s_fixed : choose_slices(m, n, k);
-  if (use_picker) {
-    if (!check_cuda(cudaMemcpyAsync(cx.hflags, df, sizeof(DeviceFlags), cudaMemcpyDeviceToHost, st), "read scan") ||
-        !check_cuda(cudaStreamSynchronize(st), "scan"))
-      return EB2_ERR_CUDA;
-    const double spread = cx.hflags->spread[1] > 0 ? cx.hflags->spread[0] / cx.hflags->spread[1] : 0.0;
-    info.spread = spread;
-    if (picker_predict(m, n, k, 'd', spread, 1, &pick_cfg, &pick_s)) {
-      if (auto_method && pick_cfg == 0 && !cx.hflags->nonfinite) return run_native(true);
-      if (auto_tile && pick_cfg > 0) tile_n = pick_cfg == 1 ? 128 : (pick_cfg == 2 ? 256 : kTilePair);
-      if (auto_slices) s = std::min(pick_s, smax);
-    }
-  }
+  // The digit-slice form is an explicit method: tile and starting digit count from the size
+  // rules (the picker's precision head counts CRT moduli); the a-posteriori check adds digits.
+  const int tile_n = opt.tile_n ? opt.tile_n : choose_tile_n(cx, m, n, true);
+  int s = s_fixed;
   const int64_t m_pad = round_up(m, tile_m_of(tile_n, true)), n_pad = round_up(n, tile_n_of(tile_n, true));
   oa.rows_pad = m_pad;
   ob.rows_pad = n_pad;
@@ -555,6 +595,8 @@ int sgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   info.kernel_ms = -1.0;
   info.gemm_kernel_ms = -1.0;
   info.launches = 0;
+  info.config = -1;
+  info.splits = 1;
   set_pending_timing(nullptr, false);
   if (m == 0 || n == 0) return EB2_OK;
   if (k == 0 || alpha == 0.0f) {
@@ -564,10 +606,22 @@ int sgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
     return check_cuda(launch_scale_matrix_s(m, n, beta, C, ldc, st), "scale C") ? EB2_OK : EB2_ERR_CUDA;
   }
   int method = opt.method ? opt.method : settings().sgemm_method.load();
-  if (method == EB2_METHOD_AUTO) method = EB2_METHOD_EMULATED;
+  int cfg_tile = 0;  // tile of an automatic split-BF16 choice (0: the size rule)
+  if (method == EB2_METHOD_AUTO) {
+    // a forced configuration class (the tuner), else the learned picker, else split-BF16
+    const int fc = forced_config();
+    int cfg = -1, cls = 0;
+    if (fc >= kCfgSgemmFfma && fc <= kCfgSgemmBf16Pair)
+      cfg = fc;
+    else if (picker_weights() == nullptr || !picker_predict(m, n, k, 's', 0.0, 1, kSgemmTolFeature, &cfg, &cls))
+      cfg = -1;
+    method = cfg == kCfgSgemmFfma ? EB2_METHOD_NATIVE : EB2_METHOD_EMULATED;
+    if (cfg > kCfgSgemmFfma) cfg_tile = cfg == kCfgSgemmBf16_128 ? 128 : (cfg == kCfgSgemmBf16_256 ? 256 : kTilePair);
+  }
   info.method = method;
   if (opt.timed) cudaEventRecord(cx.ev_start, st);
   if (method == EB2_METHOD_NATIVE) {
+    info.config = kCfgSgemmFfma;
     if (opt.timed) cudaEventRecord(cx.ev_gemm0, st);
     if (!check_cuda(launch_sgemm_native(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, st),
                     "native SGEMM"))
@@ -583,7 +637,9 @@ int sgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   }
 
   // ---------------------------------------------------------- split-BF16 emulation
-  const int tile_n = opt.tile_n ? opt.tile_n : choose_tile_n(cx, m, n, false);
+  const int tile_n = opt.tile_n ? opt.tile_n
+                                : (cfg_tile && settings().tile_n.load() == 0 ? cfg_tile : choose_tile_n(cx, m, n, false));
+  info.config = tile_n == 128 ? kCfgSgemmBf16_128 : (tile_n == 256 ? kCfgSgemmBf16_256 : kCfgSgemmBf16Pair);
   const int pieces = opt.pieces ? opt.pieces : settings().sgemm_pieces.load();
   const int64_t m_pad = round_up(m, tile_m_of(tile_n, false)), n_pad = round_up(n, tile_n_of(tile_n, false)),
                 k_pad = round_up(k, 64);

@@ -34,6 +34,9 @@ struct SgemmOptions {
 int choose_tile_n(const Context& cx, int64_t m, int64_t n, bool ozaki);
 int choose_slices(int64_t m, int64_t n, int64_t k);
 int choose_crt_tile(const Context& cx, int64_t m, int64_t n);
+// K splits of the CRT GEMM's split-K configuration (one-CTA tiles): about two waves of work
+// items over the SMs, each split at least two K blocks, at most kCrtMaxSplits.
+int crt_split_rule(const Context& cx, int64_t m_pad, int64_t n_pad, int64_t k_pad, int moduli);
 // DGEMM method without a per-call override: the settings, else the learned picker on the
 // shape, else the size rule (auto_method_rule).
 int resolve_dgemm_method(int64_t m, int64_t n, int64_t k);

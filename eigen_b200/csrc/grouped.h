@@ -51,6 +51,7 @@ size_t grouped_block_smem(bool f64);
 struct GroupedClasses {
   int small_max = 8;
   int mid_max = 16;
+  bool automatic = true;  // not set by the caller: a forced configuration class or the picker decides
 };
 GroupedClasses& grouped_classes();
 

@@ -4,12 +4,14 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <vector>
 
 #include "context.h"
 #include "eigen_b200/blas.h"
 #include "grouped.h"
 #include "kernels.h"
+#include "mlp.h"
 
 struct eb2_grouped_plan {
   int device = -1;
@@ -48,6 +50,37 @@ bool cuda_ok(cudaError_t e, const char* what) {
   return false;
 }
 
+// The size classes of a plan: the caller's setting, else a forced configuration class (the
+// tuner), else the learned picker on the batch's geometric-mean shape and count, else 8 / 16.
+GroupedClasses resolve_classes(char dtype, int64_t count, const eb2_gemm_problem* ps) {
+  GroupedClasses c = grouped_classes();
+  if (!c.automatic) return c;
+  c.small_max = 8;
+  c.mid_max = 16;
+  int cfg = forced_config();
+  if (cfg != kCfgBatchClasses && cfg != kCfgBatchTiles) {
+    cfg = -1;
+    if (picker_weights() != nullptr && count > 1) {
+      double lm = 0, ln = 0, lk = 0;
+      int64_t used = 0;
+      for (int64_t i = 0; i < count; ++i) {
+        if (ps[i].m <= 0 || ps[i].n <= 0) continue;
+        lm += std::log(double(ps[i].m));
+        ln += std::log(double(ps[i].n));
+        lk += std::log(double(std::max<int64_t>(ps[i].k, 1)));
+        ++used;
+      }
+      int cls = 0;
+      if (used > 0)
+        (void)picker_predict(int64_t(std::llround(std::exp(lm / used))), int64_t(std::llround(std::exp(ln / used))),
+                             int64_t(std::llround(std::exp(lk / used))), dtype, 0.0, count,
+                             dtype == 'd' ? 1.1102230246251565e-16 : 5.9604644775390625e-08, &cfg, &cls);
+    }
+  }
+  if (cfg == kCfgBatchTiles) c.small_max = c.mid_max = 0;
+  return c;
+}
+
 // Validates and converts the problems; builds the work items in schedule order: products of
 // at most small_max x small_max four to a warp, of at most mid_max two to a warp (each group
 // of similar K), larger ones cut into 32 x 32 tiles; then all items longest-K first.
@@ -56,7 +89,7 @@ int build(char dtype, int64_t count, const eb2_gemm_problem* ps, std::vector<Gro
   out.resize(size_t(count));
   std::vector<std::pair<int64_t, GroupedItem>> keyed;
   std::vector<std::pair<int64_t, uint32_t>> small, mid;  // (k, problem) of the shared-warp classes
-  const GroupedClasses cls = grouped_classes();
+  const GroupedClasses cls = resolve_classes(dtype, count, ps);
   for (int64_t i = 0; i < count; ++i) {
     const eb2_gemm_problem& q = ps[i];
     const int oa = op_code(q.transa), ob = op_code(q.transb);
@@ -268,12 +301,17 @@ int eb2_gemm_each(char dtype, int64_t count, const eb2_gemm_problem* problems, v
 }
 
 int eb2_set_grouped_classes(int small_max, int mid_max) {
+  if (small_max == -1 && mid_max == -1) {
+    eb2::grouped_classes() = eb2::GroupedClasses{};
+    return EB2_OK;
+  }
   if (small_max < 0 || small_max > 8 || mid_max < 0 || mid_max > 16) {
-    eb2::set_error(EB2_ERR_ARG, "eb2_set_grouped_classes: small_max in [0, 8], mid_max in [0, 16]");
+    eb2::set_error(EB2_ERR_ARG, "eb2_set_grouped_classes: small_max in [0, 8], mid_max in [0, 16] (or both -1)");
     return EB2_ERR_ARG;
   }
   eb2::grouped_classes().small_max = small_max;
   eb2::grouped_classes().mid_max = mid_max;
+  eb2::grouped_classes().automatic = false;
   return EB2_OK;
 }
 

@@ -89,7 +89,9 @@ cudaError_t launch_ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, cons
 // Moduli of the CRT product: pairwise coprime, <= 256, largest first.
 constexpr int kCrtMaxModuli = 20;
 constexpr int kCrtDefaultModuli = 16;
+constexpr int kCrtMinModuli = 8;  // fewest moduli the picker and the tuner use
 constexpr int kCrtLimbs = 6;  // 192-bit reconstruction arithmetic (32-bit limbs)
+constexpr int kCrtMaxSplits = 16;  // K splits of the CRT GEMM (split residues summed < 2^12)
 constexpr int kCrtZeroRow = -(1 << 20);  // mu of a row without a nonzero finite entry
 // (p - 1 packed one byte each, so device code indexes no local array)
 __host__ __device__ constexpr int crt_modulus(int l) {
@@ -144,8 +146,17 @@ struct CrtGemmArgs {
   int num_listed = 0;
   int tri_k = 0;  // triangular operand whose zero K blocks are skipped: 1/2 = op(A) lower/upper,
                   // 3/4 = op(B) lower/upper (0: dense)
+  // split-K: every (tile, modulus) is computed as `splits` K ranges, each into its own residue
+  // plane: cres is [moduli][splits][n_pad][ld_res], merged by launch_crt_merge_splits (dense
+  // operands, no tile list, splits <= the K blocks).  1: none.
+  int splits = 1;
+  int group_m = 0;  // row tiles per raster group (0: the process-wide tuning)
 };
 cudaError_t launch_crt_gemm(const CrtOperand& a, const CrtOperand& b, const CrtGemmArgs& args, cudaStream_t stream);
+// Adds the `splits` residue planes of every modulus modulo its p into the modulus's first
+// plane (plane = bytes of one plane, a multiple of 16): the layout the reconstruction reads
+// with a plane stride of splits * plane.
+cudaError_t launch_crt_merge_splits(uint8_t* cres, int64_t plane, int moduli, int splits, cudaStream_t stream);
 
 struct CrtReconstructArgs {
   int64_t m, n;

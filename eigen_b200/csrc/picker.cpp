@@ -2,6 +2,7 @@
 // host forward pass of the MLP (the same operations as mlp_forward_kernel, in FP32 with
 // fused multiply-adds), and the process-wide installed weights.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -24,9 +25,11 @@ std::mutex g_mu;
 std::vector<float> g_weights;  // empty: no picker installed
 }  // namespace
 
-void picker_features(int64_t m, int64_t n, int64_t k, char dtype, double spread, int64_t batch, float* out) {
+void picker_features(int64_t m, int64_t n, int64_t k, char dtype, double spread, int64_t batch, double tol,
+                     float* out) {
   const double lm = std::log2(double(m > 0 ? m : 1)), ln = std::log2(double(n > 0 ? n : 1)),
                lk = std::log2(double(k > 0 ? k : 1));
+  const double t = tol > 0.0 && tol < 1.0 ? tol : 1.0;
   out[0] = float(lm / 14.0);
   out[1] = float(ln / 14.0);
   out[2] = float(lk / 14.0);
@@ -34,8 +37,26 @@ void picker_features(int64_t m, int64_t n, int64_t k, char dtype, double spread,
   out[4] = float(spread / 32.0);
   out[5] = float(std::log2(double(batch > 0 ? batch : 1)) / 14.0);
   out[6] = float((lm + ln + lk) / 42.0);
-  out[7] = float(std::log2(std::min(lm, ln) + 1.0) / 4.0);
+  out[7] = float(-std::log2(t) / 64.0);
 }
+
+void picker_config_range(char dtype, int64_t batch, int* lo, int* hi) {
+  if (batch > 1) {
+    *lo = kCfgBatchClasses;
+    *hi = kCfgBatchTiles + 1;
+  } else if (dtype == 's') {
+    *lo = kCfgSgemmFfma;
+    *hi = kCfgSgemmBf16Pair + 1;
+  } else {
+    *lo = kCfgNative;
+    *hi = kCfgCrtSplitK + 1;
+  }
+}
+
+namespace {
+std::atomic<int> g_forced_config{-1};
+}
+int forced_config() { return g_forced_config.load(); }
 
 void picker_forward(const float* w, const float* x, float* logits) {
   constexpr int H = kMlpHidden;
@@ -68,8 +89,8 @@ const float* picker_weights() {
   return g_weights.empty() ? nullptr : g_weights.data();
 }
 
-bool picker_predict(int64_t m, int64_t n, int64_t k, char dtype, double spread, int64_t batch, int* config,
-                    int* slices) {
+bool picker_predict(int64_t m, int64_t n, int64_t k, char dtype, double spread, int64_t batch, double tol,
+                    int* config, int* slices) {
   std::vector<float> w;
   {
     std::lock_guard<std::mutex> lock(g_mu);
@@ -77,10 +98,12 @@ bool picker_predict(int64_t m, int64_t n, int64_t k, char dtype, double spread, 
     w = g_weights;
   }
   float x[kMlpIn], lg[kMlpOut];
-  picker_features(m, n, k, dtype, spread, batch, x);
+  picker_features(m, n, k, dtype, spread, batch, tol, x);
   picker_forward(w.data(), x, lg);
-  int c = 0;
-  for (int j = 1; j < kMlpConfigs; ++j)
+  int lo = 0, hi = 0;
+  picker_config_range(dtype, batch, &lo, &hi);
+  int c = lo;
+  for (int j = lo + 1; j < hi; ++j)
     if (lg[j] > lg[c]) c = j;
   int s = 0;
   for (int j = 1; j < kMlpSlices; ++j)
@@ -148,11 +171,24 @@ int eb2_picker_set_weights(const float* weights, int count) {
   return EB2_OK;
 }
 
-int eb2_picker_features(int64_t m, int64_t n, int64_t k, char dtype, double spread, int64_t batch, float* out) {
+int eb2_picker_features(int64_t m, int64_t n, int64_t k, char dtype, double spread, int64_t batch, double tol,
+                        float* out) {
   if (!out) return EB2_ERR_ARG;
-  eb2::picker_features(m, n, k, dtype, spread, batch, out);
+  eb2::picker_features(m, n, k, dtype, spread, batch, tol, out);
   return EB2_OK;
 }
+
+int eb2_set_config(int config) {
+  if (config < -1 || config >= eb2::kMlpConfigs) {
+    eb2::set_error(EB2_ERR_ARG, "eb2_set_config: %d is not a configuration class (-1 .. %d)", config,
+                   eb2::kMlpConfigs - 1);
+    return EB2_ERR_ARG;
+  }
+  eb2::g_forced_config = config;
+  return EB2_OK;
+}
+
+int eb2_config_count(void) { return eb2::kMlpConfigs; }
 
 int eb2_picker_forward_host(const float* weights, const float* features, float* logits) {
   if (!weights || !features || !logits) return EB2_ERR_ARG;
@@ -160,10 +196,10 @@ int eb2_picker_forward_host(const float* weights, const float* features, float* 
   return EB2_OK;
 }
 
-int eb2_picker_predict(int64_t m, int64_t n, int64_t k, char dtype, double spread, int64_t batch, int* config,
-                       int* slices) {
+int eb2_picker_predict(int64_t m, int64_t n, int64_t k, char dtype, double spread, int64_t batch, double tol,
+                       int* config, int* slices) {
   if (!config || !slices) return EB2_ERR_ARG;
-  return eb2::picker_predict(m, n, k, dtype, spread, batch, config, slices) ? EB2_OK : EB2_ERR_ARG;
+  return eb2::picker_predict(m, n, k, dtype, spread, batch, tol, config, slices) ? EB2_OK : EB2_ERR_ARG;
 }
 
 int eb2_mlp_forward(const float* w, const float* X, int batch, float* logits, void* stream) {

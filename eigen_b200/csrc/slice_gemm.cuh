@@ -94,6 +94,7 @@ struct SliceGemmParams {
   int tri_k;             // CRT: 1 = op(A) lower, 2 = op(A) upper, 3 = op(B) lower, 4 = op(B) upper
                          // triangular (zero blocks of K skipped per tile); 0 = dense
   uint64_t wait_limit_ns;  // wall-time bound of the pipeline waits (the drain waits keep kWaitLimitNs)
+  int splits;            // CRT: K ranges per (tile, modulus), each with its own residue plane (1: none)
 };
 
 // Pair range of diagonal t: p = p_lo .. p_lo + total/num_kb - 1 (q = t - p).
@@ -127,10 +128,18 @@ __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, 
 // blocks have zero residues and add exact zeros, so leaving them out changes no bit.  A tile
 // wholly in the padding keeps one block (its operand rows are zero), so every role walks at
 // least one block per item.
-__device__ __forceinline__ void tile_k_range(const SliceGemmParams& P, int tile, int rows, int cols, int& kb_lo,
-                                             int& kb_hi) {
+//
+// CRT split-K (P.splits > 1, dense operands only): split s of an item walks the K blocks
+// [s num_kb / splits, (s+1) num_kb / splits), a non-empty range since splits <= num_kb.
+__device__ __forceinline__ void tile_k_range(const SliceGemmParams& P, int tile, int split, int rows, int cols,
+                                             int& kb_lo, int& kb_hi) {
   kb_lo = 0;
   kb_hi = P.num_kb;
+  if (P.splits > 1) {
+    kb_lo = int(int64_t(split) * P.num_kb / P.splits);
+    kb_hi = int(int64_t(split + 1) * P.num_kb / P.splits);
+    return;
+  }
   if (P.tri_k == 0) return;
   int tm, tn;
   tile_coords(tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
@@ -144,24 +153,28 @@ __device__ __forceinline__ void tile_k_range(const SliceGemmParams& P, int tile,
   if (kb_hi <= kb_lo) kb_hi = kb_lo + 1;
 }
 
-// Work items: one per output tile, or in CRT mode one per (tile, modulus): the moduli are
-// independent products, so small outputs still spread over the SMs, and the items in
-// flight at any time share one modulus (its residue planes stay in L2).
+// Work items: one per output tile, or in CRT mode one per (tile, K split, modulus): the
+// moduli are independent products, so small outputs still spread over the SMs, and the
+// items in flight at any time share one modulus (its residue planes stay in L2).
 // LISTED: the tiles are P.tile_list[0 .. num_listed) (the triangle of C of a gemmtr / syrk).
 template <bool LISTED>
 __host__ __device__ __forceinline__ int num_work(const SliceGemmParams& P) {
   if (LISTED) return P.num_listed * P.slices;
-  return P.tiles_m * P.tiles_n * (P.crt ? P.slices : 1);
+  return P.tiles_m * P.tiles_n * (P.crt ? P.slices * P.splits : 1);
 }
 template <bool LISTED>
-__device__ __forceinline__ void work_item(const SliceGemmParams& P, int w, int& tile, int& t_hi, int& t_lo) {
+__device__ __forceinline__ void work_item(const SliceGemmParams& P, int w, int& tile, int& t_hi, int& t_lo,
+                                          int& split) {
+  split = 0;
   if (LISTED) {
     tile = P.tile_list[w % P.num_listed];
     t_hi = t_lo = w / P.num_listed;
   } else if (P.crt) {
     const int nt = P.tiles_m * P.tiles_n;
     tile = w % nt;
-    t_hi = t_lo = w / nt;
+    const int r = w / nt;
+    t_hi = t_lo = r / P.splits;
+    split = r % P.splits;
   } else {
     tile = w;
     t_hi = P.diag_hi;
@@ -174,16 +187,16 @@ __device__ __forceinline__ void work_item(const SliceGemmParams& P, int w, int& 
 // producer's per-block path stays as short as the dense one).
 template <bool LISTED, bool CRT>
 struct BlockIter {
-  int work, tile, t, t_lo, f, p_lo, total, stride;
+  int work, tile, t, t_lo, f, p_lo, total, stride, split;
   int rows, cols, kb_lo, kb_hi;  // tile shape; CRT: the item's K blocks
   int kbi, pi;                   // f as (K block, pair offset): f = pi * num_kb + kbi, kept by adds
   bool valid;
   __device__ __forceinline__ void load(const SliceGemmParams& P) {
     int t_hi;
-    work_item<LISTED>(P, work, tile, t_hi, t_lo);
+    work_item<LISTED>(P, work, tile, t_hi, t_lo, split);
     t = t_hi;
     f = kbi = pi = 0;
-    if constexpr (CRT) tile_k_range(P, tile, rows, cols, kb_lo, kb_hi);
+    if constexpr (CRT) tile_k_range(P, tile, split, rows, cols, kb_lo, kb_hi);
   }
   __device__ __forceinline__ void settle(const SliceGemmParams& P, int nwork) {
     valid = false;
@@ -422,14 +435,14 @@ __device__ __forceinline__ void slice_mma(uint8_t* smem, uint64_t* full, uint64_
     // one accumulation unit per diagonal (Ozaki) or modulus (CRT), cut where K exceeds what
     // the INT32 accumulator holds exactly
     for (int w = first_tile<PAIR>(); w < nwork && ok; w += tile_step<PAIR>()) {
-      int tile, t_hi, t_lo;
-      work_item<kListed>(P, w, tile, t_hi, t_lo);
+      int tile, t_hi, t_lo, split;
+      work_item<kListed>(P, w, tile, t_hi, t_lo, split);
       for (int t = t_hi; t >= t_lo && ok; --t) {
         int p_lo, total;
         if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, is_crt_mode(MODE))) continue;
         if constexpr (is_crt_mode(MODE)) {
           int kb_lo, kb_hi;
-          tile_k_range(P, tile, PAIR ? 2 * kSliceBM : kSliceBM, BN, kb_lo, kb_hi);
+          tile_k_range(P, tile, split, PAIR ? 2 * kSliceBM : kSliceBM, BN, kb_lo, kb_hi);
           total = kb_hi - kb_lo;
         }
         constexpr int kUnit = SliceTraits<MODE, BN, PAIR>::kUnitKb;
@@ -595,8 +608,8 @@ __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull
   uint32_t ephase = 0u;
   bool ok = true;
   for (int w = first_tile<PAIR>(); w < nwork && ok; w += tile_step<PAIR>()) {
-    int tile, t_hi, t_lo, tm, tn;
-    work_item<LISTED>(P, w, tile, t_hi, t_lo);
+    int tile, t_hi, t_lo, tm, tn, split;
+    work_item<LISTED>(P, w, tile, t_hi, t_lo, split);
     tile_coords(tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
     const int64_t m0 = int64_t(tm) * (PAIR ? 2 * kSliceBM : kSliceBM) + row_base;
     const int64_t n0 = int64_t(tn) * BN + col_base;
@@ -606,7 +619,7 @@ __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull
       if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, true)) continue;
       {
         int kb_lo, kb_hi;
-        tile_k_range(P, tile, PAIR ? 2 * kSliceBM : kSliceBM, BN, kb_lo, kb_hi);
+        tile_k_range(P, tile, split, PAIR ? 2 * kSliceBM : kSliceBM, BN, kb_lo, kb_hi);
         total = kb_hi - kb_lo;
       }
       const uint32_t pm = uint32_t(crt_modulus(t));
@@ -615,7 +628,7 @@ __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull
       // multiple of p in [2^31 - 2^21, 2^31 - 2^21 + p), v + bias lies in [0, 2^32) and
       // (v + bias) mod p = v mod p: one reduction of an unsigned word, no sign handling
       const uint32_t bias = (0x7FE00000u + pm - 1u) / pm * pm;
-      uint8_t* rp = P.residues + int64_t(t) * plane + grow;
+      uint8_t* rp = P.residues + (int64_t(t) * P.splits + split) * plane + grow;
       for (int u0 = 0; u0 < total && ok; u0 += kMaxUnitKbCrt) {
         if (!mbar_wait(&tfull[buf], (ephase >> buf) & 1u, abort_flag, P.status, P.wait_limit_ns)) {
           ok = false;

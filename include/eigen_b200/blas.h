@@ -276,6 +276,8 @@ typedef struct eb2_call_info {
   int launches;       /* kernels this library launched for the call */
   double spread;      /* emulated DGEMM: mean (largest - mean) binary exponent of 64-entry
                          row chunks of op(A) and op(B)^T, the picker's data feature; else 0 */
+  int config;         /* configuration class of the call (see eb2_set_config), -1 if none */
+  int splits;         /* CRT DGEMM: K ranges per output tile and modulus (1: no split) */
 } eb2_call_info;
 int eb2_last_call_info(eb2_call_info* out);
 
@@ -365,33 +367,47 @@ int eb2_gemm_each(char dtype, int64_t count, const eb2_gemm_problem* problems, v
 
 /* Size classes of later plans (process-wide): products with max(m, n) <= small_max go four
  * to a warp, those <= mid_max two to a warp, the rest as 32 x 32 tiles.  small_max in
- * [0, 8], mid_max in [0, 16]; 0 disables a class.  Defaults 8 and 16.  The tuner times the
- * alternatives.  No counterpart in the reference. */
+ * [0, 8], mid_max in [0, 16]; 0 disables a class.  (-1, -1) restores the automatic choice
+ * (the default): the learned picker decides between 8 / 16 and tiles only, from the batch's
+ * geometric-mean shape and count; without weights 8 / 16.  No counterpart in the reference. */
 int eb2_set_grouped_classes(int small_max, int mid_max);
 
 /* ---------------------------------------------------------------- learned picker
- * A 3-layer MLP (8 features -> 64 -> 64 -> 11, ReLU, FP32) that plays the role of Eigen's
- * computeProductBlockingSizes (Eigen/src/Core/products/GeneralBlockPanelKernel.h:202-452):
- * from log2 m, n, k, the dtype, the inputs' exponent spread and the batch size it scores
- * 4 DGEMM configurations (0 native FP64 kernel, 1 CRT emulation with one CTA per 128x256
- * tile, 2 CRT emulation with a CTA pair per 256x256 tile, 3 digit-slice emulation) and 7
+ * A 3-layer MLP (8 features -> 64 -> 64 -> 19, ReLU, FP32) that plays the role of Eigen's
+ * computeProductBlockingSizes (Eigen/src/Core/products/GeneralBlockPanelKernel.h:202-452).
+ * Features: log2 m, n, k, the dtype, the inputs' exponent spread, log2 of the batch size,
+ * log2 mnk and -log2 of the accuracy target.  Outputs: 12 configuration classes and 7
  * precision classes c (eb2_picker_predict reports 6 + c; the CRT path uses 8 + 2c moduli).
- * DGEMM with an automatic method consults it twice: on the shape (native or emulated) and,
- * once the scan has measured the exponent spread, for the tile and modulus count.  The
- * library loads eigen_b200/data/picker_weights.bin (trained by python -m eigen_b200.tune)
- * when its SM count matches the device.  Weights are a flat float array of
- * eb2_mlp_param_count() entries:
- *   W1[64][8] b1[64] W2[64][64] b2[64] W3[11][64] b3[11]. */
+ * Configuration classes (a prediction takes the best class of its kind):
+ *   DGEMM   0 native FP64 kernel; CRT emulation with 1 one CTA per 128x256 tile, 2 a CTA
+ *           pair per 256x256 tile, 3 / 4 the same with raster groups of 16 row tiles,
+ *           5 one CTA with K split so that the work items fill the SMs;
+ *   SGEMM   6 FP32 FFMA kernel; split-BF16 on 7 128x128, 8 128x256, 9 256x256 (pair) tiles;
+ *   grouped 10 small products share a warp (size classes 8 and 16), 11 32x32 tiles only.
+ * A DGEMM with an automatic method consults it twice: on the shape (native or emulated)
+ * and, once the scan has measured the exponent spread, for the configuration and modulus
+ * count; an SGEMM with an automatic method once; a grouped plan with automatic size
+ * classes once, on the batch's geometric-mean shape and size.  The library loads
+ * eigen_b200/data/picker_weights.bin (trained by python -m eigen_b200.tune) when its SM
+ * count matches the device.  Weights are a flat float array of eb2_mlp_param_count()
+ * entries:  W1[64][8] b1[64] W2[64][64] b2[64] W3[19][64] b3[19]. */
 int eb2_mlp_param_count(void);
 /* Installs the weights the product path consults when method/tile/moduli are automatic
  * (copied; NULL or count 0 removes the picker).  The a-posteriori accuracy check still
  * adds moduli when a prediction falls short. */
 int eb2_picker_set_weights(const float* weights, int count);
-int eb2_picker_features(int64_t m, int64_t n, int64_t k, char dtype, double spread, int64_t batch, float* out8);
-int eb2_picker_forward_host(const float* weights, const float* features8, float* logits11);
-int eb2_picker_predict(int64_t m, int64_t n, int64_t k, char dtype, double spread, int64_t batch, int* config,
-                       int* slices);
-/* Training kernels (device pointers, stream-ordered): forward logits[batch][11];
+int eb2_picker_features(int64_t m, int64_t n, int64_t k, char dtype, double spread, int64_t batch, double tol,
+                        float* out8);
+int eb2_picker_forward_host(const float* weights, const float* features8, float* logits19);
+int eb2_picker_predict(int64_t m, int64_t n, int64_t k, char dtype, double spread, int64_t batch, double tol,
+                       int* config, int* slices);
+/* Forces configuration class `config` (above) for every later call of its kind with an
+ * automatic method -- what the tuner times; -1 restores the picker / the size rules.
+ * Explicit method, tile and size-class settings still win.  No counterpart in the reference. */
+int eb2_set_config(int config);
+/* Number of configuration classes (12). */
+int eb2_config_count(void);
+/* Training kernels (device pointers, stream-ordered): forward logits[batch][19];
  * backward writes the batch-mean gradient (and loss) of the config cross-entropy plus
  * the slice cross-entropy for samples whose slice label is >= 0; Adam step t >= 1. */
 int eb2_mlp_forward(const float* w, const float* X, int batch, float* logits, void* stream);

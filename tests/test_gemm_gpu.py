@@ -243,8 +243,12 @@ def test_device_entry_on_a_torch_stream():
     tB = torch.from_numpy(B.T.copy()).cuda()
     tC = torch.from_numpy(C.T.copy()).cuda()
     torch.cuda.synchronize()
-    rc = eb.dgemm_device("N", "N", m, n, k, 1.0, tA, lda, tB, ldb, 0.0, tC, ldc, stream=s.cuda_stream,
-                         check_accuracy=False)
+    eb.set_dgemm_method(eb.METHOD_CRT)  # the emulated product's accuracy, whatever the picker would choose
+    try:
+        rc = eb.dgemm_device("N", "N", m, n, k, 1.0, tA, lda, tB, ldb, 0.0, tC, ldc, stream=s.cuda_stream,
+                             check_accuracy=False)
+    finally:
+        eb.set_dgemm_method(eb.METHOD_AUTO)
     assert rc == eb.EB2_OK
     s.synchronize()
     Cg = np.asfortranarray(tC.cpu().numpy().T)

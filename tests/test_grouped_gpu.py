@@ -28,7 +28,7 @@ def _defaults():
     yield
     eb.set_dgemm_method(eb.METHOD_AUTO)
     eb.set_sgemm_method(eb.METHOD_AUTO)
-    eb.set_grouped_classes(8, 16)
+    eb.set_grouped_classes(-1, -1)
 
 
 def batch_sizes(count, seed, lo=3, hi=256):
