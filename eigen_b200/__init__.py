@@ -52,8 +52,6 @@ class CallInfo(ctypes.Structure):
         ("gemm_kernel_ms", ctypes.c_double),
         ("launches", ctypes.c_int),
         ("spread", ctypes.c_double),
-        ("config", ctypes.c_int),
-        ("splits", ctypes.c_int),
     ]
 
     def as_dict(self) -> dict:
@@ -338,9 +336,15 @@ def routine_calls(name: str) -> int:
 
 
 def last_call_info() -> dict:
+    """eb2_last_call_info plus eb2_last_call_config (keys "config" and "splits")."""
+    lib = load()
     ci = CallInfo()
-    load().eb2_last_call_info(ctypes.byref(ci))
-    return ci.as_dict()
+    lib.eb2_last_call_info(ctypes.byref(ci))
+    d = ci.as_dict()
+    cfg, splits = ctypes.c_int(), ctypes.c_int()
+    lib.eb2_last_call_config(ctypes.byref(cfg), ctypes.byref(splits))
+    d["config"], d["splits"] = cfg.value, splits.value
+    return d
 
 
 def problems_array(problems) -> "ctypes.Array":

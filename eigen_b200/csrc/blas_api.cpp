@@ -134,6 +134,7 @@ void blas_gemm(char transa, char transb, int64_t m, int64_t n, int64_t k, T alph
   const bool need_ab = (k > 0 && alpha != T(0));
   eb2_call_info& ci = call_info();
   ci = eb2_call_info{};
+  call_config() = CallConfig{};
   cudaStream_t st = cx->stream;
   StreamFence fence(*cx, st);
 
@@ -344,6 +345,7 @@ int eb2_dgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, 
   o.timed = eb2::settings().timing.load() != 0;
   eb2_call_info& ci = eb2::call_info();
   ci = eb2_call_info{};
+  eb2::call_config() = eb2::CallConfig{};
   return eb2::dgemm_on_device(*cx, eb2::op_code(transa) != eb2::kNoTr, eb2::op_code(transb) != eb2::kNoTr, m, n, k,
                               alpha, a, lda, b, ldb, beta, c, ldc, static_cast<cudaStream_t>(stream), o, ci);
 }
@@ -364,6 +366,7 @@ int eb2_sgemm_device(char transa, char transb, int64_t m, int64_t n, int64_t k, 
   o.timed = eb2::settings().timing.load() != 0;
   eb2_call_info& ci = eb2::call_info();
   ci = eb2_call_info{};
+  eb2::call_config() = eb2::CallConfig{};
   return eb2::sgemm_on_device(*cx, eb2::op_code(transa) != eb2::kNoTr, eb2::op_code(transb) != eb2::kNoTr, m, n, k,
                               alpha, a, lda, b, ldb, beta, c, ldc, static_cast<cudaStream_t>(stream), o, ci);
 }

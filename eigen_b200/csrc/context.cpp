@@ -12,7 +12,8 @@ namespace eb2 {
 namespace {
 thread_local int t_error = EB2_OK;
 thread_local char t_message[512] = "";
-thread_local eb2_call_info t_info = {0, 0, 0, 0, 0, 0, 0, -1.0, -1.0, -1.0, 0, 0.0, -1, 1};
+thread_local eb2_call_info t_info = {0, 0, 0, 0, 0, 0, 0, -1.0, -1.0, -1.0, 0, 0.0};
+thread_local CallConfig t_config;
 thread_local Context* t_pending = nullptr;
 thread_local bool t_pending_gemm = false;
 
@@ -42,6 +43,7 @@ void set_error(int code, const char* fmt, ...) {
 int last_error() { return t_error; }
 const char* last_error_string() { return t_message; }
 eb2_call_info& call_info() { return t_info; }
+CallConfig& call_config() { return t_config; }
 
 void set_pending_timing(Context* cx, bool gemm_timed) {
   t_pending = cx;
@@ -219,3 +221,10 @@ Context* context_for_stream(cudaStream_t st) {
 }  // namespace eb2
 
 extern "C" const char* eb2_last_error_string(void) { return eb2::last_error_string(); }
+
+extern "C" int eb2_last_call_config(int* config, int* splits) {
+  if (!config || !splits) return EB2_ERR_ARG;
+  *config = eb2::call_config().config;
+  *splits = eb2::call_config().splits;
+  return EB2_OK;
+}

@@ -115,6 +115,12 @@ void set_error(int code, const char* fmt, ...);
 int last_error();
 const char* last_error_string();
 eb2_call_info& call_info();
+// The configuration class and K splits of the thread's last product (eb2_last_call_config).
+struct CallConfig {
+  int config = -1;
+  int splits = 1;
+};
+CallConfig& call_config();
 // The context whose events hold the calling thread's last timed call (or null);
 // `gemm_timed` tells whether ev_gemm0/ev_gemm1 bracket a kernel in that call.
 void set_pending_timing(Context* cx, bool gemm_timed);

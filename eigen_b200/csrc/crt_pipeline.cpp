@@ -272,8 +272,8 @@ int dgemm_crt_pipelined(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int
   if (!check_cuda(cudaStreamSynchronize(cout), "copy C") || !check_cuda(cudaStreamSynchronize(st), "DGEMM"))
     return EB2_ERR_CUDA;
   info.tile_n = choose_crt_tile(cx, m, nc);
-  info.config = info.tile_n == kTilePair ? kCfgCrtPair : kCfgCrtCta;
-  info.splits = 1;
+  call_config().config = info.tile_n == kTilePair ? kCfgCrtPair : kCfgCrtCta;
+  call_config().splits = 1;
   if (rc_all == EB2_ERR_ACCURACY)
     set_error(EB2_ERR_ACCURACY, "emulated DGEMM estimate above target %.3g in a column block", tol);
   return rc_all;

@@ -321,8 +321,8 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   if (!ok) return EB2_ERR_CUDA;
   info.slices = nmod;
   info.tile_n = tile;
-  info.splits = splits;
-  info.config = splits > 1 ? kCfgCrtSplitK
+  call_config().splits = splits;
+  call_config().config = splits > 1 ? kCfgCrtSplitK
                            : (tile == kTilePair ? (group_m ? kCfgCrtPairGroup : kCfgCrtPair)
                                                 : (group_m ? kCfgCrtCtaGroup : kCfgCrtCta));
   auto finish_timing = [&](bool gemm_timed) {
@@ -399,8 +399,8 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   info.gemm_kernel_ms = -1.0;
   info.launches = 0;
   info.spread = 0.0;
-  info.config = -1;
-  info.splits = 1;
+  call_config().config = -1;
+  call_config().splits = 1;
   set_pending_timing(nullptr, false);
   if (m == 0 || n == 0) return EB2_OK;
   if (opt.uplo != 0 && (m != n || opt.method != EB2_METHOD_CRT || k == 0 || alpha == 0.0)) {
@@ -433,7 +433,7 @@ int dgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
 
   auto run_native = [&](bool from_auto) -> int {
     info.method = EB2_METHOD_NATIVE;
-    info.config = kCfgNative;
+    call_config().config = kCfgNative;
     if (opt.timed && !from_auto) cudaEventRecord(cx.ev_start, st);
     if (opt.timed) cudaEventRecord(cx.ev_gemm0, st);
     if (!check_cuda(launch_dgemm_native(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, st),
@@ -595,8 +595,8 @@ int sgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   info.kernel_ms = -1.0;
   info.gemm_kernel_ms = -1.0;
   info.launches = 0;
-  info.config = -1;
-  info.splits = 1;
+  call_config().config = -1;
+  call_config().splits = 1;
   set_pending_timing(nullptr, false);
   if (m == 0 || n == 0) return EB2_OK;
   if (k == 0 || alpha == 0.0f) {
@@ -621,7 +621,7 @@ int sgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   info.method = method;
   if (opt.timed) cudaEventRecord(cx.ev_start, st);
   if (method == EB2_METHOD_NATIVE) {
-    info.config = kCfgSgemmFfma;
+    call_config().config = kCfgSgemmFfma;
     if (opt.timed) cudaEventRecord(cx.ev_gemm0, st);
     if (!check_cuda(launch_sgemm_native(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, st),
                     "native SGEMM"))
@@ -639,7 +639,7 @@ int sgemm_on_device(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t
   // ---------------------------------------------------------- split-BF16 emulation
   const int tile_n = opt.tile_n ? opt.tile_n
                                 : (cfg_tile && settings().tile_n.load() == 0 ? cfg_tile : choose_tile_n(cx, m, n, false));
-  info.config = tile_n == 128 ? kCfgSgemmBf16_128 : (tile_n == 256 ? kCfgSgemmBf16_256 : kCfgSgemmBf16Pair);
+  call_config().config = tile_n == 128 ? kCfgSgemmBf16_128 : (tile_n == 256 ? kCfgSgemmBf16_256 : kCfgSgemmBf16Pair);
   const int pieces = opt.pieces ? opt.pieces : settings().sgemm_pieces.load();
   const int64_t m_pad = round_up(m, tile_m_of(tile_n, false)), n_pad = round_up(n, tile_n_of(tile_n, false)),
                 k_pad = round_up(k, 64);

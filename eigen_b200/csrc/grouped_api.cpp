@@ -22,6 +22,7 @@ struct eb2_grouped_plan {
   cudaStream_t capture_stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  bool classes_on = true;  // products share warps (size classes), else 32 x 32 tiles only
 };
 
 namespace eb2 {
@@ -85,11 +86,12 @@ GroupedClasses resolve_classes(char dtype, int64_t count, const eb2_gemm_problem
 // at most small_max x small_max four to a warp, of at most mid_max two to a warp (each group
 // of similar K), larger ones cut into 32 x 32 tiles; then all items longest-K first.
 int build(char dtype, int64_t count, const eb2_gemm_problem* ps, std::vector<GroupedProblem>& out,
-          std::vector<GroupedItem>& items) {
+          std::vector<GroupedItem>& items, bool* classes_on = nullptr) {
   out.resize(size_t(count));
   std::vector<std::pair<int64_t, GroupedItem>> keyed;
   std::vector<std::pair<int64_t, uint32_t>> small, mid;  // (k, problem) of the shared-warp classes
   const GroupedClasses cls = resolve_classes(dtype, count, ps);
+  if (classes_on) *classes_on = cls.small_max > 0 || cls.mid_max > 0;
   for (int64_t i = 0; i < count; ++i) {
     const eb2_gemm_problem& q = ps[i];
     const int oa = op_code(q.transa), ob = op_code(q.transb);
@@ -190,9 +192,11 @@ int eb2_grouped_plan_create(char dtype, int64_t count, const eb2_gemm_problem* p
   if (!cx) return EB2_ERR_NO_DEVICE;
   std::vector<eb2::GroupedProblem> ps;
   std::vector<eb2::GroupedItem> items;
-  int rc = eb2::build(dtype, count, problems, ps, items);
+  bool classes_on = true;
+  int rc = eb2::build(dtype, count, problems, ps, items, &classes_on);
   if (rc != EB2_OK) return rc;
   auto* p = new eb2_grouped_plan();
+  p->classes_on = classes_on;
   p->device = cx->device;
   p->f64 = (dtype == 'd');
   p->count = count;
@@ -237,6 +241,8 @@ int eb2_grouped_plan_execute(eb2_grouped_plan_t plan, void* stream) {
   }
   eb2_call_info& ci = eb2::call_info();
   ci = eb2_call_info{};
+  eb2::call_config() = eb2::CallConfig{};
+  eb2::call_config().config = plan->classes_on ? eb2::kCfgBatchClasses : eb2::kCfgBatchTiles;
   ci.dtype = plan->f64 ? 'd' : 's';
   ci.method = EB2_METHOD_NATIVE;
   ci.launches = plan->num_items > 0 ? 1 : 0;

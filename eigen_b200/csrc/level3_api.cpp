@@ -570,6 +570,7 @@ struct Call {
     st = cx->stream;
     fence.emplace(*cx, st);
     call_info() = eb2_call_info{};
+    call_config() = CallConfig{};
     set_pending_timing(nullptr, false);
     return true;
   }

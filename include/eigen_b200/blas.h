@@ -276,10 +276,12 @@ typedef struct eb2_call_info {
   int launches;       /* kernels this library launched for the call */
   double spread;      /* emulated DGEMM: mean (largest - mean) binary exponent of 64-entry
                          row chunks of op(A) and op(B)^T, the picker's data feature; else 0 */
-  int config;         /* configuration class of the call (see eb2_set_config), -1 if none */
-  int splits;         /* CRT DGEMM: K ranges per output tile and modulus (1: no split) */
 } eb2_call_info;
 int eb2_last_call_info(eb2_call_info* out);
+/* The configuration class of this thread's last product (see eb2_set_config; -1 if none) and,
+ * for a CRT DGEMM, its K splits per output tile and modulus (1: no split).  A separate call,
+ * so that eb2_call_info keeps its layout for programs built against it. */
+int eb2_last_call_config(int* config, int* splits);
 
 /* How many calls of the named BLAS routine ("dgemm", "zgemm", "dtrsm", "ssyrk", ...: lower
  * case, no underscore) reached the device in this process: every call past its argument

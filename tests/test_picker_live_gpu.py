@@ -53,7 +53,7 @@ def test_picker_choice_against_live_best():
     assert eb.set_picker(w) == eb.EB2_OK
     rows = json.loads((DATA / "tune_report.json").read_text())["holdout_rows"]
     # problems of 0.05 .. 5 ms (live timing noise stays small against them), DGEMM and SGEMM
-    cand = [r for r in rows if r["kind"] in ("d", "s") and 0.05 <= r["t_best"] <= 5.0]
+    cand = [r for r in rows if r["kind"] in ("d", "s") and 0.05 <= r["times_ms"][str(r["best"])] <= 5.0]
     rng = np.random.default_rng(0)
     pick = rng.choice(len(cand), size=min(20, len(cand)), replace=False)
     g = torch.Generator(device="cuda")
