@@ -279,6 +279,51 @@ def profiled_traffic(size: int, instantiation: str):
     return None, None
 
 
+# ------------------------------------------------------------------------ end-to-end legs
+def pageable_e2e_leg(eb, A, B, S, steps, rank_max, world):
+    """dgemm_ on ordinary (pageable) numpy buffers, as a C or Fortran caller with malloc'd
+    matrices calls it: beta = 0 (C not read) and beta = 1 (C copied in as well, what Eigen's
+    operator* passes); host-timed synchronous calls, copies included."""
+    import numpy as np
+
+    hA = np.asfortranarray(A.cpu().numpy().T)  # column-major S x S, pageable
+    hB = np.asfortranarray(B.cpu().numpy().T)
+    hC = np.zeros((S, S), order="F")
+    out = {}
+    for beta in (0.0, 1.0):
+        eb.dgemm("N", "N", S, S, S, 1.0, hA, S, hB, S, beta, hC, S)  # warm-up (staging buffers)
+        times = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            eb.dgemm("N", "N", S, S, S, 1.0, hA, S, hB, S, beta, hC, S)
+            times.append(time.perf_counter() - t0)
+        t = rank_max(float(np.median(times)))
+        out[f"beta{int(beta)}"] = {
+            "value": round(whole_job_tflops(world, 2.0 * S ** 3, t * 1e3), 3), "unit": UNIT,
+            "ms_per_step": round(t * 1e3, 3), "steps": steps,
+            "h2d_bytes_per_step": (2 + int(beta != 0.0)) * S * S * 8, "d2h_bytes_per_step": S * S * 8}
+    out["api"] = "dgemm_ (Fortran BLAS ABI) on pageable host buffers; synchronous call timed on the host"
+    return out
+
+
+def eigen_seam_leg(S, reps=3):
+    """Eigen's operator* (C.noalias() = A * B on pageable MatrixXd) compiled with EIGEN_USE_BLAS
+    against the reference headers and linked to the library (tests/eigen_seam/eigen_seam_bench):
+    beta = 1 after Eigen's setZero, so C is copied in too; host-timed, median of `reps`."""
+    exe = ROOT / "tests" / "eigen_seam" / "_bin" / "eigen_seam_bench"
+    if not exe.exists():
+        return {"error": "tests/eigen_seam/_bin/eigen_seam_bench not built (make -C tests/eigen_seam REF=...)"}
+    r = subprocess.run([str(exe), str(S), str(reps), "1"], capture_output=True, text=True, timeout=900)
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return {"error": f"eigen_seam_bench rc={r.returncode}: {(r.stderr or r.stdout).strip()[:200]}"}
+    res = json.loads(lines[-1])
+    return {"value": round(res["tflops"], 3), "unit": UNIT, "ms_per_step": round(res["seconds_median"] * 1e3, 3),
+            "steps": res["reps"], "h2d_bytes_per_step": 3 * S * S * 8, "d2h_bytes_per_step": S * S * 8,
+            "method": res["method"], "moduli_or_slices": res["slices"], "spot_rel_err": res["spot_rel_err"],
+            "api": "Eigen MatrixXd operator* (C.noalias() = A * B) through EIGEN_USE_BLAS -> dgemm_, pageable"}
+
+
 # ------------------------------------------------------------------------ native sweep
 def native_sweep_leg(eb, torch, dev, rank_max, sizes=(1024, 2048, 4096, 8192), reps=3):
     """The native-precision sweep: DGEMM and SGEMM at M = N = K in `sizes`, NN / NT / TN,
@@ -713,6 +758,12 @@ def our_arm(a, world, rank, local):
                "ms_per_step": round(t_step * 1e3, 3), "steps": e2e_steps,
                "api": "dgemm_ (Fortran BLAS ABI) on pinned host buffers; synchronous call timed on the host"}
 
+    e2e_pageable = e2e_eigen = None
+    if not a.no_e2e:
+        e2e_pageable = pageable_e2e_leg(eb, A, B, S, min(a.steps, 3), rank_max, world)
+        if rank == 0 and world == 1:
+            e2e_eigen = eigen_seam_leg(S, reps=3)
+
     accuracy = None
     if not a.no_accuracy:
         accuracy = accuracy_leg(eb, torch, dev, S, (0, 8, 32))
@@ -788,7 +839,8 @@ def our_arm(a, world, rank, local):
                            kernel_ms_per_call=kernel_ms_per_call),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "native_fp64": native, "accuracy": accuracy, "sgemm": sgemm, "grouped_batch": grouped,
-            "level3_routines": level3, "native_sweep": sweep,
+            "level3_routines": level3, "native_sweep": sweep, "e2e_pageable": e2e_pageable,
+            "e2e_eigen_operator": e2e_eigen,
             "emulated_over_native": round(value / native["tflops"], 3) if native else None,
         }
         print(json.dumps(line))

@@ -59,7 +59,18 @@ bool device_usable(const void* p) {
 bool copy_block(void* dst, size_t dpitch, const void* src, size_t spitch, size_t row_bytes, int64_t cols,
                 cudaMemcpyKind kind, cudaStream_t st) {
   if (cols <= 0 || row_bytes == 0) return true;
-  cudaError_t e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, row_bytes, size_t(cols), kind, st);
+  // through the context's stager (pinned bounce buffers for pageable host memory); the caller
+  // holds the context's mutex.  Device -> host copies have landed when this returns.
+  Context* cx = current_context();
+  cudaError_t e;
+  if (cx && kind == cudaMemcpyHostToDevice) {
+    e = cx->stager.to_device(dst, dpitch, src, spitch, row_bytes, size_t(cols), st);
+  } else if (cx && kind == cudaMemcpyDeviceToHost) {
+    e = cx->stager.to_host(dst, dpitch, src, spitch, row_bytes, size_t(cols), st);
+    if (e == cudaSuccess) e = cx->stager.drain();
+  } else {
+    e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, row_bytes, size_t(cols), kind, st);
+  }
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
     set_error(EB2_ERR_CUDA, "staging copy failed: %s", cudaGetErrorString(e));

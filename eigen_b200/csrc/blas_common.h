@@ -48,8 +48,10 @@ void count_call(const char* name);
 // True when the device can use the pointer in place (device or managed memory).
 bool device_usable(const void* p);
 
-// Copy a column-major block of `cols` columns, `row_bytes` each, between host and device;
-// sets the thread's error and returns false when the copy cannot be queued.
+// Copy a column-major block of `cols` columns, `row_bytes` each, between host and device
+// (pageable host memory through the context's pinned bounce buffers; a device -> host copy
+// has landed when this returns); sets the thread's error and returns false when the copy
+// cannot be queued.  The caller holds the context's mutex.
 bool copy_block(void* dst, size_t dpitch, const void* src, size_t spitch, size_t row_bytes, int64_t cols,
                 cudaMemcpyKind kind, cudaStream_t st);
 

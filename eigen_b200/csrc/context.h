@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "eigen_b200/blas.h"
+#include "host_stager.h"
 
 namespace eb2 {
 
@@ -69,6 +70,8 @@ struct Context {
   // see StreamFence.
   cudaEvent_t ev_fence = nullptr;
   bool fence_armed = false;
+  // host <-> device copies of the BLAS entry points (bounce buffers for pageable memory)
+  HostStager stager;
 };
 
 // The workspaces and the flag block of a context pass from one call to the next in stream

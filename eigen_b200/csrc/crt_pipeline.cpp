@@ -18,6 +18,7 @@
 
 #include "context.h"
 #include "gemm_driver.h"
+#include "host_stager.h"
 #include "mlp.h"
 #include "kernels.h"
 
@@ -32,12 +33,6 @@ bool check_cuda(cudaError_t e, const char* what) {
   (void)cudaGetLastError();
   set_error(EB2_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
   return false;
-}
-
-bool copy2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t height,
-            cudaMemcpyKind kind, cudaStream_t st) {
-  if (width == 0 || height == 0) return true;
-  return check_cuda(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height, kind, st), "staging copy");
 }
 
 constexpr int64_t kBlockCols = 1024;  // target columns per block (rounded to the 256-column tile)
@@ -105,20 +100,28 @@ int dgemm_crt_pipelined(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int
   info.err_estimate = 0.0;
 
   // ------------------------------------------------ copy-in: A, then B (and C) by blocks
-  if (!copy2d(dA, a_rows * 8, A, lda * 8, a_rows * 8, a_cols, cudaMemcpyHostToDevice, cin) ||
+  // Pinned sources are enqueued at once; pageable ones go through the stager's bounce buffers
+  // (the host copies a block while the device works on the ones before it), a few blocks ahead.
+  HostStager& hs = cx.stager;
+  const bool all_pinned = HostStager::pinned(A) && HostStager::pinned(B) && (beta == 0.0 || HostStager::pinned(C));
+  const int lookahead = all_pinned ? nb : 2;
+  if (!check_cuda(hs.to_device(dA, a_rows * 8, A, lda * 8, a_rows * 8, a_cols, cin), "copy A") ||
       !check_cuda(cudaEventRecord(cx.ev_a, cin), "event"))
     return EB2_ERR_CUDA;
-  for (int c = 0; c < nb; ++c) {
+  int staged = 0;  // blocks whose copies are enqueued
+  auto stage_block = [&](int c) -> bool {
     const int64_t j0 = c * nc, w = std::min(nc, n - j0);
     // op(B)(:, j0:j0+w) is B(:, j0:...) (N) or B(j0:..., :) (T); staged with ld = b_rows
-    const bool okb = tb ? copy2d(dB + j0, b_rows * 8, B + j0, ldb * 8, w * 8, k, cudaMemcpyHostToDevice, cin)
-                        : copy2d(dB + j0 * b_rows, b_rows * 8, B + j0 * ldb, ldb * 8, k * 8, w,
-                                 cudaMemcpyHostToDevice, cin);
+    const bool okb = tb ? check_cuda(hs.to_device(dB + j0, b_rows * 8, B + j0, ldb * 8, w * 8, k, cin), "copy B")
+                        : check_cuda(hs.to_device(dB + j0 * b_rows, b_rows * 8, B + j0 * ldb, ldb * 8, k * 8, w, cin),
+                                     "copy B");
     // beta == 0 never reads C (blas/level3_impl.h:82-84)
-    const bool okc = beta == 0.0 ||
-                     copy2d(dC + j0 * m, m * 8, C + j0 * ldc, ldc * 8, m * 8, w, cudaMemcpyHostToDevice, cin);
-    if (!okb || !okc || !check_cuda(cudaEventRecord(cx.ev_in[c], cin), "event")) return EB2_ERR_CUDA;
-  }
+    const bool okc =
+        beta == 0.0 || check_cuda(hs.to_device(dC + j0 * m, m * 8, C + j0 * ldc, ldc * 8, m * 8, w, cin), "copy C");
+    return okb && okc && check_cuda(cudaEventRecord(cx.ev_in[c], cin), "event");
+  };
+  while (staged < std::min(nb, lookahead))
+    if (!stage_block(staged++)) return EB2_ERR_CUDA;
 
   // ------------------------------------------------ compute: A once
   const StridedView<double> va = ta ? StridedView<double>{dA, m, k, a_rows, 1} : StridedView<double>{dA, m, k, 1, a_rows};
@@ -142,9 +145,12 @@ int dgemm_crt_pipelined(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int
   // the ordinary device path for block c (adds moduli as needed), C block restored first
   auto ordinary_block = [&](int c) -> int {
     const int64_t j0 = c * nc, w = std::min(nc, n - j0);
-    if (!check_cuda(cudaStreamSynchronize(st), "DGEMM") ||
+    while (staged <= c)  // its B block
+      if (!stage_block(staged++)) return EB2_ERR_CUDA;
+    if (!check_cuda(cudaStreamWaitEvent(st, cx.ev_in[c], 0), "wait block") ||
+        !check_cuda(cudaStreamSynchronize(st), "DGEMM") ||
         (beta != 0.0 &&
-         !copy2d(dC + j0 * m, m * 8, C + j0 * ldc, ldc * 8, m * 8, w, cudaMemcpyHostToDevice, st)))
+         !check_cuda(hs.to_device(dC + j0 * m, m * 8, C + j0 * ldc, ldc * 8, m * 8, w, st), "restore C")))
       return EB2_ERR_CUDA;
     const double* bblk = tb ? dB + j0 : dB + j0 * b_rows;
     DgemmOptions o;
@@ -187,7 +193,7 @@ int dgemm_crt_pipelined(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int
     }
     const int64_t j0 = c * nc, w = std::min(nc, n - j0);
     if (!check_cuda(cudaStreamWaitEvent(cout, cx.ev_done[c], 0), "wait block") ||
-        !copy2d(C + j0 * ldc, ldc * 8, dC + j0 * m, m * 8, m * 8, w, cudaMemcpyDeviceToHost, cout))
+        !check_cuda(hs.to_host(C + j0 * ldc, ldc * 8, dC + j0 * m, m * 8, m * 8, w, cout), "copy C out"))
       return EB2_ERR_CUDA;
     return EB2_OK;
   };
@@ -207,10 +213,12 @@ int dgemm_crt_pipelined(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int
       if (rc == EB2_ERR_ACCURACY) rc_all = rc;
       const int64_t jj = c * nc;
       if (!check_cuda(cudaStreamWaitEvent(cout, cx.ev_done[c], 0), "wait block") ||
-          !copy2d(C + jj * ldc, ldc * 8, dC + jj * m, m * 8, m * 8, w, cudaMemcpyDeviceToHost, cout))
+          !check_cuda(hs.to_host(C + jj * ldc, ldc * 8, dC + jj * m, m * 8, m * 8, w, cout), "copy C out"))
         return EB2_ERR_CUDA;
       continue;
     }
+    while (staged <= c)
+      if (!stage_block(staged++)) return EB2_ERR_CUDA;
     const double* bblk = tb ? dB + j0 : dB + j0 * b_rows;
     const StridedView<double> vb =
         tb ? StridedView<double>{bblk, w, k, 1, b_rows} : StridedView<double>{bblk, w, k, b_rows, 1};
@@ -257,10 +265,13 @@ int dgemm_crt_pipelined(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int
     ok = ok && check_cuda(cudaEventRecord(cx.ev_done[c], st), "event");
     if (!ok) return EB2_ERR_CUDA;
     info.launches += 8;
+    // while the device computes this block: the host side of the next input block's copies
+    if (staged < nb && staged < c + 1 + lookahead && !stage_block(staged++)) return EB2_ERR_CUDA;
     if (pending >= 0) {  // check the previous block while this one runs
       const int rc = finish_block(pending);
       if (rc != EB2_OK) return rc;
     }
+    if (!check_cuda(hs.progress(), "copy C out")) return EB2_ERR_CUDA;
     pending = c;
   }
   if (pending >= 0) {
@@ -269,7 +280,8 @@ int dgemm_crt_pipelined(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int
   }
   cudaEventRecord(cx.ev_stop, st);
   set_pending_timing(&cx, false);
-  if (!check_cuda(cudaStreamSynchronize(cout), "copy C") || !check_cuda(cudaStreamSynchronize(st), "DGEMM"))
+  if (!check_cuda(hs.drain(), "copy C out") || !check_cuda(cudaStreamSynchronize(cout), "copy C") ||
+      !check_cuda(cudaStreamSynchronize(st), "DGEMM"))
     return EB2_ERR_CUDA;
   info.tile_n = choose_crt_tile(cx, m, nc);
   call_config().config = info.tile_n == kTilePair ? kCfgCrtPair : kCfgCrtCta;

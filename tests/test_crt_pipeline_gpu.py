@@ -86,3 +86,27 @@ def test_pipelined_nonfinite_block_uses_native_kernel():
     fin = np.isfinite(Cn)
     # blocks computed before the Inf was seen are CRT results; the rest are native
     assert np.max(np.abs(Ch[fin] - Cn[fin])) <= 1e-12 * np.max(np.abs(Cn[fin]))
+
+
+@pytest.mark.parametrize("kinds", ["pageable", "pinned", "mixed"])
+def test_pipelined_host_call_bounce_buffers(kinds):
+    """Pageable host operands go through the library's pinned bounce buffers (16 MB chunks of
+    whole columns, several per operand and per C block here, both directions), pinned ones
+    straight to the copy engine: every mix gives the device path's bits."""
+    m, n, k = 4096, 3000, 700
+    A, lda, B, ldb, C, ldc = make_operands(m, n, k, "N", "N", pad=3, r=2, seed=77)
+
+    def host(x, pin):
+        if not pin:
+            return np.asfortranarray(x.copy())
+        t = torch.empty(x.shape[::-1], dtype=torch.float64, pin_memory=True)  # column-major view
+        t.copy_(torch.from_numpy(np.ascontiguousarray(x.T)))
+        return t
+
+    pins = {"pageable": (False, False, False), "pinned": (True, True, True), "mixed": (True, False, False)}[kinds]
+    hA, hB, hC = host(A, pins[0]), host(B, pins[1]), host(C, pins[2])
+    eb.dgemm("N", "N", m, n, k, 0.5, hA, lda, hB, ldb, 1.0, hC, ldc)
+    assert eb.last_error()[0] == eb.EB2_OK, eb.last_error()
+    assert eb.last_call_info()["staged"] == 1
+    got = np.asfortranarray(hC.numpy().T) if isinstance(hC, torch.Tensor) else hC
+    np.testing.assert_array_equal(got, _device("N", "N", m, n, k, 0.5, A, lda, B, ldb, 1.0, C, ldc))
