@@ -204,8 +204,9 @@ def main(argv=None):
     ap.add_argument("--count", type=int, default=10000)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-check", action="store_true", help="DGEMM without the a-posteriori accuracy check")
-    ap.add_argument("--tile", type=int, choices=[0, 128, 256, 512], default=0,
-                    help="tcgen05 tile configuration (256: one CTA per 128x256 tile, 512: CTA pair; 0: per call)")
+    ap.add_argument("--tile", type=int, choices=[0, 128, 256, 512, 1024], default=0,
+                    help="tcgen05 tile configuration (256: one CTA per 128x256 tile, 512: CTA pair, "
+                         "1024: one CTA per 256x256 tile, CRT only; 0: per call)")
     a = ap.parse_args(argv)
     import torch
 

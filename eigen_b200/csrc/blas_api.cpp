@@ -293,7 +293,8 @@ int eb2_set_dgemm_tolerance(double tol) {
 }
 
 int eb2_set_tile_n(int tile_n) {
-  if (tile_n != 0 && tile_n != 128 && tile_n != 256 && tile_n != eb2::kTilePair) return EB2_ERR_ARG;
+  if (tile_n != 0 && tile_n != 128 && tile_n != 256 && tile_n != eb2::kTilePair && tile_n != eb2::kTileWide)
+    return EB2_ERR_ARG;
   eb2::settings().tile_n = tile_n;
   return EB2_OK;
 }

@@ -913,15 +913,15 @@ void launch_rec128(bool est, dim3 grid, cudaStream_t stream, const CrtRecParams&
     crt_reconstruct128_kernel<N, false><<<grid, 256, 0, stream>>>(R);
 }
 
-template <int BN, int STAGES, bool PAIR>
+template <int BN, int STAGES, bool PAIR, int MT = 1, int NW = 4>
 cudaError_t launch_gemm_config(const CrtOperand& a, const CrtOperand& b, const CrtGemmArgs& args,
                                cudaStream_t stream) {
-  constexpr int kRowsPerTile = PAIR ? 2 * kSliceBM : kSliceBM;
+  constexpr int kRowsPerTile = PAIR ? 2 * kSliceBM : MT * kSliceBM;
   if (a.rows_pad % kRowsPerTile != 0 || b.rows_pad % BN != 0 || args.ld_res != a.rows_pad)
     return cudaErrorInvalidValue;
   CUtensorMap tmA, tmB;
   if (!make_tensor_map_3d(&tmA, a.residues, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, uint64_t(a.k_pad), uint64_t(a.rows_pad),
-                          uint64_t(a.nmax), kSliceKBytes, kSliceBM))
+                          uint64_t(a.nmax), kSliceKBytes, PAIR ? kSliceBM : MT * kSliceBM))
     return cudaErrorInvalidValue;
   if (!make_tensor_map_3d(&tmB, b.residues, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, uint64_t(b.k_pad), uint64_t(b.rows_pad),
                           uint64_t(b.nmax), kSliceKBytes, PAIR ? BN / 2 : BN))
@@ -951,14 +951,14 @@ cudaError_t launch_gemm_config(const CrtOperand& a, const CrtOperand& b, const C
   P.tri_k = args.tri_k;
   if (P.tile_list) {
     if (P.num_listed < 1 || P.num_listed > P.tiles_m * P.tiles_n) return cudaErrorInvalidValue;
-    return launch_slice_gemm<kModeCrtI8Listed, BN, STAGES, 4, PAIR>(tmA, tmB, P, args.num_sms, stream);
+    return launch_slice_gemm<kModeCrtI8Listed, BN, STAGES, NW, PAIR, MT>(tmA, tmB, P, args.num_sms, stream);
   }
-  return launch_slice_gemm<kModeCrtI8, BN, STAGES, 4, PAIR>(tmA, tmB, P, args.num_sms, stream);
+  return launch_slice_gemm<kModeCrtI8, BN, STAGES, NW, PAIR, MT>(tmA, tmB, P, args.num_sms, stream);
 }
 
 }  // namespace
 
-int64_t crt_tile_rows(int tile_n) { return tile_n == kTilePair ? 256 : 128; }
+int64_t crt_tile_rows(int tile_n) { return (tile_n == kTilePair || tile_n == kTileWide) ? 256 : 128; }
 int64_t crt_tile_cols(int tile_n) { return tile_n == 128 ? 128 : 256; }
 
 void crt_triangle_tiles(int tile_n, int64_t rows_pad, int64_t cols_pad, int64_t n, bool upper, int group_m, int* out,
@@ -1021,6 +1021,8 @@ cudaError_t launch_crt_gemm(const CrtOperand& a, const CrtOperand& b, const CrtG
   if (a.k_pad != b.k_pad || a.k_pad % kSliceKBytes != 0) return cudaErrorInvalidValue;
   if (args.tile_n == kTilePair) return launch_gemm_config<256, 6, true>(a, b, args, stream);
   if (args.tile_n == 256) return launch_gemm_config<256, 4, false>(a, b, args, stream);
+  // 256 x 256 per CTA: 64 KB stages (three), eight epilogue warps (two per TMEM lane quadrant)
+  if (args.tile_n == kTileWide) return launch_gemm_config<256, 3, false, 2, 8>(a, b, args, stream);
   return cudaErrorInvalidValue;
 }
 

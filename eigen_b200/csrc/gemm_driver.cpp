@@ -103,7 +103,7 @@ int crt_split_rule(const Context& cx, int64_t m_pad, int64_t n_pad, int64_t k_pa
 
 int choose_crt_tile(const Context& cx, int64_t m, int64_t n) {
   const int forced = settings().tile_n.load();
-  if (forced == kTilePair) return kTilePair;
+  if (forced == kTilePair || forced == kTileWide) return forced;
   if (forced == 128 || forced == 256) return 256;
   // CTA pairs (256 x 256) unless that leaves most SMs idle
   const int64_t pair_tiles = ((m + 255) / 256) * ((n + 255) / 256);
@@ -123,7 +123,8 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   const bool check = opt.check_accuracy;
   const int forced = opt.moduli ? opt.moduli : settings().dgemm_moduli.load();
   int nmod = forced ? forced : kCrtDefaultModuli;
-  const bool auto_tile = opt.tile_n != kTilePair && opt.tile_n != 256 && settings().tile_n.load() == 0;
+  const bool auto_tile =
+      opt.tile_n != kTilePair && opt.tile_n != kTileWide && opt.tile_n != 256 && settings().tile_n.load() == 0;
   // Stage 2 of the learned picker: tile configuration and modulus count, once the scan
   // has measured the inputs' exponent spread.  It needs the host to read the scan's result,
   // so a call captured into a graph keeps the stage-1 choice.
@@ -137,7 +138,8 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   const bool stage2 = picker_weights() != nullptr && !forced_cfg && (auto_tile || forced == 0) &&
                       capture == cudaStreamCaptureStatusNone;
   const int nmax = (check || stage2) ? std::max(nmod, kCrtMaxModuli) : nmod;
-  int tile = (opt.tile_n == kTilePair || opt.tile_n == 256) ? opt.tile_n : choose_crt_tile(cx, m, n);
+  int tile = (opt.tile_n == kTilePair || opt.tile_n == kTileWide || opt.tile_n == 256) ? opt.tile_n
+                                                                                         : choose_crt_tile(cx, m, n);
   int group_m = 0, splits = 1;
   const StridedView<double> va = view_a(ta, A, lda, m, k);
   const StridedView<double> vb = view_bt(tb, B, ldb, n, k);

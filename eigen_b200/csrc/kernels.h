@@ -45,6 +45,9 @@ constexpr int kOzakiMaxSlices = 12;
 // Tile configurations of the tcgen05 kernels: 128 / 256 = one CTA computing 128 x 128 /
 // 128 x 256 tiles; kTilePair = a CTA pair (cluster of 2) computing 256 x 256 tiles.
 constexpr int kTilePair = 512;
+// CRT GEMM only: one CTA computing 256 x 256 tiles (two M = 128 MMAs per K step share the B
+// tile; the accumulator fills the TMEM, so consecutive tiles do not overlap).
+constexpr int kTileWide = 1024;
 constexpr int kOzakiKBlock = 128;  // bytes of K per pipeline stage (int8 digits)
 constexpr int kOzakiBM = 128;
 
@@ -138,7 +141,7 @@ struct CrtGemmArgs {
   int moduli;
   const int* skip_if_flag;
   uint32_t* status;
-  int tile_n;  // 256 or kTilePair
+  int tile_n;  // 256, kTilePair or kTileWide
   int num_sms;
   uint8_t* cres;   // [moduli][n_pad][ld_res] residues of C' (uint8 in [0, p))
   int64_t ld_res;  // = a.rows_pad

@@ -52,10 +52,12 @@ constexpr int kMaxUnitKbCrt = 1023;
 // nearest, into FP32 registers of the epilogue; the accumulator restarts from zero.
 constexpr int kBf16ChunkKb = 4;
 
-template <int BN, int STAGES, bool PAIR>
+// MT: row tiles of 128 per CTA (1, or 2 for the one-CTA 256-row tile of the CRT GEMM: two
+// M = 128 MMAs per K step share the B tile, and the accumulator fills the whole TMEM).
+template <int BN, int STAGES, bool PAIR, int MT = 1>
 struct SliceLayout {
   static constexpr int kBRows = PAIR ? BN / 2 : BN;  // rows of B loaded by one CTA
-  static constexpr int kABytes = kSliceBM * kSliceKBytes;
+  static constexpr int kABytes = MT * kSliceBM * kSliceKBytes;
   static constexpr int kBBytes = kBRows * kSliceKBytes;
   static constexpr int kAOff = 0;
   static constexpr int kBOff = kAOff + STAGES * kABytes;
@@ -267,11 +269,12 @@ __device__ __forceinline__ int tile_step() {
 
 
 // ------------------------------------------------------------------ producer (warp 0, one lane)
-template <int MODE, int BN, int STAGES, bool PAIR>
+template <int MODE, int BN, int STAGES, bool PAIR, int MT>
 __device__ __forceinline__ void slice_producer(const CUtensorMap* tmA, const CUtensorMap* tmB, uint8_t* smem,
                                                uint64_t* full, uint64_t* empty, volatile int* abort_flag,
                                                const SliceGemmParams& P, uint32_t rank) {
-  using L = SliceLayout<BN, STAGES, PAIR>;
+  using L = SliceLayout<BN, STAGES, PAIR, MT>;
+  constexpr int kTileRows = PAIR ? 2 * kSliceBM : MT * kSliceBM;
   constexpr int ke = SliceTraits<MODE, BN, PAIR>::kKElems;  // innermost coordinate step (elements)
   constexpr uint32_t kTx = (PAIR ? 2u : 1u) * uint32_t(L::kABytes + L::kBBytes);
   constexpr bool kListed = MODE == kModeCrtI8Listed;
@@ -284,7 +287,7 @@ __device__ __forceinline__ void slice_producer(const CUtensorMap* tmA, const CUt
   auto issue = [&](int tm, int tn, int p, int q_slice, int kb) -> bool {
     const int stage = int(issued % STAGES);
     if (!mbar_wait(&empty[stage], ((issued / STAGES) & 1u) ^ 1u, abort_flag, P.status, P.wait_limit_ns)) return false;
-    const int a_row = tm * (PAIR ? 2 * kSliceBM : kSliceBM) + a_row_off;
+    const int a_row = tm * kTileRows + a_row_off;
     const int b_row = tn * BN + b_row_off;
     if (PAIR) {
       // both CTAs' bytes land on the leader's barrier; only the leader posts expect-tx
@@ -319,7 +322,7 @@ __device__ __forceinline__ void slice_producer(const CUtensorMap* tmA, const CUt
     }
   } else {
     BlockIter<kListed, is_crt_mode(MODE)> it;
-    it.start(P, nwork, first_tile<PAIR>(), tile_step<PAIR>(), PAIR ? 2 * kSliceBM : kSliceBM, BN);
+    it.start(P, nwork, first_tile<PAIR>(), tile_step<PAIR>(), kTileRows, BN);
     while (it.valid) {
       int tm, tn;
       tile_coords(it.tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
@@ -364,11 +367,12 @@ __device__ __forceinline__ void commit_to(uint64_t* bar) {
   }
 }
 
-template <int MODE, int BN, int STAGES, bool PAIR>
+template <int MODE, int BN, int STAGES, bool PAIR, int MT>
 __device__ __forceinline__ void slice_mma(uint8_t* smem, uint64_t* full, uint64_t* empty, uint64_t* tfull,
                                           uint64_t* tempty, uint64_t* drain, uint32_t tmem_base,
                                           volatile int* abort_flag, const SliceGemmParams& P) {
-  using L = SliceLayout<BN, STAGES, PAIR>;
+  using L = SliceLayout<BN, STAGES, PAIR, MT>;
+  constexpr int kTileRows = PAIR ? 2 * kSliceBM : MT * kSliceBM;
   constexpr uint32_t idesc = SliceTraits<MODE, BN, PAIR>::kIdesc;
   constexpr bool kListed = MODE == kModeCrtI8Listed;
   const int nwork = num_work<kListed>(P);
@@ -386,17 +390,24 @@ __device__ __forceinline__ void slice_mma(uint8_t* smem, uint64_t* full, uint64_
 #pragma unroll
     for (int kk = 0; kk < kSliceKBytes / 32; ++kk) {
       const uint32_t acc = (fresh && kk == 0) ? 0u : 1u;
-      const uint64_t ad = adesc + uint64_t(2 * kk), bd = bdesc + uint64_t(2 * kk);
-      if (PAIR) {
-        if (MODE != kModeSplitBF16)
-          mma_i8_pair(d_tmem, ad, bd, idesc, acc);
-        else
-          mma_f16_pair(d_tmem, ad, bd, idesc, acc);
-      } else {
-        if (MODE != kModeSplitBF16)
-          mma_i8(d_tmem, ad, bd, idesc, acc);
-        else
-          mma_f16(d_tmem, ad, bd, idesc, acc);
+      const uint64_t bd = bdesc + uint64_t(2 * kk);
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) {
+        // row tile mt: 128 rows of 128 bytes further on (descriptor addresses count 16 bytes);
+        // its accumulator is the TMEM region of columns mt * BN ..
+        const uint64_t ad = adesc + uint64_t(mt * (kSliceBM * kSliceKBytes / 16)) + uint64_t(2 * kk);
+        const uint32_t dt = d_tmem + uint32_t(mt * BN);
+        if (PAIR) {
+          if (MODE != kModeSplitBF16)
+            mma_i8_pair(dt, ad, bd, idesc, acc);
+          else
+            mma_f16_pair(dt, ad, bd, idesc, acc);
+        } else {
+          if (MODE != kModeSplitBF16)
+            mma_i8(dt, ad, bd, idesc, acc);
+          else
+            mma_f16(dt, ad, bd, idesc, acc);
+        }
       }
     }
     commit_to<PAIR>(&empty[stage]);
@@ -442,7 +453,7 @@ __device__ __forceinline__ void slice_mma(uint8_t* smem, uint64_t* full, uint64_
         if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, is_crt_mode(MODE))) continue;
         if constexpr (is_crt_mode(MODE)) {
           int kb_lo, kb_hi;
-          tile_k_range(P, tile, split, PAIR ? 2 * kSliceBM : kSliceBM, BN, kb_lo, kb_hi);
+          tile_k_range(P, tile, split, kTileRows, BN, kb_lo, kb_hi);
           total = kb_hi - kb_lo;
         }
         constexpr int kUnit = SliceTraits<MODE, BN, PAIR>::kUnitKb;
@@ -458,7 +469,7 @@ __device__ __forceinline__ void slice_mma(uint8_t* smem, uint64_t* full, uint64_
           if (!ok) break;
           commit_to<PAIR>(&tfull[buf]);
           tphase ^= 1u << buf;
-          buf ^= 1;
+          if constexpr (MT == 1) buf ^= 1;  // MT = 2: one accumulator fills the TMEM
           u0 = u1;
         }
       }
@@ -592,15 +603,21 @@ __device__ __forceinline__ uint32_t mod_small(uint32_t x, uint32_t p, uint32_t m
 // CRT: unit t is modulus p_t; every INT32 product entry is reduced to [0, p_t) and stored
 // as one byte of residue plane t (column-major, ld_res).  K beyond one unit comes in
 // further chunks whose residues are added mod p_t.
-template <int BN, int NW, bool PAIR, bool LISTED>
+// MT = 2: warp group g = (warp - 2) / 4 drains row tile g % 2 (TMEM columns (g % 2) * BN ..)
+// and its columns (g / 2) * kCols ..; the accumulator has a single buffer then.
+template <int BN, int NW, bool PAIR, bool LISTED, int MT>
 __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull, uint64_t* tempty,
                                              volatile int* abort_flag, const SliceGemmParams& P) {
-  constexpr int kCols = BN * 4 / NW;
+  static_assert(NW % (4 * MT) == 0, "whole warp groups per row tile");
+  constexpr int kCols = BN * 4 * MT / NW;
   static_assert(kCols % 32 == 0, "column slice");
+  constexpr int kTileRows = PAIR ? 2 * kSliceBM : MT * kSliceBM;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int quad = warp & 3;
-  const int col_base = ((warp - 2) >> 2) * kCols;
-  const int row = quad * 32 + lane;
+  const int group = (warp - 2) >> 2;
+  const int region = group % MT;  // row tile within the CTA's tile
+  const int col_base = (group / MT) * kCols;
+  const int row = region * kSliceBM + quad * 32 + lane;
   const int nwork = num_work<LISTED>(P);
   const int row_base = PAIR ? int(cluster_ctarank()) * kSliceBM : 0;
   const int64_t plane = P.ld_res * int64_t(P.tiles_n) * BN;
@@ -611,7 +628,7 @@ __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull
     int tile, t_hi, t_lo, tm, tn, split;
     work_item<LISTED>(P, w, tile, t_hi, t_lo, split);
     tile_coords(tile, P.tiles_m, P.tiles_n, P.group_m, tm, tn);
-    const int64_t m0 = int64_t(tm) * (PAIR ? 2 * kSliceBM : kSliceBM) + row_base;
+    const int64_t m0 = int64_t(tm) * kTileRows + row_base;
     const int64_t n0 = int64_t(tn) * BN + col_base;
     const int64_t grow = m0 + row;
     for (int t = t_hi; t >= t_lo && ok; --t) {
@@ -619,7 +636,7 @@ __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull
       if (!diag_bounds(t, P.slices, P.num_kb, p_lo, total, true)) continue;
       {
         int kb_lo, kb_hi;
-        tile_k_range(P, tile, split, PAIR ? 2 * kSliceBM : kSliceBM, BN, kb_lo, kb_hi);
+        tile_k_range(P, tile, split, kTileRows, BN, kb_lo, kb_hi);
         total = kb_hi - kb_lo;
       }
       const uint32_t pm = uint32_t(crt_modulus(t));
@@ -635,7 +652,8 @@ __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull
           break;
         }
         tc_fence_after();
-        const uint32_t taddr = tmem_base + uint32_t(buf * BN + col_base) + (uint32_t(quad * 32) << 16);
+        const uint32_t taddr =
+            tmem_base + uint32_t((MT == 1 ? buf * BN : region * BN) + col_base) + (uint32_t(quad * 32) << 16);
 #pragma unroll 1
         for (int c = 0; c < kCols / 32; ++c) {
           uint32_t r[32];
@@ -657,7 +675,7 @@ __device__ __forceinline__ void crt_epilogue(uint32_t tmem_base, uint64_t* tfull
         tc_fence_before();
         acc_release<PAIR>(&tempty[buf]);
         ephase ^= 1u << buf;
-        buf ^= 1;
+        if constexpr (MT == 1) buf ^= 1;  // two accumulators alternate; MT = 2 fills the TMEM
       }
     }
   }
@@ -725,11 +743,12 @@ __device__ __forceinline__ void bf16_epilogue(uint32_t tmem_base, uint64_t* tful
 }
 
 // ------------------------------------------------------------------ kernel
-template <int MODE, int BN, int STAGES, int NW, bool PAIR>
+template <int MODE, int BN, int STAGES, int NW, bool PAIR, int MT = 1>
 __global__ void __launch_bounds__(64 + 32 * NW, 1)
     slice_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const SliceGemmParams P) {
-  using L = SliceLayout<BN, STAGES, PAIR>;
+  static_assert(MT == 1 || (is_crt_mode(MODE) && !PAIR && MT == 2 && 2 * BN <= 512), "256-row tiles: CRT, one CTA");
+  using L = SliceLayout<BN, STAGES, PAIR, MT>;
   // both CTAs of a pair read the same flag, so they leave together
   if (P.skip_if_flag && *P.skip_if_flag) return;
 
@@ -783,15 +802,15 @@ __global__ void __launch_bounds__(64 + 32 * NW, 1)
   const uint32_t tmem_base = *tmem_holder;
 
   if (warp == 0) {
-    if (lane == 0) slice_producer<MODE, BN, STAGES, PAIR>(&tmA, &tmB, smem, full, empty, abort_flag, P, rank);
+    if (lane == 0) slice_producer<MODE, BN, STAGES, PAIR, MT>(&tmA, &tmB, smem, full, empty, abort_flag, P, rank);
   } else if (warp == 1) {
     if (lane == 0 && rank == 0)
-      slice_mma<MODE, BN, STAGES, PAIR>(smem, full, empty, tfull, tempty, drain, tmem_base, abort_flag, P);
+      slice_mma<MODE, BN, STAGES, PAIR, MT>(smem, full, empty, tfull, tempty, drain, tmem_base, abort_flag, P);
   } else {
     if constexpr (MODE == kModeOzakiI8)
       ozaki_epilogue<BN, NW, PAIR>(tmem_base, tfull, tempty, col_exp, abort_flag, P);
     else if constexpr (is_crt_mode(MODE))
-      crt_epilogue<BN, NW, PAIR, MODE == kModeCrtI8Listed>(tmem_base, tfull, tempty, abort_flag, P);
+      crt_epilogue<BN, NW, PAIR, MODE == kModeCrtI8Listed, MT>(tmem_base, tfull, tempty, abort_flag, P);
     else
       bf16_epilogue<BN, NW, PAIR>(tmem_base, tfull, tempty, abort_flag, P);
   }
@@ -811,11 +830,11 @@ __global__ void __launch_bounds__(64 + 32 * NW, 1)
 }
 
 // Host-side launch: one CTA (or one CTA pair) per SM pair, persistent over the tiles.
-template <int MODE, int BN, int STAGES, int NW, bool PAIR>
+template <int MODE, int BN, int STAGES, int NW, bool PAIR, int MT = 1>
 inline cudaError_t launch_slice_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const SliceGemmParams& P,
                                      int num_sms, cudaStream_t stream) {
-  using L = SliceLayout<BN, STAGES, PAIR>;
-  auto kern = slice_gemm_kernel<MODE, BN, STAGES, NW, PAIR>;
+  using L = SliceLayout<BN, STAGES, PAIR, MT>;
+  auto kern = slice_gemm_kernel<MODE, BN, STAGES, NW, PAIR, MT>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kAlloc);
   if (e != cudaSuccess) return e;
   const int tiles = num_work<MODE == kModeCrtI8Listed>(P);

@@ -57,7 +57,8 @@ SHAPES = [("N", "N", 130, 300, 257), ("T", "N", 64, 64, 1000), ("N", "T", 333, 1
 
 @pytest.mark.parametrize("ta,tb,m,n,k", SHAPES)
 @pytest.mark.parametrize("moduli,tile_n,beta", [(16, 256, 0.0), (16, 512, 0.5), (20, 256, -1.25), (8, 512, 0.0),
-                                                (18, 256, 0.75), (11, 256, 0.25), (15, 512, 0.0)])
+                                                (18, 256, 0.75), (11, 256, 0.25), (15, 512, 0.0), (16, 1024, 0.0),
+                                                (12, 1024, 0.5)])
 def test_crt_bit_exact_vs_oracle_model(ta, tb, m, n, k, moduli, tile_n, beta):
     A, lda, B, ldb, C, ldc = make_operands(m, n, k, ta, tb, pad=3, r=4, seed=m + n + k + moduli)
     eb.set_dgemm_moduli(moduli)
@@ -99,11 +100,14 @@ def test_crt_subnormal_and_huge_rows():
     assert np.all(Cg[2, :n] == 0.0) and np.all(Cg[:m, 3] == 0.0)
 
 
-def test_crt_long_k_accumulates_in_chunks():
-    """K beyond one exact INT32 unit (1023 x 128): the epilogue adds residues mod p."""
+@pytest.mark.parametrize("tile_n", [0, 1024])
+def test_crt_long_k_accumulates_in_chunks(tile_n):
+    """K beyond one exact INT32 unit (1023 x 128): the epilogue adds residues mod p (with the
+    256 x 256 one-CTA tile, whose single accumulator is drained between the chunks)."""
     m, n, k = 3, 2, 1023 * 128 + 300
     A, lda, B, ldb, C, ldc = make_operands(m, n, k, "T", "N", seed=9)
     eb.set_dgemm_tolerance(1.0)
+    eb.set_tile_n(tile_n)
     Cg = C.copy(order="F")
     eb.dgemm("T", "N", m, n, k, 1.0, A, lda, B, ldb, 0.0, Cg, ldc)
     np.testing.assert_array_equal(Cg, _model(A, "T", B, "N", m, n, k, 1.0, 0.0, C, 16))

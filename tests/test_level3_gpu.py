@@ -391,7 +391,7 @@ def test_trsm_alpha_applied_after_the_solve():
 
 
 # ------------------------------------------------------------------ the CRT triangle product
-@pytest.mark.parametrize("tile_n", [256, 512])
+@pytest.mark.parametrize("tile_n", [256, 512, 1024])
 @pytest.mark.parametrize("n,k,uplo,trans,group", [(700, 300, "L", "N", 0), (1024, 512, "U", "T", 0),
                                                   (1500, 257, "U", "N", 3), (2100, 1000, "L", "T", 2)])
 def test_crt_syrk_is_the_triangle_of_the_full_product(tile_n, n, k, uplo, trans, group):

@@ -42,7 +42,7 @@ def _run(dtype, A, lda, B, ldb, C, ldc, m, n, k):
     return got, eb.last_error()
 
 
-@pytest.mark.parametrize("dtype,tile", [("d", 256), ("s", 256), ("s", 128)])
+@pytest.mark.parametrize("dtype,tile", [("d", 256), ("d", 1024), ("s", 256), ("s", 128)])
 def test_short_wait_limit_times_out_and_context_recovers(dtype, tile):
     if dtype == "d":
         eb.set_dgemm_method(eb.METHOD_CRT)
