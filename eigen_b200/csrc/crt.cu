@@ -145,6 +145,30 @@ namespace {
 constexpr uint64_t kInfBitsCrt = 0x7FF0000000000000ull;
 constexpr int kNormRows = 32;
 constexpr int kNormCols = 128;
+constexpr int kNormThreads = 256;
+
+// A ROWS x COLS tile of op(X) (row r, column l at X[r*sr + l*sl], zero outside rows x cols)
+// into shared memory by cp.async: all ROWS*COLS/THREADS copies of a thread are in flight at
+// once without holding registers; consecutive lanes take consecutive addresses along
+// whichever of the two strides is 1.  The caller synchronises the block afterwards.
+template <int ROWS, int COLS, int THREADS>
+__device__ __forceinline__ void load_tile(double (&tile)[ROWS][COLS + 1], const double* __restrict__ X, int64_t r0,
+                                          int64_t l0, int64_t rows, int64_t cols, int64_t sr, int64_t sl) {
+  static_assert((ROWS * COLS) % THREADS == 0, "whole tile per pass");
+  constexpr int kPer = ROWS * COLS / THREADS;
+  const bool rows_contig = (sr == 1);
+#pragma unroll
+  for (int q = 0; q < kPer; ++q) {
+    const int idx = int(threadIdx.x) + q * THREADS;
+    const int rr = rows_contig ? idx % ROWS : idx / COLS;
+    const int ll = rows_contig ? idx / ROWS : idx % COLS;
+    const int64_t r = r0 + rr, l = l0 + ll;
+    const bool valid = r < rows && l < cols;
+    cp_async_elem<8>(smem_u32(&tile[rr][ll]), valid ? X + r * sr + l * sl : X, valid);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+}
 
 // exponent e of a finite nonzero |x| given by its bit pattern: |x| in [2^(e-1), 2^e)
 __device__ __forceinline__ int frexp_exp(unsigned long long mb) {
@@ -169,27 +193,16 @@ __device__ __forceinline__ double scale2(double x, int e) {
 //     S_c = sum over nonzero x of ceil(rn(x'^2) 2^32) + 1, x' = x 2^-e_c (|x'| < 1); the +1
 //     covers the rounding of x'^2 and a product that underflows.
 // Every (row, chunk) record is written by exactly one thread group.
-__global__ void __launch_bounds__(256) crt_scan_norm_kernel(const double* __restrict__ X, int64_t rows, int64_t cols,
+__global__ void __launch_bounds__(kNormThreads) crt_scan_norm_kernel(const double* __restrict__ X, int64_t rows, int64_t cols,
                                                             int64_t sr, int64_t sl, unsigned long long* maxbits,
                                                             int32_t* __restrict__ chunk_e,
                                                             unsigned long long* __restrict__ chunk_s,
                                                             int64_t nchunks, int* nonfinite, double* spread) {
   __shared__ double tile[kNormRows][kNormCols + 1];
+  __shared__ double spread_part[2][kNormThreads / 32];
   const int64_t r0 = int64_t(blockIdx.y) * kNormRows;
   const int64_t l0 = int64_t(blockIdx.x) * kNormCols;
-  const bool rows_contig = (sr == 1);
-  for (int idx = threadIdx.x; idx < kNormRows * kNormCols; idx += blockDim.x) {
-    int rr, ll;
-    if (rows_contig) {
-      rr = idx % kNormRows;
-      ll = idx / kNormRows;
-    } else {
-      ll = idx % kNormCols;
-      rr = idx / kNormCols;
-    }
-    const int64_t r = r0 + rr, l = l0 + ll;
-    tile[rr][ll] = (r < rows && l < cols) ? X[r * sr + l * sl] : 0.0;
-  }
+  load_tile<kNormRows, kNormCols, kNormThreads>(tile, X, r0, l0, rows, cols, sr, sl);
   __syncthreads();
   // 8 threads per row, reduced with shuffles inside each 8-lane group; thread `sub` takes
   // columns sub, sub + 8, ..., so that the 8 lanes of a row read 8 consecutive words of the
@@ -257,9 +270,23 @@ __global__ void __launch_bounds__(256) crt_scan_norm_kernel(const double* __rest
       chunk_spread += __shfl_xor_sync(0xffffffffu, chunk_spread, o);
       chunk_count += __shfl_xor_sync(0xffffffffu, chunk_count, o);
     }
-    if ((threadIdx.x & 31) == 0 && chunk_count > 0.0) {
-      atomicAdd(&spread[0], chunk_spread);
-      atomicAdd(&spread[1], chunk_count);
+    // one atomic pair per block: same-address atomics serialise in L2
+    if ((threadIdx.x & 31) == 0) {
+      spread_part[0][threadIdx.x >> 5] = chunk_spread;
+      spread_part[1][threadIdx.x >> 5] = chunk_count;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double sum = 0.0, count = 0.0;
+#pragma unroll
+      for (int w = 0; w < kNormThreads / 32; ++w) {
+        sum += spread_part[0][w];
+        count += spread_part[1][w];
+      }
+      if (count > 0.0) {
+        atomicAdd(&spread[0], sum);
+        atomicAdd(&spread[1], count);
+      }
     }
   }
 }
@@ -271,25 +298,29 @@ __global__ void __launch_bounds__(256) crt_mu_kernel(const unsigned long long* _
                                                      const int32_t* __restrict__ chunk_e,
                                                      const unsigned long long* __restrict__ chunk_s, int64_t nchunks,
                                                      int64_t rows, int64_t rows_pad, int b, int32_t* __restrict__ mu) {
-  const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (r >= rows_pad) return;
+  // one warp per row: the lanes read consecutive chunk records
+  const int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = int(threadIdx.x & 31);
+  if (r >= rows_pad) return;  // whole warps
   int m = kCrtZeroRow;
   const unsigned long long mb = r < rows ? maxbits[r] : 0ull;
   if (mb != 0 && mb < kInfBitsCrt) {
     const int e = frexp_exp(mb);
     unsigned long long S = 0;
-    for (int64_t c = 0; c < nchunks; ++c) {
+    for (int64_t c = lane; c < nchunks; c += 32) {
       const unsigned long long sc = chunk_s[r * nchunks + c];
       if (sc == 0) continue;
       const int sh = 2 * (e - chunk_e[r * nchunks + c]);
       S += sh >= 64 ? 1ull : ((sc - 1) >> sh) + 1;  // ceil(sc / 2^sh), sc >= 1
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) S += __shfl_xor_sync(0xffffffffu, S, o);  // exact: integer sum
     if (S != 0) {
       const int L = S > 1 ? 64 - __clzll(static_cast<long long>(S - 1)) : 0;
       m = b - (e - 16 + (L + 1) / 2);
     }
   }
-  mu[r] = m;
+  if (lane == 0) mu[r] = m;
 }
 
 // Per-modulus constants: p, floor((2^32 - 1) / p) for mod_small, 2^21, 2^42, 2^63 and 2^32
@@ -343,23 +374,24 @@ __device__ __forceinline__ uint32_t residue_of(const Chunks21& c, const CrtModCo
 constexpr int kSplitRowsCrt = 32;
 constexpr int kSplitColsCrt = 128;
 
-constexpr int kSplitThreadsCrt = 512;  // 16 threads per row, 8 entries each
+constexpr int kSplitThreadsCrt = 512;  // a warp per row (4 entries per lane), 16 rows per pass
+constexpr int kSplitEntries = 4;      // entries (consecutive columns) per thread and row
 
-// The 8 symmetric residues of one thread's entries for one modulus, from 21-bit chunks of
-// |t| < 2^84 (more than 16 moduli), packed into 8 bytes.
-__device__ __forceinline__ void store_residues_wide(const CrtModConst& k, const Chunks21 (&ch)[8], uint32_t neg,
-                                                    int8_t* dst) {
+// The 4 symmetric residues of one thread's entries for one modulus, from 21-bit chunks of
+// |t| < 2^84 (more than 16 moduli), packed into 4 bytes.
+__device__ __forceinline__ void store_residues_wide(const CrtModConst& k, const Chunks21 (&ch)[kSplitEntries],
+                                                    uint32_t neg, int8_t* dst) {
   const int hi = int(k.p >> 1) - ((k.p & 1u) ? 0 : 1);  // largest representative kept as is
-  uint32_t w[2] = {0u, 0u};
+  uint32_t w = 0u;
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
+  for (int j = 0; j < kSplitEntries; ++j) {
     const int res = int(residue_of(ch[j], k));
     int sres = res > hi ? res - int(k.p) : res;  // symmetric residue of |t|: [-(p/2), (p-1)/2]
     // of -|t|: its negation (for p = 256, 128 packs to the same byte as -128)
     if ((neg >> j) & 1u) sres = -sres;
-    w[j >> 2] |= (uint32_t(sres) & 0xFFu) << (8 * (j & 3));
+    w |= (uint32_t(sres) & 0xFFu) << (8 * j);
   }
-  *reinterpret_cast<uint2*>(dst) = make_uint2(w[0], w[1]);
+  *reinterpret_cast<uint32_t*>(dst) = w;
 }
 
 // An entry t = trunc(2^mu x) with |t| <= 2^62 (at most 16 moduli) as hi 2^32 + lo (hi signed,
@@ -397,25 +429,26 @@ __device__ __forceinline__ uint32_t pack_low_bytes(uint32_t a, uint32_t b, uint3
   return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
 
-// The 8 symmetric residues of one thread's entries for one modulus, packed into 8 bytes.  For
+// The 4 symmetric residues of one thread's entries for one modulus, packed into 4 bytes.  For
 // p = 256 the residue of t is its low byte read as int8 (the representative in [-128, 127]).
-__device__ __forceinline__ void store_residues(const CrtModConst& k, const SplitEntry (&e)[8], int8_t* dst) {
-  uint32_t r[8];
+__device__ __forceinline__ void store_residues(const CrtModConst& k, const SplitEntry (&e)[kSplitEntries],
+                                               int8_t* dst) {
+  uint32_t r[kSplitEntries];
   if ((k.p & (k.p - 1u)) == 0u) {
 #pragma unroll
-    for (int j = 0; j < 8; ++j) r[j] = e[j].lo;
+    for (int j = 0; j < kSplitEntries; ++j) r[j] = e[j].lo;
   } else {
     const double c32d = double(k.c32);
 #pragma unroll
-    for (int j = 0; j < 8; ++j) r[j] = symmetric_residue(e[j], k, c32d);
+    for (int j = 0; j < kSplitEntries; ++j) r[j] = symmetric_residue(e[j], k, c32d);
   }
-  *reinterpret_cast<uint2*>(dst) =
-      make_uint2(pack_low_bytes(r[0], r[1], r[2], r[3]), pack_low_bytes(r[4], r[5], r[6], r[7]));
+  *reinterpret_cast<uint32_t*>(dst) = pack_low_bytes(r[0], r[1], r[2], r[3]);
 }
 
 // Moduli L .. NT-1 with their constants as compile-time immediates.
 template <int L, int NT>
-__device__ __forceinline__ void store_residues_static(const SplitEntry (&e)[8], int8_t* dst, size_t plane) {
+__device__ __forceinline__ void store_residues_static(const SplitEntry (&e)[kSplitEntries], int8_t* dst,
+                                                      size_t plane) {
   if constexpr (L < NT) {
     constexpr CrtModConst k = crt_mod_const(L);
     store_residues(k, e, dst + size_t(L) * plane);
@@ -426,58 +459,50 @@ __device__ __forceinline__ void store_residues_static(const SplitEntry (&e)[8], 
 // Residues of A' = trunc(2^mu_r x) for moduli [0, n): plane l at residues + l*rows_pad*k_pad,
 // row r contiguous along k; symmetric int8 representatives (mu from crt_mu_kernel).
 // NT > 0: the modulus count is NT (constants as immediates); NT = 0: n, read at run time.
-// Two blocks per SM (64 registers, a few bytes spilled) run faster than one block with the
-// 84 registers the compiler would take otherwise.
+// A 32 x 128 tile per block: each warp takes a row at a time, four consecutive entries per
+// lane, so that every modulus plane receives 128 contiguous bytes per warp store.
 template <bool kWide, int NT>  // kWide: |t| may reach 2^63 (more than 16 moduli)
 __global__ void __launch_bounds__(kSplitThreadsCrt, 2) crt_split_kernel(
     const double* __restrict__ X, int64_t rows, int64_t cols, int64_t sr, int64_t sl,
     const int32_t* __restrict__ mu, int n, int8_t* __restrict__ residues, int64_t rows_pad, int64_t k_pad) {
+  static_assert(kSplitColsCrt == 32 * kSplitEntries, "a warp per tile row");
   __shared__ double tile[kSplitRowsCrt][kSplitColsCrt + 1];
   __shared__ int row_mu_s[kSplitRowsCrt];
   const int64_t r0 = int64_t(blockIdx.y) * kSplitRowsCrt;
   const int64_t l0 = int64_t(blockIdx.x) * kSplitColsCrt;
-  const bool rows_contig = (sr == 1);
   if (threadIdx.x < kSplitRowsCrt) {
     const int64_t r = r0 + threadIdx.x;
     row_mu_s[threadIdx.x] = mu[r];
   }
-  for (int idx = threadIdx.x; idx < kSplitRowsCrt * kSplitColsCrt; idx += blockDim.x) {
-    int rr, ll;
-    if (rows_contig) {
-      rr = idx % kSplitRowsCrt;
-      ll = idx / kSplitRowsCrt;
-    } else {
-      ll = idx % kSplitColsCrt;
-      rr = idx / kSplitColsCrt;
-    }
-    const int64_t r = r0 + rr, l = l0 + ll;
-    tile[rr][ll] = (r < rows && l < cols) ? X[r * sr + l * sl] : 0.0;
-  }
+  load_tile<kSplitRowsCrt, kSplitColsCrt, kSplitThreadsCrt>(tile, X, r0, l0, rows, cols, sr, sl);
   __syncthreads();
-  const int rr = threadIdx.x >> 4;
-  const int cb = (threadIdx.x & 15) * 8;
-  const int m = row_mu_s[rr];
-  int8_t* dst = residues + (size_t(r0 + rr)) * size_t(k_pad) + size_t(l0 + cb);
+  const int cb = int(threadIdx.x & 31) * kSplitEntries;
   const size_t plane = size_t(rows_pad) * size_t(k_pad);
-  if constexpr (kWide) {
-    Chunks21 ch[8];
-    uint32_t neg = 0;
+  constexpr int kRowsPerPass = kSplitThreadsCrt / 32;
+#pragma unroll 1
+  for (int rr = int(threadIdx.x >> 5); rr < kSplitRowsCrt; rr += kRowsPerPass) {
+    const int m = row_mu_s[rr];
+    int8_t* dst = residues + (size_t(r0 + rr)) * size_t(k_pad) + size_t(l0 + cb);
+    if constexpr (kWide) {
+      Chunks21 ch[kSplitEntries];
+      uint32_t neg = 0;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      // |v| <= 2^b, an exact integer (0 in zero rows: 2^kCrtZeroRow underflows to 0)
-      const double v = trunc(scale2(tile[rr][cb + j], m));
-      ch[j] = chunks21(fabs(v));
-      neg |= (v < 0.0 ? 1u : 0u) << j;
-    }
-    for (int l = 0; l < n; ++l) store_residues_wide(kModConst[l], ch, neg, dst + size_t(l) * plane);
-  } else {
-    SplitEntry e[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) e[j] = split_entry(__double2ll_rz(scale2(tile[rr][cb + j], m)));  // trunc
-    if constexpr (NT > 0) {
-      store_residues_static<0, NT>(e, dst, plane);
+      for (int j = 0; j < kSplitEntries; ++j) {
+        // |v| <= 2^b, an exact integer (0 in zero rows: 2^kCrtZeroRow underflows to 0)
+        const double v = trunc(scale2(tile[rr][cb + j], m));
+        ch[j] = chunks21(fabs(v));
+        neg |= (v < 0.0 ? 1u : 0u) << j;
+      }
+      for (int l = 0; l < n; ++l) store_residues_wide(kModConst[l], ch, neg, dst + size_t(l) * plane);
     } else {
-      for (int l = 0; l < n; ++l) store_residues(kModConst[l], e, dst + size_t(l) * plane);
+      SplitEntry e[kSplitEntries];
+#pragma unroll
+      for (int j = 0; j < kSplitEntries; ++j) e[j] = split_entry(__double2ll_rz(scale2(tile[rr][cb + j], m)));  // trunc
+      if constexpr (NT > 0) {
+        store_residues_static<0, NT>(e, dst, plane);
+      } else {
+        for (int l = 0; l < n; ++l) store_residues(kModConst[l], e, dst + size_t(l) * plane);
+      }
     }
   }
 }
@@ -545,6 +570,8 @@ __host__ __device__ constexpr CrtTable make_crt_table() {
   return t;
 }
 __constant__ CrtTable kCrtTable = make_crt_table();
+// the same table as a compile-time value, for constants folded into instructions
+constexpr CrtTable kCrtTableC = make_crt_table();
 
 // Moduli 2g and 2g+1 share the factor Q_g = P / (p_2g p_2g+1) of their weights:
 // W_2g = Q_g X_2g and W_2g+1 = Q_g X_2g+1 with X_2g = p_2g+1 ((P/p_2g)^-1 mod p_2g) and
@@ -603,6 +630,7 @@ struct CrtRecParams {
   double* save;
   int64_t ld_save;
   int cols_per_block;  // columns one block handles per pass (fewer when the grid would be small)
+  int vec_store;       // C 16-byte aligned with an even ldc (the save array likewise)
   int uplo;            // 0: all of C; 1: i <= j only; 2: i >= j only
 };
 
@@ -660,14 +688,25 @@ __device__ __forceinline__ CrtStoreCtx store_ctx(const CrtRecParams& R) {
                      R.ld_save, R.mu_a, R.mu_b, R.b, R.write_c != 0, R.err_sq != nullptr};
 }
 
-// C_ij from RN(C'_ij) = d 2^shift (signed d): scale by 2^-(mu_i + nu_j), apply alpha and
-// beta, and add the estimate terms: e += 2^(2(b - mu_i - nu_j)) (the squared truncation
-// error bound, up to the factor 2/3 alpha^2 applied per block), v += (alpha C')^2.
-__device__ __forceinline__ void crt_store(const CrtStoreCtx& S, int64_t i, int64_t j, double d, int shift,
-                                          double& e_acc, double& v_acc) {
-  const int mu_i = S.mu_a[i], nu_j = S.mu_b[j];
+// alpha C_ij from RN(C'_ij) = d 2^shift (signed d): scaled by 2^-(mu_i + nu_j); with the
+// estimate, e += 2^(2(b - mu_i - nu_j)) (the squared truncation error bound, up to the factor
+// 2/3 alpha^2 applied per block) and v += (alpha C')^2.
+__device__ __forceinline__ double crt_value(const CrtStoreCtx& S, int mu_i, int nu_j, double d, int shift,
+                                            double& e_acc, double& v_acc) {
   const double val = d != 0.0 ? scale_exp(d, shift - mu_i - nu_j) : 0.0;  // d = 0 in zero rows
   const double v = __dmul_rn(S.alpha, val);
+  if (S.estimate) {
+    // truncation errors need a nonzero row on both sides
+    if (mu_i != kCrtZeroRow && nu_j != kCrtZeroRow) e_acc += exp2_int(2 * (S.b - mu_i - nu_j));
+    v_acc += v * v;
+  }
+  return v;
+}
+
+// C_ij = alpha C_ij' (+ beta C_ij, the old value kept in `save` when there is one)
+__device__ __forceinline__ void crt_store(const CrtStoreCtx& S, int64_t i, int64_t j, double d, int shift,
+                                          double& e_acc, double& v_acc) {
+  const double v = crt_value(S, S.mu_a[i], S.mu_b[j], d, shift, e_acc, v_acc);
   if (S.write_c) {
     double* c = S.C + j * S.ldc + i;
     if (S.beta == 0.0) {
@@ -677,11 +716,6 @@ __device__ __forceinline__ void crt_store(const CrtStoreCtx& S, int64_t i, int64
       if (S.save) S.save[j * S.ld_save + i] = old;
       *c = __fma_rn(S.beta, old, v);
     }
-  }
-  if (S.estimate) {
-    // truncation errors need a nonzero row on both sides
-    if (mu_i != kCrtZeroRow && nu_j != kCrtZeroRow) e_acc += exp2_int(2 * (S.b - mu_i - nu_j));
-    v_acc += v * v;
   }
 }
 
@@ -798,6 +832,55 @@ __global__ void __launch_bounds__(256) crt_reconstruct_kernel(const __grid_const
   if (R.err_sq) crt_reduce_energies(R, e_acc, v_acc);
 }
 
+// C' from the residues rc[0..N) of one entry (N <= 16): RN(|C'|) = d 2^shift, returns the
+// sign.  S = sum_g Q_g R_g, then R = S - q P with q = rint(S / P) and a range fix, exact in
+// 128-bit two's complement.
+template <int N>
+__device__ __forceinline__ bool crt_combine128(const uint32_t (&rc)[N], double P_inv, double& d, int& shift) {
+  using u128 = unsigned __int128;
+  using s128 = __int128;
+  const u128 P = (u128(kCrtTable.P[N][3]) << 96) | (u128(kCrtTable.P[N][2]) << 64) | (u128(kCrtTable.P[N][1]) << 32) |
+                 u128(kCrtTable.P[N][0]);
+  const s128 half = s128(P >> 1);
+  // S = sum_g Q_g R_g in four 32-bit limb columns (each < 8 * 2^25 * 2^32 = 2^60); S itself
+  // (< 2^28 P) may pass 2^128, and the 128-bit arithmetic below works modulo 2^128, which
+  // leaves the small remainder S - q P exact
+  unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
+#pragma unroll
+  for (int g = 0; 2 * g < N; ++g) {
+    uint32_t Rg = rc[2 * g] * kCrtPairs.X[N][2 * g];
+    if (2 * g + 1 < N) Rg += rc[2 * g + 1] * kCrtPairs.X[N][2 * g + 1];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] += static_cast<unsigned long long>(Rg) * kCrtPairs.Q[N][g][q];
+  }
+  // q = rint(S / P) from the partial sums in FP64; it may be off by one near a
+  // half-integer, which the range fix below absorbs
+  const double sd =
+      fma(double(acc[3]), 0x1p96, fma(double(acc[2]), 0x1p64, fma(double(acc[1]), 0x1p32, double(acc[0]))));
+  const u128 q = u128(static_cast<unsigned long long>(rint(sd * P_inv)));
+  const u128 S = u128(acc[0]) + (u128(acc[1]) << 32) + (u128(acc[2]) << 64) + (u128(acc[3]) << 96);
+  s128 r = s128(S - q * P);
+  if (r > half)
+    r -= s128(P);
+  else if (r < -half)
+    r += s128(P);
+  const bool negative = r < 0;
+  const u128 mag = negative ? u128(-r) : u128(r);
+  const unsigned long long hi = static_cast<unsigned long long>(mag >> 64);
+  const unsigned long long lo = static_cast<unsigned long long>(mag);
+  shift = 0;
+  if (hi == 0) {
+    d = __ull2double_rn(lo);
+  } else {  // top 64 bits and a sticky bit: one correct rounding
+    const int lz = __clzll(static_cast<long long>(hi));
+    const unsigned long long u = lz ? (hi << lz) | (lo >> (64 - lz)) : hi;
+    const unsigned long long sticky = (lo << lz) != 0ull ? 1ull : 0ull;
+    d = __ull2double_rn(u | sticky);
+    shift = 64 - lz;
+  }
+  return negative;
+}
+
 // The same for N <= 16 moduli, N a template parameter: P < 2^126, so W_l fits four limbs,
 // S = sum r_l W_l is known modulo 2^128, and R = S - q P (|R| < 1.5 P < 2^127) is exact in
 // 128-bit two's complement.  W_l, P and P/2 come from the compile-time table.  Bit for bit
@@ -806,8 +889,6 @@ __global__ void __launch_bounds__(256) crt_reconstruct_kernel(const __grid_const
 template <int N, bool EST>
 __global__ void __launch_bounds__(256, 4) crt_reconstruct128_kernel(const __grid_constant__ CrtRecParams R) {
   static_assert(N >= 1 && N <= 16, "128-bit path");
-  using u128 = unsigned __int128;
-  using s128 = __int128;
   if (R.skip_if_flag && *R.skip_if_flag) return;
   CrtStoreCtx sc = store_ctx(R);
   sc.estimate = EST;  // compiled separately with and without the estimate
@@ -816,9 +897,6 @@ __global__ void __launch_bounds__(256, 4) crt_reconstruct128_kernel(const __grid
   const double P_inv = R.P_inv;
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double e_acc = 0.0, v_acc = 0.0;
-  const u128 P = (u128(kCrtTable.P[N][3]) << 96) | (u128(kCrtTable.P[N][2]) << 64) | (u128(kCrtTable.P[N][1]) << 32) |
-                 u128(kCrtTable.P[N][0]);
-  const s128 half = s128(P >> 1);
   const int cpb = R.cols_per_block;
   const int64_t jstep = int64_t(gridDim.y) * cpb;
   for (int64_t j0 = int64_t(blockIdx.y) * cpb; i < m && j0 < ncols; j0 += jstep) {
@@ -837,44 +915,256 @@ __global__ void __launch_bounds__(256, 4) crt_reconstruct128_kernel(const __grid
 #pragma unroll
         for (int l = 0; l < N; ++l) rn[l] = res[(j + 1) * ld_res + i + l * plane];
       }
-      // S = sum_g Q_g R_g in four 32-bit limb columns (each < 8 * 2^25 * 2^32 = 2^60); S itself
-      // (< 2^28 P) may pass 2^128, and the 128-bit arithmetic below works modulo 2^128, which
-      // leaves the small remainder S - q P exact
-      unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
-#pragma unroll
-      for (int g = 0; 2 * g < N; ++g) {
-        uint32_t Rg = rc[2 * g] * kCrtPairs.X[N][2 * g];
-        if (2 * g + 1 < N) Rg += rc[2 * g + 1] * kCrtPairs.X[N][2 * g + 1];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[q] += static_cast<unsigned long long>(Rg) * kCrtPairs.Q[N][g][q];
-      }
-      // q = rint(S / P) from the partial sums in FP64; it may be off by one near a
-      // half-integer, which the range fix below absorbs
-      const double sd =
-          fma(double(acc[3]), 0x1p96, fma(double(acc[2]), 0x1p64, fma(double(acc[1]), 0x1p32, double(acc[0]))));
-      const u128 q = u128(static_cast<unsigned long long>(rint(sd * P_inv)));
-      const u128 S = u128(acc[0]) + (u128(acc[1]) << 32) + (u128(acc[2]) << 64) + (u128(acc[3]) << 96);
-      s128 r = s128(S - q * P);
-      if (r > half)
-        r -= s128(P);
-      else if (r < -half)
-        r += s128(P);
-      const bool negative = r < 0;
-      const u128 mag = negative ? u128(-r) : u128(r);
-      const unsigned long long hi = static_cast<unsigned long long>(mag >> 64);
-      const unsigned long long lo = static_cast<unsigned long long>(mag);
       double d;
-      int shift = 0;
-      if (hi == 0) {
-        d = __ull2double_rn(lo);
-      } else {  // top 64 bits and a sticky bit: one correct rounding
-        const int lz = __clzll(static_cast<long long>(hi));
-        const unsigned long long u = lz ? (hi << lz) | (lo >> (64 - lz)) : hi;
-        const unsigned long long sticky = (lo << lz) != 0ull ? 1ull : 0ull;
-        d = __ull2double_rn(u | sticky);
-        shift = 64 - lz;
-      }
+      int shift;
+      const bool negative = crt_combine128<N>(rc, P_inv, d, shift);
       crt_store(sc, i, j, negative ? -d : d, shift, e_acc, v_acc);
+    }
+  }
+  if (EST) crt_reduce_energies(R, e_acc, v_acc);
+}
+
+// The exact double of a 32-bit unsigned integer without a conversion instruction: the word
+// under the exponent of 2^52, minus 2^52.
+__device__ __forceinline__ double u32_to_double(uint32_t x) { return __hiloint2double(0x43300000, int(x)) - 0x1p52; }
+
+// RN(C'_ij 2^escale) from the residues rc[0..N) of one entry (8 <= N <= 16), in 32-bit limbs:
+//   * S = sum_g Q_g R_g as four 64-bit limb columns, carried into S mod 2^128 and the part
+//     above 2^128;
+//   * q = rint(S / P) from the bits of S above 2^32 in FP64 (off by one at most, near a
+//     half-integer), R = S - q P modulo 2^128 with signed 64-bit borrows, and the range fix
+//     only when R's top limbs do not already place it in [-P/2, P/2);
+//   * the magnitude rounded to nearest even from its top 64 bits and a sticky bit, written
+//     straight into the bits of the scaled double when that is a normal number (scaling by
+//     2^escale is then exact).  Subnormal and overflowing results take the per-row kernel's
+//     steps (RN of the top 64 bits, then scale_exp), so every result is bit for bit that
+//     kernel's.
+template <int N>
+__device__ __forceinline__ double crt_entry_fast(const uint32_t (&rc)[N], double P_inv32, int escale) {
+  static_assert(N >= kCrtMinModuli && N <= 16, "P at least 2^63 and below 2^128");
+  unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
+#pragma unroll
+  for (int g = 0; 2 * g < N; ++g) {
+    uint32_t Rg = rc[2 * g] * kCrtPairs.X[N][2 * g];
+    if (2 * g + 1 < N) Rg += rc[2 * g + 1] * kCrtPairs.X[N][2 * g + 1];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] += static_cast<unsigned long long>(Rg) * kCrtPairs.Q[N][g][q];
+  }
+  // S = top 2^128 + s3 2^96 + s2 2^64 + s1 2^32 + s0
+  const uint32_t s0 = uint32_t(acc[0]);
+  const unsigned long long t1 = acc[1] + (acc[0] >> 32);
+  const unsigned long long t2 = acc[2] + (t1 >> 32);
+  const unsigned long long t3 = acc[3] + (t2 >> 32);
+  const uint32_t s1 = uint32_t(t1), s2 = uint32_t(t2), s3 = uint32_t(t3), top = uint32_t(t3 >> 32);
+  // S / 2^32 in FP64 (s0 < 2^32 <= 2^-31 P left out), then q in the low word of
+  // rint(S / P) + 1.5 2^52 (0 <= q < 2^31)
+  const double hi = fma(u32_to_double(top), 0x1p32, u32_to_double(s3));
+  const double mid = fma(hi, 0x1p32, u32_to_double(s2));
+  const double sd = fma(mid, 0x1p32, u32_to_double(s1));
+  const uint32_t q = uint32_t(__double2loint(fma(sd, P_inv32, 0x1.8p52)));
+  // R = S - q P modulo 2^128
+  constexpr uint32_t P0 = kCrtTableC.P[N][0], P1 = kCrtTableC.P[N][1], P2 = kCrtTableC.P[N][2], P3 = kCrtTableC.P[N][3];
+  long long d = static_cast<long long>(s0) - static_cast<long long>(static_cast<unsigned long long>(q) * P0);
+  uint32_t r0 = uint32_t(d);
+  d = (d >> 32) + static_cast<long long>(s1) - static_cast<long long>(static_cast<unsigned long long>(q) * P1);
+  uint32_t r1 = uint32_t(d);
+  d = (d >> 32) + static_cast<long long>(s2) - static_cast<long long>(static_cast<unsigned long long>(q) * P2);
+  uint32_t r2 = uint32_t(d);
+  d = (d >> 32) + static_cast<long long>(s3) - static_cast<long long>(static_cast<unsigned long long>(q) * P3);
+  uint32_t r3 = uint32_t(d);
+  // R lies in [-half, half) when the 64-bit window of R at half's two top limbs is in
+  // [-Hw, Hw) and the limbs above the window extend its sign: nothing to fix then
+  constexpr int kW = kCrtTableC.half[N][3] != 0 ? 2 : (kCrtTableC.half[N][2] != 0 ? 1 : 0);
+  constexpr long long Hw = static_cast<long long>((static_cast<unsigned long long>(kCrtTableC.half[N][kW + 1]) << 32) |
+                                                  kCrtTableC.half[N][kW]);
+  const uint32_t rl[4] = {r0, r1, r2, r3};
+  const long long win = static_cast<long long>((static_cast<unsigned long long>(rl[kW + 1]) << 32) | rl[kW]);
+  const uint32_t ext = win < 0 ? 0xFFFFFFFFu : 0u;
+  bool in_range = win >= -Hw && win < Hw;
+#pragma unroll
+  for (int t = kW + 2; t < 4; ++t) in_range = in_range && rl[t] == ext;
+  if (!in_range) {
+    using u128 = unsigned __int128;
+    using s128 = __int128;
+    const u128 P = (u128(P3) << 96) | (u128(P2) << 64) | (u128(P1) << 32) | u128(P0);
+    const s128 half = s128(P >> 1);
+    s128 r = s128((u128(r3) << 96) | (u128(r2) << 64) | (u128(r1) << 32) | u128(r0));
+    if (r > half)
+      r -= s128(P);
+    else if (r < -half)
+      r += s128(P);
+    const u128 ur = u128(r);
+    r0 = uint32_t(ur);
+    r1 = uint32_t(ur >> 32);
+    r2 = uint32_t(ur >> 64);
+    r3 = uint32_t(ur >> 96);
+  }
+  const bool negative = int(r3) < 0;
+  // |R| = (hi64, lo64)
+  unsigned long long lo64 = (static_cast<unsigned long long>(r1) << 32) | r0;
+  unsigned long long hi64 = (static_cast<unsigned long long>(r3) << 32) | r2;
+  if (negative) {
+    lo64 = ~lo64 + 1ull;
+    hi64 = ~hi64 + (lo64 == 0ull ? 1ull : 0ull);
+  }
+  if ((hi64 | lo64) == 0ull) return 0.0;
+  // top 64 bits u (leading one at bit 63), bit length L, sticky for the bits below u
+  int L;
+  unsigned long long u;
+  bool sticky;
+  if (hi64 != 0ull) {
+    const int lz = __clzll(static_cast<long long>(hi64));
+    u = lz ? (hi64 << lz) | (lo64 >> (64 - lz)) : hi64;
+    sticky = (lo64 << lz) != 0ull;
+    L = 128 - lz;
+  } else {
+    const int lz = __clzll(static_cast<long long>(lo64));
+    u = lo64 << lz;
+    sticky = false;
+    L = 64 - lz;
+  }
+  const int E = L - 1 + escale;  // exponent of the scaled magnitude before rounding
+  if (E < -1022 || E > 1023) {
+    // the per-row kernel's two steps: RN(|R|) = d 2^shift, then scale_exp
+    double dd;
+    int shift;
+    if (hi64 == 0ull) {
+      dd = __ull2double_rn(lo64);
+      shift = 0;
+    } else {
+      const int lz = __clzll(static_cast<long long>(hi64));
+      const unsigned long long uu = lz ? (hi64 << lz) | (lo64 >> (64 - lz)) : hi64;
+      dd = __ull2double_rn(uu | ((lo64 << lz) != 0ull ? 1ull : 0ull));
+      shift = 64 - lz;
+    }
+    const double v = scale_exp(dd, shift + escale);
+    return negative ? -v : v;
+  }
+  // round the 53-bit significand to nearest even; a carry out of it moves into the exponent
+  unsigned long long mant = u >> 11;
+  const bool round_bit = ((u >> 10) & 1ull) != 0ull;
+  const bool rest = (u & 0x3FFull) != 0ull || sticky;
+  mant += (round_bit && (rest || (mant & 1ull))) ? 1ull : 0ull;
+  const unsigned long long bits =
+      (static_cast<unsigned long long>(E + 1022) << 52) + mant + (negative ? 0x8000000000000000ull : 0ull);
+  return __longlong_as_double(static_cast<long long>(bits));
+}
+
+// The same, four consecutive rows per thread: one 32-bit load per modulus and column brings
+// the residues of rows i0 .. i0+3 (a warp reads 128 contiguous bytes of a residue plane), the
+// row scales stay in registers across the columns, the entries go through crt_entry_fast,
+// the estimate's exponent terms are summed once per group of four rows, and interior groups
+// store C (and read the old C) as two 16-byte vectors.  Needs the residue base, ld_res and the
+// plane size to be multiples of 4 and ld_res >= m rounded up to 4 (the launcher checks).  Bit
+// for bit the per-row kernel; only the order of the estimate's partial sums differs.
+constexpr int kRecRowsPerThread = 4;
+template <int N, bool EST>
+__global__ void __launch_bounds__(256, 2) crt_reconstruct128x4_kernel(const __grid_constant__ CrtRecParams R) {
+  if (R.skip_if_flag && *R.skip_if_flag) return;
+  CrtStoreCtx sc = store_ctx(R);
+  sc.estimate = EST;
+  const uint8_t* const res = R.res;
+  const int64_t ld_res = R.ld_res, plane = R.plane, m = R.m, ncols = R.ncols;
+  const int uplo = R.uplo;
+  const bool vec = R.vec_store != 0;
+  const double P_inv32 = R.P_inv * 0x1p32;
+  const int64_t i0 = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) * kRecRowsPerThread;
+  double e_acc = 0.0, v_acc = 0.0;
+  int mu_i[kRecRowsPerThread];
+#pragma unroll
+  for (int q = 0; q < kRecRowsPerThread; ++q) mu_i[q] = i0 + q < m ? sc.mu_a[i0 + q] : kCrtZeroRow;
+  // estimate: sum_q 2^(2(b - mu_q - nu_j)) = rowsum 2^(2(T - nu_j)) over the nonzero rows of
+  // the group, T the largest b - mu_q (every term of rowsum at most 1)
+  int T = -0x40000000;
+  double rowsum = 0.0;
+  if (EST) {
+#pragma unroll
+    for (int q = 0; q < kRecRowsPerThread; ++q)
+      if (mu_i[q] != kCrtZeroRow) T = max(T, sc.b - mu_i[q]);
+#pragma unroll
+    for (int q = 0; q < kRecRowsPerThread; ++q)
+      if (mu_i[q] != kCrtZeroRow) rowsum += exp2_int(2 * (sc.b - mu_i[q] - T));
+  }
+  const int cpb = R.cols_per_block;
+  const int64_t jstep = int64_t(gridDim.y) * cpb;
+  for (int64_t j0 = int64_t(blockIdx.y) * cpb; i0 < m && j0 < ncols; j0 += jstep) {
+    // the columns that some row of the group keeps
+    int64_t jb = j0, j1 = j0 + cpb < ncols ? j0 + cpb : ncols;
+    if (uplo == 1 && jb < i0) jb = i0;                                          // i <= j
+    if (uplo == 2 && j1 > i0 + kRecRowsPerThread) j1 = i0 + kRecRowsPerThread;  // i >= j
+    if (jb >= j1) continue;
+    uint32_t wn[N];
+#pragma unroll
+    for (int l = 0; l < N; ++l) wn[l] = __ldg(reinterpret_cast<const uint32_t*>(res + jb * ld_res + i0 + l * plane));
+    for (int64_t j = jb; j < j1; ++j) {
+      uint32_t wc[N];
+#pragma unroll
+      for (int l = 0; l < N; ++l) wc[l] = wn[l];
+      if (j + 1 < j1) {
+#pragma unroll
+        for (int l = 0; l < N; ++l)
+          wn[l] = __ldg(reinterpret_cast<const uint32_t*>(res + (j + 1) * ld_res + i0 + l * plane));
+      }
+      const int nu_j = sc.mu_b[j];
+      double v[kRecRowsPerThread];
+      bool all = true;
+      uint32_t keep = 0;
+#pragma unroll
+      for (int q = 0; q < kRecRowsPerThread; ++q) {
+        const int64_t i = i0 + q;
+        const bool k = i < m && (uplo == 0 || (uplo == 1 ? i <= j : i >= j));
+        all = all && k;
+        v[q] = 0.0;
+        if (k) {
+          keep |= 1u << q;
+          uint32_t rc[N];
+#pragma unroll
+          for (int l = 0; l < N; ++l) rc[l] = (wc[l] >> (8 * q)) & 0xFFu;
+          v[q] = __dmul_rn(sc.alpha, crt_entry_fast<N>(rc, P_inv32, -mu_i[q] - nu_j));
+          if (EST) v_acc += v[q] * v[q];
+        }
+      }
+      if (EST && nu_j != kCrtZeroRow) {
+        if (all) {
+          if (rowsum != 0.0) e_acc += rowsum * exp2_int(2 * (T - nu_j));
+        } else {
+#pragma unroll
+          for (int q = 0; q < kRecRowsPerThread; ++q)
+            if (((keep >> q) & 1u) && mu_i[q] != kCrtZeroRow) e_acc += exp2_int(2 * (sc.b - mu_i[q] - nu_j));
+        }
+      }
+      if (!sc.write_c) continue;
+      double* c = sc.C + j * sc.ldc + i0;
+      if (all && vec) {
+        double2* c2 = reinterpret_cast<double2*>(c);
+        if (sc.beta == 0.0) {
+          c2[0] = make_double2(v[0], v[1]);
+          c2[1] = make_double2(v[2], v[3]);
+        } else {
+          const double2 o0 = c2[0], o1 = c2[1];
+          if (sc.save) {
+            double* s = sc.save + j * sc.ld_save + i0;
+            s[0] = o0.x;
+            s[1] = o0.y;
+            s[2] = o1.x;
+            s[3] = o1.y;
+          }
+          c2[0] = make_double2(__fma_rn(sc.beta, o0.x, v[0]), __fma_rn(sc.beta, o0.y, v[1]));
+          c2[1] = make_double2(__fma_rn(sc.beta, o1.x, v[2]), __fma_rn(sc.beta, o1.y, v[3]));
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < kRecRowsPerThread; ++q) {
+          if (!((keep >> q) & 1u)) continue;
+          if (sc.beta == 0.0) {
+            c[q] = v[q];
+          } else {
+            const double old = c[q];
+            if (sc.save) sc.save[j * sc.ld_save + i0 + q] = old;
+            c[q] = __fma_rn(sc.beta, old, v[q]);
+          }
+        }
+      }
     }
   }
   if (EST) crt_reduce_energies(R, e_acc, v_acc);
@@ -906,7 +1196,16 @@ __global__ void __launch_bounds__(256) crt_merge_splits_kernel(uint8_t* __restri
 }
 
 template <int N>
-void launch_rec128(bool est, dim3 grid, cudaStream_t stream, const CrtRecParams& R) {
+void launch_rec128(bool est, bool x4, dim3 grid, cudaStream_t stream, const CrtRecParams& R) {
+  if constexpr (N >= kCrtMinModuli) {
+    if (x4) {
+      if (est)
+        crt_reconstruct128x4_kernel<N, true><<<grid, 256, 0, stream>>>(R);
+      else
+        crt_reconstruct128x4_kernel<N, false><<<grid, 256, 0, stream>>>(R);
+      return;
+    }
+  }
   if (est)
     crt_reconstruct128_kernel<N, true><<<grid, 256, 0, stream>>>(R);
   else
@@ -988,7 +1287,7 @@ cudaError_t launch_crt_scan_norms(const StridedView<double>& x, const CrtOperand
   if (op.k_pad % kNormCols != 0) return cudaErrorInvalidValue;
   dim3 grid(unsigned((x.cols + kNormCols - 1) / kNormCols), unsigned((x.rows + kNormRows - 1) / kNormRows));
   if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
-  crt_scan_norm_kernel<<<grid, 256, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl,
+  crt_scan_norm_kernel<<<grid, kNormThreads, 0, stream>>>(x.ptr, x.rows, x.cols, x.sr, x.sl,
                                                  reinterpret_cast<unsigned long long*>(op.maxbits), op.chunk_e,
                                                  reinterpret_cast<unsigned long long*>(op.chunk_s),
                                                  op.k_pad / kNormCols, nonfinite, spread);
@@ -1001,7 +1300,7 @@ cudaError_t launch_crt_split(const StridedView<double>& x, const CrtOperand& op,
   dim3 grid(unsigned(op.k_pad / kSplitColsCrt), unsigned(op.rows_pad / kSplitRowsCrt));
   if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
   const int b = crt_bits(moduli);
-  crt_mu_kernel<<<unsigned((op.rows_pad + 255) / 256), 256, 0, stream>>>(
+  crt_mu_kernel<<<unsigned((op.rows_pad + 7) / 8), 256, 0, stream>>>(
       reinterpret_cast<const unsigned long long*>(op.maxbits), op.chunk_e,
       reinterpret_cast<const unsigned long long*>(op.chunk_s), op.k_pad / kNormCols, op.rows, op.rows_pad, b, op.mu);
   if (moduli == kCrtDefaultModuli && b <= 62)
@@ -1064,7 +1363,14 @@ cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t 
   R.save = args.save;
   R.ld_save = args.ld_save;
   R.uplo = args.uplo;
-  const unsigned gx = unsigned((args.m + 255) / 256);
+  // four rows per thread where the residue planes allow 32-bit loads
+  const bool x4 = args.moduli >= kCrtMinModuli && args.moduli <= 16 && reinterpret_cast<uintptr_t>(args.cres) % 4 == 0 &&
+                  args.ld_res % 4 == 0 && args.plane % 4 == 0 && args.ld_res >= (args.m + 3) / 4 * 4;
+  const int64_t rows_per_block = x4 ? 256 * kRecRowsPerThread : 256;
+  const bool c_vec = reinterpret_cast<uintptr_t>(args.C) % 16 == 0 && args.ldc % 2 == 0;
+  const bool s_vec = args.save == nullptr || (reinterpret_cast<uintptr_t>(args.save) % 16 == 0 && args.ld_save % 2 == 0);
+  R.vec_store = (c_vec && s_vec) ? 1 : 0;
+  const unsigned gx = unsigned((args.m + rows_per_block - 1) / rows_per_block);
   // up to kRecCols columns per block, fewer while the grid is under ~4 blocks per SM
   int64_t cpb = int64_t(gx) * args.n / (4 * 148);
   cpb = cpb < 1 ? 1 : (cpb > kRecCols ? kRecCols : cpb);
@@ -1074,15 +1380,15 @@ cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t 
   const dim3 grid(gx, gy);
   const bool est = args.err_sq != nullptr;
   switch (args.moduli) {
-    case 8: launch_rec128<8>(est, grid, stream, R); break;
-    case 9: launch_rec128<9>(est, grid, stream, R); break;
-    case 10: launch_rec128<10>(est, grid, stream, R); break;
-    case 11: launch_rec128<11>(est, grid, stream, R); break;
-    case 12: launch_rec128<12>(est, grid, stream, R); break;
-    case 13: launch_rec128<13>(est, grid, stream, R); break;
-    case 14: launch_rec128<14>(est, grid, stream, R); break;
-    case 15: launch_rec128<15>(est, grid, stream, R); break;
-    case 16: launch_rec128<16>(est, grid, stream, R); break;
+    case 8: launch_rec128<8>(est, x4, grid, stream, R); break;
+    case 9: launch_rec128<9>(est, x4, grid, stream, R); break;
+    case 10: launch_rec128<10>(est, x4, grid, stream, R); break;
+    case 11: launch_rec128<11>(est, x4, grid, stream, R); break;
+    case 12: launch_rec128<12>(est, x4, grid, stream, R); break;
+    case 13: launch_rec128<13>(est, x4, grid, stream, R); break;
+    case 14: launch_rec128<14>(est, x4, grid, stream, R); break;
+    case 15: launch_rec128<15>(est, x4, grid, stream, R); break;
+    case 16: launch_rec128<16>(est, x4, grid, stream, R); break;
     default: crt_reconstruct_kernel<<<grid, 256, 0, stream>>>(R); break;  // other counts: 192-bit path
   }
   return cudaGetLastError();

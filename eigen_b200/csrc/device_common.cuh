@@ -307,4 +307,18 @@ __device__ __forceinline__ void mma_commit_pair(uint32_t bar_cluster_addr) {
                : "memory");
 }
 
+// ------------------------------------------------------------------ cp.async (LDGSTS)
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+// one element global -> shared, zero-filled when !valid (nothing is read then)
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(uint32_t dst, const void* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(dst), "l"(src), "n"(BYTES),
+               "r"(valid ? BYTES : 0)
+               : "memory");
+}
+
 }  // namespace eb2

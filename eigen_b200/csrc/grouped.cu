@@ -51,19 +51,6 @@ struct GroupedTraits<false> {
 constexpr int kPanelElems = kKc * kLineStride;
 constexpr int kStageElems = 2 * kPanelElems;
 
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-// one element global -> shared, zero-filled when !valid (nothing is read then)
-template <int BYTES>
-__device__ __forceinline__ void cp_async_elem(uint32_t dst, const void* src, bool valid) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(dst), "l"(src), "n"(BYTES),
-               "r"(valid ? BYTES : 0)
-               : "memory");
-}
-
 __device__ __forceinline__ void dmma_16x8x4_g(double (&d)[4], double a0, double a1, double b0) {
   asm volatile(
       "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
