@@ -260,10 +260,12 @@ def peaks():
         return FALLBACK_BF16_TFLOPS, 1400.0, FALLBACK_HBM_GBS, "fallback"
 
 
-# The main GEMM kernel's instantiation for a method and tile configuration (tile 512 = CTA pair).
+# The main GEMM kernel's instantiation for a method and tile configuration (tile 512 = CTA pair,
+# 1024 = one CTA per 256x256 tile).
 def gemm_instantiation(method_crt: bool, tile: int) -> str:
     if method_crt:
-        return "slice_gemm_kernel<2, 256, 6, 4, true>" if tile == 512 else "slice_gemm_kernel<2, 256, 4, 4, false>"
+        return {512: "slice_gemm_kernel<2, 256, 6, 4, true>",
+                1024: "slice_gemm_kernel<2, 256, 3, 8, false, 2>"}.get(tile, "slice_gemm_kernel<2, 256, 4, 4, false>")
     return "slice_gemm_kernel<0, 128, 8, 8, true>" if tile == 512 else "slice_gemm_kernel<0, 128, 6, 8, false>"
 
 
@@ -813,7 +815,8 @@ def our_arm(a, world, rank, local):
         sustained = timed_s >= 2.0
         int8_peak = 2.0 * (bf16_sus if sustained else bf16)
         peak = int8_peak / products  # the FP64-equivalent ceiling of an int8 kernel doing `products` GEMMs
-        shape = "CTA pair, 256x256 tiles, cta_group::2" if tile == 512 else "one CTA, 128x256 tiles"
+        shape = {512: "CTA pair, 256x256 tiles, cta_group::2",
+                 1024: "one CTA, 256x256 tiles (two M=128 MMAs per K step)"}.get(tile, "one CTA, 128x256 tiles")
         inst = gemm_instantiation(method == eb.METHOD_CRT, tile)
         traffic, traffic_src = profiled_traffic(S, inst)
         roof = {"bound": "tensor", "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": UNIT,

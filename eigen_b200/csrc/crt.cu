@@ -939,17 +939,11 @@ __device__ __forceinline__ double u32_to_double(uint32_t x) { return __hiloint2d
 //     2^escale is then exact).  Subnormal and overflowing results take the per-row kernel's
 //     steps (RN of the top 64 bits, then scale_exp), so every result is bit for bit that
 //     kernel's.
+// The second half of crt_entry_fast: RN(C' 2^escale) from S = sum_q acc[q] 2^(32q) (each
+// column below 2^62).
 template <int N>
-__device__ __forceinline__ double crt_entry_fast(const uint32_t (&rc)[N], double P_inv32, int escale) {
+__device__ __forceinline__ double crt_finish(const unsigned long long (&acc)[4], double P_inv32, int escale) {
   static_assert(N >= kCrtMinModuli && N <= 16, "P at least 2^63 and below 2^128");
-  unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
-#pragma unroll
-  for (int g = 0; 2 * g < N; ++g) {
-    uint32_t Rg = rc[2 * g] * kCrtPairs.X[N][2 * g];
-    if (2 * g + 1 < N) Rg += rc[2 * g + 1] * kCrtPairs.X[N][2 * g + 1];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) acc[q] += static_cast<unsigned long long>(Rg) * kCrtPairs.Q[N][g][q];
-  }
   // S = top 2^128 + s3 2^96 + s2 2^64 + s1 2^32 + s0
   const uint32_t s0 = uint32_t(acc[0]);
   const unsigned long long t1 = acc[1] + (acc[0] >> 32);
@@ -1048,6 +1042,154 @@ __device__ __forceinline__ double crt_entry_fast(const uint32_t (&rc)[N], double
   const unsigned long long bits =
       (static_cast<unsigned long long>(E + 1022) << 52) + mant + (negative ? 0x8000000000000000ull : 0ull);
   return __longlong_as_double(static_cast<long long>(bits));
+}
+
+template <int N>
+__device__ __forceinline__ double crt_entry_fast(const uint32_t (&rc)[N], double P_inv32, int escale) {
+  unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
+#pragma unroll
+  for (int g = 0; 2 * g < N; ++g) {
+    uint32_t Rg = rc[2 * g] * kCrtPairs.X[N][2 * g];
+    if (2 * g + 1 < N) Rg += rc[2 * g + 1] * kCrtPairs.X[N][2 * g + 1];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] += static_cast<unsigned long long>(Rg) * kCrtPairs.Q[N][g][q];
+  }
+  return crt_finish<N>(acc, P_inv32, escale);
+}
+
+// ---- reconstruction with the weighted residue sum on the tensor cores
+// S = sum_l r_l W_l = sum_b 2^(8b) T_b with T_b = sum_l r_l w_lb, w_lb byte b of W_l (W_l < P <
+// 2^128: 16 bytes) and T_b < 16 * 255 * 255 < 2^20: a [32 entries x 16 moduli] x [16 moduli x 16
+// bytes] product of unsigned bytes with exact INT32 sums, four mma.sync m16n8k16 per warp.
+__device__ __forceinline__ void mma_u8_16x8x16(int (&d)[4], uint32_t a0, uint32_t a1, uint32_t b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.s32.u8.u8.s32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+      : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+      : "r"(a0), "r"(a1), "r"(b0));
+}
+
+// Rows i0 .. i0+31 of one column per warp.  Lane (g, c) = (lane / 4, lane % 4) loads moduli
+// 4c .. 4c+3 at rows i0 + 4g .. i0 + 4g + 3 (one 32-bit word per modulus), transposes the
+// 4 x 4 bytes so that each word holds the four moduli of one row (the A fragment rows), and
+// the MMAs leave with lane (g, c) the byte sums T_2c, T_2c+1, T_8+2c, T_9+2c of those four
+// rows.  Its share of S is two 64-bit limb columns per row (bits 16c and 64 + 16c); a
+// reduce-scatter over the quad (two shuffle rounds) gives lane (g, c) the four columns of row
+// i0 + 4g + c = i0 + lane, whose tail (crt_finish) and store follow.  Bit for bit the other
+// reconstruction kernels: S is the same integer.
+template <int N, bool EST>
+__global__ void __launch_bounds__(256) crt_reconstruct_mma_kernel(const __grid_constant__ CrtRecParams R) {
+  static_assert(N >= kCrtMinModuli && N <= 16, "16 moduli per MMA K step");
+  if (R.skip_if_flag && *R.skip_if_flag) return;
+  CrtStoreCtx sc = store_ctx(R);
+  const uint8_t* const res = R.res;
+  const int64_t ld_res = R.ld_res, plane = R.plane, m = R.m, ncols = R.ncols;
+  const int uplo = R.uplo;
+  const double P_inv32 = R.P_inv * 0x1p32;
+  const int lane = int(threadIdx.x & 31);
+  const int g = lane >> 2, c = lane & 3;
+  const int64_t i0 = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) - lane;  // the warp's first row
+  const int64_t i = i0 + lane;                                                   // this lane's row
+  // B fragments: byte (8h + g) of W_4c .. W_4c+3
+  uint32_t bfrag[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int byte = 8 * h + g;
+    uint32_t w = 0u;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int l = 4 * c + k;
+      const uint32_t wb = l < N ? (kCrtTable.W[N][l][byte >> 2] >> (8 * (byte & 3))) & 0xFFu : 0u;
+      w |= wb << (8 * k);
+    }
+    bfrag[h] = w;
+  }
+  const int mu_i = i < m ? sc.mu_a[i] : kCrtZeroRow;
+  double e_acc = 0.0, v_acc = 0.0;
+  const uint8_t* const rbase = res + i0 + 4 * g + int64_t(4 * c) * plane;
+  const int cpb = R.cols_per_block;
+  const int64_t jstep = int64_t(gridDim.y) * cpb;
+  for (int64_t j0 = int64_t(blockIdx.y) * cpb; i0 < m && j0 < ncols; j0 += jstep) {
+    // the columns that some row of the warp keeps
+    int64_t jb = j0, j1 = j0 + cpb < ncols ? j0 + cpb : ncols;
+    if (uplo == 1 && jb < i0) jb = i0;            // i <= j
+    if (uplo == 2 && j1 > i0 + 32) j1 = i0 + 32;  // i >= j
+    if (jb >= j1) continue;
+    uint32_t wn[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      wn[k] = 4 * c + k < N ? __ldg(reinterpret_cast<const uint32_t*>(rbase + jb * ld_res + k * plane)) : 0u;
+    for (int64_t j = jb; j < j1; ++j) {
+      uint32_t w[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) w[k] = wn[k];
+      if (j + 1 < j1) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          wn[k] = 4 * c + k < N ? __ldg(reinterpret_cast<const uint32_t*>(rbase + (j + 1) * ld_res + k * plane)) : 0u;
+      }
+      // 4 x 4 byte transpose: w[k] byte e (modulus 4c+k, row 4g+e) -> v[e] byte k
+      const uint32_t t0 = __byte_perm(w[0], w[1], 0x5140), t1 = __byte_perm(w[0], w[1], 0x7362);
+      const uint32_t t2 = __byte_perm(w[2], w[3], 0x5140), t3 = __byte_perm(w[2], w[3], 0x7362);
+      const uint32_t v0 = __byte_perm(t0, t2, 0x5410), v1 = __byte_perm(t0, t2, 0x7632);
+      const uint32_t v2 = __byte_perm(t1, t3, 0x5410), v3 = __byte_perm(t1, t3, 0x7632);
+      // rows 4g+0 / 4g+1 (MMA row slots g / g+8), then rows 4g+2 / 4g+3; bytes 0..7, then 8..15
+      int d0[4] = {0, 0, 0, 0}, d1[4] = {0, 0, 0, 0}, d2[4] = {0, 0, 0, 0}, d3[4] = {0, 0, 0, 0};
+      mma_u8_16x8x16(d0, v0, v1, bfrag[0]);
+      mma_u8_16x8x16(d1, v0, v1, bfrag[1]);
+      mma_u8_16x8x16(d2, v2, v3, bfrag[0]);
+      mma_u8_16x8x16(d3, v2, v3, bfrag[1]);
+      // this lane's share of row 4g+e: lo at bit 16c (column c/2), hi at bit 64 + 16c (column 2 + c/2)
+      const int sh = 16 * (c & 1);
+      unsigned long long lo[4], hi[4];
+      lo[0] = static_cast<unsigned long long>(uint32_t(d0[0]) + (uint32_t(d0[1]) << 8)) << sh;
+      hi[0] = static_cast<unsigned long long>(uint32_t(d1[0]) + (uint32_t(d1[1]) << 8)) << sh;
+      lo[1] = static_cast<unsigned long long>(uint32_t(d0[2]) + (uint32_t(d0[3]) << 8)) << sh;
+      hi[1] = static_cast<unsigned long long>(uint32_t(d1[2]) + (uint32_t(d1[3]) << 8)) << sh;
+      lo[2] = static_cast<unsigned long long>(uint32_t(d2[0]) + (uint32_t(d2[1]) << 8)) << sh;
+      hi[2] = static_cast<unsigned long long>(uint32_t(d3[0]) + (uint32_t(d3[1]) << 8)) << sh;
+      lo[3] = static_cast<unsigned long long>(uint32_t(d2[2]) + (uint32_t(d2[3]) << 8)) << sh;
+      hi[3] = static_cast<unsigned long long>(uint32_t(d3[2]) + (uint32_t(d3[3]) << 8)) << sh;
+      // round 1 (lanes c, c^1 hold the same columns): keep rows 2k + (c & 1), k = 0, 1
+      const bool odd = (c & 1) != 0;
+      unsigned long long klo[2], khi[2];
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const unsigned long long glo = odd ? lo[2 * k] : lo[2 * k + 1];
+        const unsigned long long ghi = odd ? hi[2 * k] : hi[2 * k + 1];
+        klo[k] = (odd ? lo[2 * k + 1] : lo[2 * k]) + __shfl_xor_sync(0xffffffffu, glo, 1);
+        khi[k] = (odd ? hi[2 * k + 1] : hi[2 * k]) + __shfl_xor_sync(0xffffffffu, ghi, 1);
+      }
+      // round 2 (lanes c, c^2 hold the other columns): keep row c = 2 (c >> 1) + (c & 1)
+      const bool upper = (c & 2) != 0;
+      const unsigned long long olo = __shfl_xor_sync(0xffffffffu, upper ? klo[0] : klo[1], 2);
+      const unsigned long long ohi = __shfl_xor_sync(0xffffffffu, upper ? khi[0] : khi[1], 2);
+      const unsigned long long mlo = upper ? klo[1] : klo[0], mhi = upper ? khi[1] : khi[0];
+      unsigned long long acc[4];
+      acc[0] = upper ? olo : mlo;
+      acc[1] = upper ? mlo : olo;
+      acc[2] = upper ? ohi : mhi;
+      acc[3] = upper ? mhi : ohi;
+      const bool keep = i < m && (uplo == 0 || (uplo == 1 ? i <= j : i >= j));
+      if (!keep) continue;
+      const int nu_j = sc.mu_b[j];
+      const double v = __dmul_rn(sc.alpha, crt_finish<N>(acc, P_inv32, -mu_i - nu_j));
+      if (EST) {
+        if (mu_i != kCrtZeroRow && nu_j != kCrtZeroRow) e_acc += exp2_int(2 * (sc.b - mu_i - nu_j));
+        v_acc += v * v;
+      }
+      if (sc.write_c) {
+        double* cp = sc.C + j * sc.ldc + i;
+        if (sc.beta == 0.0) {
+          *cp = v;
+        } else {
+          const double old = *cp;
+          if (sc.save) sc.save[j * sc.ld_save + i] = old;
+          *cp = __fma_rn(sc.beta, old, v);
+        }
+      }
+    }
+  }
+  if (EST) crt_reduce_energies(R, e_acc, v_acc);
 }
 
 // The same, four consecutive rows per thread: one 32-bit load per modulus and column brings
@@ -1196,8 +1338,15 @@ __global__ void __launch_bounds__(256) crt_merge_splits_kernel(uint8_t* __restri
 }
 
 template <int N>
-void launch_rec128(bool est, bool x4, dim3 grid, cudaStream_t stream, const CrtRecParams& R) {
+void launch_rec128(bool est, bool x4, bool mma, dim3 grid, cudaStream_t stream, const CrtRecParams& R) {
   if constexpr (N >= kCrtMinModuli) {
+    if (mma) {
+      if (est)
+        crt_reconstruct_mma_kernel<N, true><<<grid, 256, 0, stream>>>(R);
+      else
+        crt_reconstruct_mma_kernel<N, false><<<grid, 256, 0, stream>>>(R);
+      return;
+    }
     if (x4) {
       if (est)
         crt_reconstruct128x4_kernel<N, true><<<grid, 256, 0, stream>>>(R);
@@ -1366,7 +1515,9 @@ cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t 
   // four rows per thread where the residue planes allow 32-bit loads
   const bool x4 = args.moduli >= kCrtMinModuli && args.moduli <= 16 && reinterpret_cast<uintptr_t>(args.cres) % 4 == 0 &&
                   args.ld_res % 4 == 0 && args.plane % 4 == 0 && args.ld_res >= (args.m + 3) / 4 * 4;
-  const int64_t rows_per_block = x4 ? 256 * kRecRowsPerThread : 256;
+  // the tensor-core sum: whole warps of 32 rows read residues, so the planes must hold them
+  const bool mma = x4 && args.ld_res % 32 == 0 && args.ld_res >= (args.m + 31) / 32 * 32;
+  const int64_t rows_per_block = mma ? 256 : (x4 ? 256 * kRecRowsPerThread : 256);
   const bool c_vec = reinterpret_cast<uintptr_t>(args.C) % 16 == 0 && args.ldc % 2 == 0;
   const bool s_vec = args.save == nullptr || (reinterpret_cast<uintptr_t>(args.save) % 16 == 0 && args.ld_save % 2 == 0);
   R.vec_store = (c_vec && s_vec) ? 1 : 0;
@@ -1380,15 +1531,15 @@ cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t 
   const dim3 grid(gx, gy);
   const bool est = args.err_sq != nullptr;
   switch (args.moduli) {
-    case 8: launch_rec128<8>(est, x4, grid, stream, R); break;
-    case 9: launch_rec128<9>(est, x4, grid, stream, R); break;
-    case 10: launch_rec128<10>(est, x4, grid, stream, R); break;
-    case 11: launch_rec128<11>(est, x4, grid, stream, R); break;
-    case 12: launch_rec128<12>(est, x4, grid, stream, R); break;
-    case 13: launch_rec128<13>(est, x4, grid, stream, R); break;
-    case 14: launch_rec128<14>(est, x4, grid, stream, R); break;
-    case 15: launch_rec128<15>(est, x4, grid, stream, R); break;
-    case 16: launch_rec128<16>(est, x4, grid, stream, R); break;
+    case 8: launch_rec128<8>(est, x4, mma, grid, stream, R); break;
+    case 9: launch_rec128<9>(est, x4, mma, grid, stream, R); break;
+    case 10: launch_rec128<10>(est, x4, mma, grid, stream, R); break;
+    case 11: launch_rec128<11>(est, x4, mma, grid, stream, R); break;
+    case 12: launch_rec128<12>(est, x4, mma, grid, stream, R); break;
+    case 13: launch_rec128<13>(est, x4, mma, grid, stream, R); break;
+    case 14: launch_rec128<14>(est, x4, mma, grid, stream, R); break;
+    case 15: launch_rec128<15>(est, x4, mma, grid, stream, R); break;
+    case 16: launch_rec128<16>(est, x4, mma, grid, stream, R); break;
     default: crt_reconstruct_kernel<<<grid, 256, 0, stream>>>(R); break;  // other counts: 192-bit path
   }
   return cudaGetLastError();

@@ -101,13 +101,19 @@ int crt_split_rule(const Context& cx, int64_t m_pad, int64_t n_pad, int64_t k_pa
   return int(std::max<int64_t>(s, 1));
 }
 
+// Padding the rows to 256 instead of 128 adds nothing (an even count of 128-row blocks) or at
+// most 1/16 of the product.
+static bool crt_rows256_cheap(int64_t m) { return ((m + 127) / 128) % 2 == 0 || m >= 2048; }
+
 int choose_crt_tile(const Context& cx, int64_t m, int64_t n) {
   const int forced = settings().tile_n.load();
   if (forced == kTilePair || forced == kTileWide) return forced;
   if (forced == 128 || forced == 256) return 256;
-  // CTA pairs (256 x 256) unless that leaves most SMs idle
-  const int64_t pair_tiles = ((m + 255) / 256) * ((n + 255) / 256);
-  return 2 * pair_tiles >= cx.num_sms ? kTilePair : 256;
+  // 128 x 256 tiles where 256-row padding would cost; otherwise 256 x 256 tiles, on one CTA
+  // while the (tile, modulus) items fill the SMs, on a CTA pair when they are few
+  if (!crt_rows256_cheap(m)) return 256;
+  const int64_t tiles = ((m + 255) / 256) * ((n + 255) / 256);
+  return tiles * kCrtMinModuli >= cx.num_sms ? kTileWide : kTilePair;
 }
 
 namespace {
@@ -147,15 +153,18 @@ int dgemm_crt(Context& cx, bool ta, bool tb, int64_t m, int64_t n, int64_t k, do
   const bool same = m == n && va.ptr == vb.ptr && va.sr == vb.sr && va.sl == vb.sl;
   // rows padded for the pair tile whenever the picker may still choose it
   // (a forced pair class switches the tile to a CTA pair below)
-  const bool pair_rows = stage2 || same || (auto_tile && (fc == kCfgCrtPair || fc == kCfgCrtPairGroup));
+  const bool pair_rows =
+      stage2 || same || crt_rows256_cheap(m) || (auto_tile && (fc == kCfgCrtPair || fc == kCfgCrtPairGroup));
   const int64_t m_pad = round_up(m, pair_rows ? 256 : crt_tile_rows(tile)),
                 n_pad = round_up(n, crt_tile_cols(tile)), k_pad = round_up(k, kOzakiKBlock);
   const bool tri = opt.uplo == 1 || opt.uplo == 2;
   const int64_t max_tiles = (m_pad / 128) * (n_pad / 256);
   // a configuration class: tile shape, raster order, K splits (dense products only)
   const bool may_split = auto_tile && !tri && opt.tri_operand == 0;
+  // the one-CTA classes take 256 x 256 tiles where the rows are padded to 256 at little cost
+  const int cta_tile = (m_pad % 256 == 0 && crt_rows256_cheap(m)) ? kTileWide : 256;
   auto apply_config = [&](int c) {
-    tile = (c == kCfgCrtPair || c == kCfgCrtPairGroup) ? kTilePair : 256;
+    tile = (c == kCfgCrtPair || c == kCfgCrtPairGroup) ? kTilePair : (c == kCfgCrtSplitK ? 256 : cta_tile);
     group_m = (c == kCfgCrtCtaGroup || c == kCfgCrtPairGroup) ? kCfgGroupM : 0;
     splits = (c == kCfgCrtSplitK && may_split) ? crt_split_rule(cx, m_pad, n_pad, k_pad, nmod) : 1;
   };

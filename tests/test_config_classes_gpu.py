@@ -59,7 +59,9 @@ def test_crt_classes_same_bits(m, n, k, ta, tb, beta):
         assert infos[cfg]["config"] == cfg or (cfg == 5 and infos[cfg]["splits"] == 1), infos[cfg]
     for cfg in (2, 3, 4, 5):
         np.testing.assert_array_equal(results[cfg], results[1], err_msg=f"class {cfg}")
-    assert infos[2]["tile_n"] == 512 and infos[1]["tile_n"] == 256
+    # one-CTA classes: 256 x 256 tiles where padding the rows to 256 costs little, else 128 x 256
+    cheap = ((m + 127) // 128) % 2 == 0 or m >= 2048
+    assert infos[2]["tile_n"] == 512 and infos[1]["tile_n"] == (1024 if cheap else 256)
     # small outputs with long K: the split-K class splits
     if m * n <= 300 * 260:
         assert infos[5]["splits"] > 1, infos[5]
