@@ -265,7 +265,7 @@ def peaks():
 def gemm_instantiation(method_crt: bool, tile: int) -> str:
     if method_crt:
         return {512: "slice_gemm_kernel<2, 256, 6, 4, true>",
-                1024: "slice_gemm_kernel<2, 256, 3, 8, false, 2>"}.get(tile, "slice_gemm_kernel<2, 256, 4, 4, false>")
+                1024: "slice_gemm_kernel<2, 256, 3, 16, false, 2>"}.get(tile, "slice_gemm_kernel<2, 256, 4, 4, false>")
     return "slice_gemm_kernel<0, 128, 8, 8, true>" if tile == 512 else "slice_gemm_kernel<0, 128, 6, 8, false>"
 
 

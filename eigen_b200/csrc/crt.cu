@@ -210,30 +210,45 @@ __global__ void __launch_bounds__(kNormThreads) crt_scan_norm_kernel(const doubl
   const int rr = threadIdx.x >> 3;
   const int sub = threadIdx.x & 7;
   const int64_t r = r0 + rr;
-  unsigned long long mb = 0, mb64 = 0;
+  // the spread statistic: the first 64 columns of every 512 (block-uniform)
+  const bool stat = spread != nullptr && (l0 & 511) == 0;
+  // maxima of |x| as doubles (their bit patterns order the same way), the largest high word
+  // for NaN / Inf (a NaN drops out of fmax but not out of the high-word maximum)
+  double dmax = 0.0, dmax64 = 0.0;
+  uint32_t hmax = 0u, hmax64 = 0u;
   int esum = 0, ecnt = 0;
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
-    const unsigned long long bits =
-        static_cast<unsigned long long>(__double_as_longlong(fabs(tile[rr][sub + 8 * j])));
-    mb = bits > mb ? bits : mb;
-    if (j < 8) {  // the first 64 columns, for the spread statistic
-      mb64 = bits > mb64 ? bits : mb64;
-      if (bits) {
-        esum += int(bits >> 52);
+    const double a = fabs(tile[rr][sub + 8 * j]);
+    const uint32_t h = uint32_t(__double2hiint(a));
+    dmax = fmax(dmax, a);
+    hmax = max(hmax, h);
+    if (stat && j < 8) {
+      dmax64 = fmax(dmax64, a);
+      hmax64 = max(hmax64, h);
+      if (a != 0.0) {
+        esum += int(h >> 20);
         ++ecnt;
       }
     }
   }
 #pragma unroll
   for (int o = 4; o > 0; o >>= 1) {
-    const unsigned long long other = __shfl_xor_sync(0xffffffffu, mb, o);
-    mb = other > mb ? other : mb;
-    const unsigned long long other64 = __shfl_xor_sync(0xffffffffu, mb64, o);
-    mb64 = other64 > mb64 ? other64 : mb64;
-    esum += __shfl_xor_sync(0xffffffffu, esum, o);
-    ecnt += __shfl_xor_sync(0xffffffffu, ecnt, o);
+    dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    hmax = max(hmax, __shfl_xor_sync(0xffffffffu, hmax, o));
+    if (stat) {
+      dmax64 = fmax(dmax64, __shfl_xor_sync(0xffffffffu, dmax64, o));
+      hmax64 = max(hmax64, __shfl_xor_sync(0xffffffffu, hmax64, o));
+      esum += __shfl_xor_sync(0xffffffffu, esum, o);
+      ecnt += __shfl_xor_sync(0xffffffffu, ecnt, o);
+    }
   }
+  // bit pattern of the largest |x|, or of at least +Inf when the chunk holds a NaN or an Inf
+  const unsigned long long mb = hmax >= 0x7FF00000u ? (static_cast<unsigned long long>(hmax) << 32)
+                                                     : static_cast<unsigned long long>(__double_as_longlong(dmax));
+  const unsigned long long mb64 = hmax64 >= 0x7FF00000u
+                                      ? (static_cast<unsigned long long>(hmax64) << 32)
+                                      : static_cast<unsigned long long>(__double_as_longlong(dmax64));
   unsigned long long s = 0;
   int e = 0;
   if (mb != 0 && mb < kInfBitsCrt) {
@@ -259,7 +274,7 @@ __global__ void __launch_bounds__(kNormThreads) crt_scan_norm_kernel(const doubl
     if (mb >= kInfBitsCrt) *nonfinite = 1;
     if (mb) atomicMax(&maxbits[r], mb);
   }
-  if (spread != nullptr && (l0 & 511) == 0) {
+  if (stat) {
     double chunk_spread = 0.0, chunk_count = 0.0;
     if (sub == 0 && r < rows && ecnt > 0 && mb64 < kInfBitsCrt) {
       chunk_spread = double(int(mb64 >> 52)) - double(esum) / double(ecnt);
@@ -374,7 +389,9 @@ __device__ __forceinline__ uint32_t residue_of(const Chunks21& c, const CrtModCo
 constexpr int kSplitRowsCrt = 32;
 constexpr int kSplitColsCrt = 128;
 
-constexpr int kSplitThreadsCrt = 512;  // a warp per row (4 entries per lane), 16 rows per pass
+// a warp per row (4 entries per lane), 8 rows per pass; three blocks per SM (80 registers)
+// measured faster than two blocks of 512 threads (64 registers, spilled) or one (124 registers)
+constexpr int kSplitThreadsCrt = 256;
 constexpr int kSplitEntries = 4;      // entries (consecutive columns) per thread and row
 
 // The 4 symmetric residues of one thread's entries for one modulus, from 21-bit chunks of
@@ -462,7 +479,7 @@ __device__ __forceinline__ void store_residues_static(const SplitEntry (&e)[kSpl
 // A 32 x 128 tile per block: each warp takes a row at a time, four consecutive entries per
 // lane, so that every modulus plane receives 128 contiguous bytes per warp store.
 template <bool kWide, int NT>  // kWide: |t| may reach 2^63 (more than 16 moduli)
-__global__ void __launch_bounds__(kSplitThreadsCrt, 2) crt_split_kernel(
+__global__ void __launch_bounds__(kSplitThreadsCrt, 3) crt_split_kernel(
     const double* __restrict__ X, int64_t rows, int64_t cols, int64_t sr, int64_t sl,
     const int32_t* __restrict__ mu, int n, int8_t* __restrict__ residues, int64_t rows_pad, int64_t k_pad) {
   static_assert(kSplitColsCrt == 32 * kSplitEntries, "a warp per tile row");
@@ -1469,8 +1486,10 @@ cudaError_t launch_crt_gemm(const CrtOperand& a, const CrtOperand& b, const CrtG
   if (a.k_pad != b.k_pad || a.k_pad % kSliceKBytes != 0) return cudaErrorInvalidValue;
   if (args.tile_n == kTilePair) return launch_gemm_config<256, 6, true>(a, b, args, stream);
   if (args.tile_n == 256) return launch_gemm_config<256, 4, false>(a, b, args, stream);
-  // 256 x 256 per CTA: 64 KB stages (three), eight epilogue warps (two per TMEM lane quadrant)
-  if (args.tile_n == kTileWide) return launch_gemm_config<256, 3, false, 2, 8>(a, b, args, stream);
+  // 256 x 256 per CTA: 64 KB stages (three), sixteen epilogue warps (four per TMEM lane
+  // quadrant: the single accumulator buffer is drained while the MMAs wait, so the drain is
+  // spread over as many warps as the registers allow)
+  if (args.tile_n == kTileWide) return launch_gemm_config<256, 3, false, 2, 16>(a, b, args, stream);
   return cudaErrorInvalidValue;
 }
 
