@@ -956,33 +956,13 @@ __device__ __forceinline__ double u32_to_double(uint32_t x) { return __hiloint2d
 //     2^escale is then exact).  Subnormal and overflowing results take the per-row kernel's
 //     steps (RN of the top 64 bits, then scale_exp), so every result is bit for bit that
 //     kernel's.
-// The second half of crt_entry_fast: RN(C' 2^escale) from S = sum_q acc[q] 2^(32q) (each
-// column below 2^62).
+// RN(R 2^escale) for R = (r3 r2 r1 r0) in 128-bit two's complement, congruent to C' modulo P
+// and within one P of [-P/2, P/2): the range fix, the magnitude's top 64 bits with a sticky
+// bit, and the double written from its rounded significand (or, for subnormal and
+// overflowing results, RN of the top bits and scale_exp).
 template <int N>
-__device__ __forceinline__ double crt_finish(const unsigned long long (&acc)[4], double P_inv32, int escale) {
-  static_assert(N >= kCrtMinModuli && N <= 16, "P at least 2^63 and below 2^128");
-  // S = top 2^128 + s3 2^96 + s2 2^64 + s1 2^32 + s0
-  const uint32_t s0 = uint32_t(acc[0]);
-  const unsigned long long t1 = acc[1] + (acc[0] >> 32);
-  const unsigned long long t2 = acc[2] + (t1 >> 32);
-  const unsigned long long t3 = acc[3] + (t2 >> 32);
-  const uint32_t s1 = uint32_t(t1), s2 = uint32_t(t2), s3 = uint32_t(t3), top = uint32_t(t3 >> 32);
-  // S / 2^32 in FP64 (s0 < 2^32 <= 2^-31 P left out), then q in the low word of
-  // rint(S / P) + 1.5 2^52 (0 <= q < 2^31)
-  const double hi = fma(u32_to_double(top), 0x1p32, u32_to_double(s3));
-  const double mid = fma(hi, 0x1p32, u32_to_double(s2));
-  const double sd = fma(mid, 0x1p32, u32_to_double(s1));
-  const uint32_t q = uint32_t(__double2loint(fma(sd, P_inv32, 0x1.8p52)));
-  // R = S - q P modulo 2^128
+__device__ __forceinline__ double crt_round(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3, int escale) {
   constexpr uint32_t P0 = kCrtTableC.P[N][0], P1 = kCrtTableC.P[N][1], P2 = kCrtTableC.P[N][2], P3 = kCrtTableC.P[N][3];
-  long long d = static_cast<long long>(s0) - static_cast<long long>(static_cast<unsigned long long>(q) * P0);
-  uint32_t r0 = uint32_t(d);
-  d = (d >> 32) + static_cast<long long>(s1) - static_cast<long long>(static_cast<unsigned long long>(q) * P1);
-  uint32_t r1 = uint32_t(d);
-  d = (d >> 32) + static_cast<long long>(s2) - static_cast<long long>(static_cast<unsigned long long>(q) * P2);
-  uint32_t r2 = uint32_t(d);
-  d = (d >> 32) + static_cast<long long>(s3) - static_cast<long long>(static_cast<unsigned long long>(q) * P3);
-  uint32_t r3 = uint32_t(d);
   // R lies in [-half, half) when the 64-bit window of R at half's two top limbs is in
   // [-Hw, Hw) and the limbs above the window extend its sign: nothing to fix then
   constexpr int kW = kCrtTableC.half[N][3] != 0 ? 2 : (kCrtTableC.half[N][2] != 0 ? 1 : 0);
@@ -1061,6 +1041,59 @@ __device__ __forceinline__ double crt_finish(const unsigned long long (&acc)[4],
   return __longlong_as_double(static_cast<long long>(bits));
 }
 
+// The second half of crt_entry_fast: RN(C' 2^escale) from S = sum_q acc[q] 2^(32q) (each
+// column below 2^62).
+template <int N>
+__device__ __forceinline__ double crt_finish(const unsigned long long (&acc)[4], double P_inv32, int escale) {
+  static_assert(N >= kCrtMinModuli && N <= 16, "P at least 2^63 and below 2^128");
+  // S = top 2^128 + s3 2^96 + s2 2^64 + s1 2^32 + s0
+  const uint32_t s0 = uint32_t(acc[0]);
+  const unsigned long long t1 = acc[1] + (acc[0] >> 32);
+  const unsigned long long t2 = acc[2] + (t1 >> 32);
+  const unsigned long long t3 = acc[3] + (t2 >> 32);
+  const uint32_t s1 = uint32_t(t1), s2 = uint32_t(t2), s3 = uint32_t(t3), top = uint32_t(t3 >> 32);
+  // S / 2^32 in FP64 (s0 < 2^32 <= 2^-31 P left out), then q in the low word of
+  // rint(S / P) + 1.5 2^52 (0 <= q < 2^31)
+  const double hi = fma(u32_to_double(top), 0x1p32, u32_to_double(s3));
+  const double mid = fma(hi, 0x1p32, u32_to_double(s2));
+  const double sd = fma(mid, 0x1p32, u32_to_double(s1));
+  const uint32_t q = uint32_t(__double2loint(fma(sd, P_inv32, 0x1.8p52)));
+  // R = S - q P modulo 2^128
+  constexpr uint32_t P0 = kCrtTableC.P[N][0], P1 = kCrtTableC.P[N][1], P2 = kCrtTableC.P[N][2], P3 = kCrtTableC.P[N][3];
+  long long d = static_cast<long long>(s0) - static_cast<long long>(static_cast<unsigned long long>(q) * P0);
+  uint32_t r0 = uint32_t(d);
+  d = (d >> 32) + static_cast<long long>(s1) - static_cast<long long>(static_cast<unsigned long long>(q) * P1);
+  uint32_t r1 = uint32_t(d);
+  d = (d >> 32) + static_cast<long long>(s2) - static_cast<long long>(static_cast<unsigned long long>(q) * P2);
+  uint32_t r2 = uint32_t(d);
+  d = (d >> 32) + static_cast<long long>(s3) - static_cast<long long>(static_cast<unsigned long long>(q) * P3);
+  uint32_t r3 = uint32_t(d);
+  return crt_round<N>(r0, r1, r2, r3, escale);
+}
+
+// crt_finish for limb columns below 2^52 (the tensor-core sum gives columns below 2^46): the
+// columns are exact doubles by one integer add and one FP64 subtraction, q comes from
+// acc[1..3] (acc[0] / P < 2^-11 left out; q is off by one at most, which the range fix
+// absorbs), and R = S - q P takes its borrows column by column without carrying S first.
+template <int N>
+__device__ __forceinline__ double crt_finish_small(const unsigned long long (&acc)[4], double P_inv32, int escale) {
+  static_assert(N >= kCrtMinModuli && N <= 16, "P at least 2^63 and below 2^128");
+  auto exact = [](unsigned long long x) {  // x < 2^52
+    return __longlong_as_double(static_cast<long long>(x + 0x4330000000000000ull)) - 0x1p52;
+  };
+  const double sd = fma(fma(exact(acc[3]), 0x1p32, exact(acc[2])), 0x1p32, exact(acc[1]));
+  const uint32_t q = uint32_t(__double2loint(fma(sd, P_inv32, 0x1.8p52)));
+  constexpr uint32_t P0 = kCrtTableC.P[N][0], P1 = kCrtTableC.P[N][1], P2 = kCrtTableC.P[N][2], P3 = kCrtTableC.P[N][3];
+  const long long d0 = static_cast<long long>(acc[0]) - static_cast<long long>(static_cast<unsigned long long>(q) * P0);
+  const long long d1 = static_cast<long long>(acc[1]) - static_cast<long long>(static_cast<unsigned long long>(q) * P1) +
+                       (d0 >> 32);
+  const long long d2 = static_cast<long long>(acc[2]) - static_cast<long long>(static_cast<unsigned long long>(q) * P2) +
+                       (d1 >> 32);
+  const long long d3 = static_cast<long long>(acc[3]) - static_cast<long long>(static_cast<unsigned long long>(q) * P3) +
+                       (d2 >> 32);
+  return crt_round<N>(uint32_t(d0), uint32_t(d1), uint32_t(d2), uint32_t(d3), escale);
+}
+
 template <int N>
 __device__ __forceinline__ double crt_entry_fast(const uint32_t (&rc)[N], double P_inv32, int escale) {
   unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
@@ -1089,14 +1122,17 @@ __device__ __forceinline__ void mma_u8_16x8x16(int (&d)[4], uint32_t a0, uint32_
 // 4c .. 4c+3 at rows i0 + 4g .. i0 + 4g + 3 (one 32-bit word per modulus), transposes the
 // 4 x 4 bytes so that each word holds the four moduli of one row (the A fragment rows), and
 // the MMAs leave with lane (g, c) the byte sums T_2c, T_2c+1, T_8+2c, T_9+2c of those four
-// rows.  Its share of S is two 64-bit limb columns per row (bits 16c and 64 + 16c); a
-// reduce-scatter over the quad (two shuffle rounds) gives lane (g, c) the four columns of row
-// i0 + 4g + c = i0 + lane, whose tail (crt_finish) and store follow.  Bit for bit the other
-// reconstruction kernels: S is the same integer.
+// rows.  The warp passes them through its own rows of shared memory so that lane L reads all
+// sixteen sums of row i0 + L and forms S in four 32-bit-aligned columns with multiply-adds;
+// the tail (crt_finish) and the store follow.  Bit for bit the other reconstruction kernels:
+// S is the same integer.
+constexpr int kRecStageStride = 18;  // words per staged row (16 byte sums + 2)
 template <int N, bool EST>
-__global__ void __launch_bounds__(256) crt_reconstruct_mma_kernel(const __grid_constant__ CrtRecParams R) {
+__global__ void __launch_bounds__(256, 4) crt_reconstruct_mma_kernel(const __grid_constant__ CrtRecParams R) {
   static_assert(N >= kCrtMinModuli && N <= 16, "16 moduli per MMA K step");
+  __shared__ __align__(16) uint32_t stage[8][32 * kRecStageStride];
   if (R.skip_if_flag && *R.skip_if_flag) return;
+  uint32_t* const wstage = stage[threadIdx.x >> 5];
   CrtStoreCtx sc = store_ctx(R);
   const uint8_t* const res = R.res;
   const int64_t ld_res = R.ld_res, plane = R.plane, m = R.m, ncols = R.ncols;
@@ -1155,41 +1191,35 @@ __global__ void __launch_bounds__(256) crt_reconstruct_mma_kernel(const __grid_c
       mma_u8_16x8x16(d1, v0, v1, bfrag[1]);
       mma_u8_16x8x16(d2, v2, v3, bfrag[0]);
       mma_u8_16x8x16(d3, v2, v3, bfrag[1]);
-      // this lane's share of row 4g+e: lo at bit 16c (column c/2), hi at bit 64 + 16c (column 2 + c/2)
-      const int sh = 16 * (c & 1);
-      unsigned long long lo[4], hi[4];
-      lo[0] = static_cast<unsigned long long>(uint32_t(d0[0]) + (uint32_t(d0[1]) << 8)) << sh;
-      hi[0] = static_cast<unsigned long long>(uint32_t(d1[0]) + (uint32_t(d1[1]) << 8)) << sh;
-      lo[1] = static_cast<unsigned long long>(uint32_t(d0[2]) + (uint32_t(d0[3]) << 8)) << sh;
-      hi[1] = static_cast<unsigned long long>(uint32_t(d1[2]) + (uint32_t(d1[3]) << 8)) << sh;
-      lo[2] = static_cast<unsigned long long>(uint32_t(d2[0]) + (uint32_t(d2[1]) << 8)) << sh;
-      hi[2] = static_cast<unsigned long long>(uint32_t(d3[0]) + (uint32_t(d3[1]) << 8)) << sh;
-      lo[3] = static_cast<unsigned long long>(uint32_t(d2[2]) + (uint32_t(d2[3]) << 8)) << sh;
-      hi[3] = static_cast<unsigned long long>(uint32_t(d3[2]) + (uint32_t(d3[3]) << 8)) << sh;
-      // round 1 (lanes c, c^1 hold the same columns): keep rows 2k + (c & 1), k = 0, 1
-      const bool odd = (c & 1) != 0;
-      unsigned long long klo[2], khi[2];
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const unsigned long long glo = odd ? lo[2 * k] : lo[2 * k + 1];
-        const unsigned long long ghi = odd ? hi[2 * k] : hi[2 * k + 1];
-        klo[k] = (odd ? lo[2 * k + 1] : lo[2 * k]) + __shfl_xor_sync(0xffffffffu, glo, 1);
-        khi[k] = (odd ? hi[2 * k + 1] : hi[2 * k]) + __shfl_xor_sync(0xffffffffu, ghi, 1);
-      }
-      // round 2 (lanes c, c^2 hold the other columns): keep row c = 2 (c >> 1) + (c & 1)
-      const bool upper = (c & 2) != 0;
-      const unsigned long long olo = __shfl_xor_sync(0xffffffffu, upper ? klo[0] : klo[1], 2);
-      const unsigned long long ohi = __shfl_xor_sync(0xffffffffu, upper ? khi[0] : khi[1], 2);
-      const unsigned long long mlo = upper ? klo[1] : klo[0], mhi = upper ? khi[1] : khi[0];
+      // byte sums of rows 4g+e through the warp's shared-memory rows (stride 18 words: the
+      // 64-bit reads below are free of bank conflicts): row 4g+e, words 2c, 2c+1 (bytes 0..7
+      // half) and 8+2c, 9+2c (bytes 8..15 half)
+      __syncwarp();
+      uint32_t* w0 = wstage + (4 * g) * kRecStageStride + 2 * c;
+      *reinterpret_cast<uint2*>(w0) = make_uint2(uint32_t(d0[0]), uint32_t(d0[1]));
+      *reinterpret_cast<uint2*>(w0 + 8) = make_uint2(uint32_t(d1[0]), uint32_t(d1[1]));
+      *reinterpret_cast<uint2*>(w0 + kRecStageStride) = make_uint2(uint32_t(d0[2]), uint32_t(d0[3]));
+      *reinterpret_cast<uint2*>(w0 + kRecStageStride + 8) = make_uint2(uint32_t(d1[2]), uint32_t(d1[3]));
+      *reinterpret_cast<uint2*>(w0 + 2 * kRecStageStride) = make_uint2(uint32_t(d2[0]), uint32_t(d2[1]));
+      *reinterpret_cast<uint2*>(w0 + 2 * kRecStageStride + 8) = make_uint2(uint32_t(d3[0]), uint32_t(d3[1]));
+      *reinterpret_cast<uint2*>(w0 + 3 * kRecStageStride) = make_uint2(uint32_t(d2[2]), uint32_t(d2[3]));
+      *reinterpret_cast<uint2*>(w0 + 3 * kRecStageStride + 8) = make_uint2(uint32_t(d3[2]), uint32_t(d3[3]));
+      __syncwarp();
+      // this lane's row: S = sum_b T_b 2^(8b) as four 32-bit-aligned columns (each < 2^45)
       unsigned long long acc[4];
-      acc[0] = upper ? olo : mlo;
-      acc[1] = upper ? mlo : olo;
-      acc[2] = upper ? ohi : mhi;
-      acc[3] = upper ? mhi : ohi;
+      const uint32_t* rrow = wstage + lane * kRecStageStride;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint2 p0 = *reinterpret_cast<const uint2*>(rrow + 4 * q);
+        const uint2 p1 = *reinterpret_cast<const uint2*>(rrow + 4 * q + 2);
+        const uint32_t low = p0.x + p0.y * 256u;  // < 2^29
+        acc[q] = static_cast<unsigned long long>(p1.x) * 65536ull + low;
+        acc[q] += static_cast<unsigned long long>(p1.y) * 16777216ull;
+      }
       const bool keep = i < m && (uplo == 0 || (uplo == 1 ? i <= j : i >= j));
       if (!keep) continue;
       const int nu_j = sc.mu_b[j];
-      const double v = __dmul_rn(sc.alpha, crt_finish<N>(acc, P_inv32, -mu_i - nu_j));
+      const double v = __dmul_rn(sc.alpha, crt_finish_small<N>(acc, P_inv32, -mu_i - nu_j));
       if (EST) {
         if (mu_i != kCrtZeroRow && nu_j != kCrtZeroRow) e_acc += exp2_int(2 * (sc.b - mu_i - nu_j));
         v_acc += v * v;
