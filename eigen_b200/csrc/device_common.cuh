@@ -313,6 +313,12 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
+// the mbarrier receives one arrival once every cp.async this thread issued before has landed
+// (.noinc: that arrival is one of the barrier's expected arrivals)
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 // one element global -> shared, zero-filled when !valid (nothing is read then)
 template <int BYTES>
 __device__ __forceinline__ void cp_async_elem(uint32_t dst, const void* src, bool valid) {

@@ -19,15 +19,35 @@ namespace eb2 {
 namespace {
 
 // ------------------------------------------------------------------ FP64 DMMA
+// 128 x 128 tiles, K in tiles of 16 through a 4-stage shared-memory ring, warp-specialised:
+// four producer warps copy the tiles with 8-byte cp.async (any alignment and leading
+// dimension; edges zero-filled) and hands each stage over with cp.async.mbarrier.arrive on
+// its `full` barrier; eight consumer warps (64 x 32 outputs each) wait on `full`, run DMMA
+// m16n8k4 with K in steps of 4 from 0 upward for every output, and release the stage on its
+// `empty` barrier.  No block-wide barrier in the main loop: measured, the copy issue and the
+// per-tile __syncthreads of a cooperative ring cost a fifth of the DMMA rate.  Shared memory
+// follows each operand's contiguous direction in global memory ([k][m] when op(A) is stored
+// column-major, [m][k] when transposed; likewise for op(B)), padded so that the 64-bit
+// fragment loads of each half-warp hit distinct banks.  Every wait is bounded (kWaitLimitNs);
+// one that runs out records EB2_DEV_ERR_TIMEOUT in *status and the roles leave.
 constexpr int kDBM = 128, kDBN = 128, kDBK = 16;
-constexpr int kDApad = kDBM + 4;  // sA[k][m] row stride (doubles): conflict-free fragment loads
-constexpr int kDBpad = kDBK + 4;  // sB[n][k] row stride
-constexpr int kDThreads = 256;
+constexpr int kDStages = 4;
+constexpr int kDPadMN = kDBM + 4;  // [k][m or n] row stride (doubles)
+constexpr int kDPadK = kDBK + 4;   // [m or n][k] row stride
+constexpr int kDConsumerWarps = 8;
+constexpr int kDProducerWarps = 4;
+constexpr int kDThreads = 32 * (kDConsumerWarps + kDProducerWarps);
+constexpr int kDTileElems = (kDBK * kDPadMN > kDBM * kDPadK) ? kDBK * kDPadMN : kDBM * kDPadK;
 
 struct DSmem {
-  double a[2][kDBK][kDApad];
-  double b[2][kDBN][kDBpad];
+  double a[kDStages][kDTileElems];
+  double b[kDStages][kDTileElems];
+  uint64_t full[kDStages], empty[kDStages];
+  int abort_flag;
 };
+
+// where a native-kernel wait that ran out is recorded when the caller passes no status word
+__device__ uint32_t g_native_status;
 
 __device__ __forceinline__ void dmma_16x8x4(double (&d)[4], double a0, double a1, double b0) {
   asm volatile(
@@ -36,90 +56,97 @@ __device__ __forceinline__ void dmma_16x8x4(double (&d)[4], double a0, double a1
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
-template <bool TA, bool TB>
-__device__ __forceinline__ void dload_tile(const double* __restrict__ A, int64_t lda, const double* __restrict__ B,
-                                           int64_t ldb, int64_t m, int64_t n, int64_t k, int64_t m0, int64_t n0,
-                                           int64_t k0, double (&ra)[8], double (&rb)[8]) {
-  const int t = threadIdx.x;
+// The producer warps' copies of one K tile of one operand (rows x k view at X, leading
+// dimension ld).  MN_CONTIG: the operand's m (or n) index is the contiguous one in global
+// memory (op(A) = A column-major, op(B) = B^T of a column-major B).  V = 2: 16-byte copies of
+// two neighbours along the contiguous index (X 16-byte aligned, ld even); a pair that
+// straddles the edge copies its first element and zero-fills the second.
+template <bool MN_CONTIG, int V>
+__device__ __forceinline__ void dcopy_operand(double* st, const double* __restrict__ X, int64_t ld, int64_t rows,
+                                              int64_t k, int64_t r0, int64_t k0, int pt) {
+  constexpr int kPT = 32 * kDProducerWarps;
+  constexpr int kRowsV = MN_CONTIG ? kDBM / V : kDBM, kColsV = MN_CONTIG ? kDBK : kDBK / V;
+  constexpr int kCopies = kRowsV * kColsV / kPT;
+  // thread pt copies a fixed contiguous-direction offset and steps through the other index
+  // (kStep columns of K, or kStep rows) from copy to copy
+  constexpr int kStep = MN_CONTIG ? kPT / kRowsV : kPT / kColsV;
+  static_assert(kPT % (MN_CONTIG ? kRowsV : kColsV) == 0, "fixed contiguous offset per thread");
+  const int c_off = (pt % (MN_CONTIG ? kRowsV : kColsV)) * V;  // along the contiguous index
+  const int s_first = pt / (MN_CONTIG ? kRowsV : kColsV);      // first value of the stepped index
+  const int64_t g_c = (MN_CONTIG ? r0 : k0) + c_off, g_s = (MN_CONTIG ? k0 : r0) + s_first;
+  const int64_t lim_c = MN_CONTIG ? rows : k, lim_s = MN_CONTIG ? k : rows;
+  // elements of the contiguous pair inside the matrix (0, 1 or V); the same for every copy
+  const int in_c = g_c + V <= lim_c ? V : (g_c < lim_c ? int(lim_c - g_c) : 0);
+  const double* src = X + g_c + g_s * ld;
+  const int64_t src_step = int64_t(kStep) * ld;
+  uint32_t dst = smem_u32(MN_CONTIG ? st + s_first * kDPadMN + c_off : st + s_first * kDPadK + c_off);
+  constexpr uint32_t kDstStep = uint32_t(kStep * (MN_CONTIG ? kDPadMN : kDPadK) * 8);
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int idx = t + kDThreads * i;
-    int mm, kk;
-    if (!TA) {
-      mm = idx % kDBM;
-      kk = idx / kDBM;
-    } else {
-      kk = idx % kDBK;
-      mm = idx / kDBK;
-    }
-    const int64_t gm = m0 + mm, gk = k0 + kk;
-    double v = 0.0;
-    if (gm < m && gk < k) v = TA ? A[gk + gm * lda] : A[gm + gk * lda];
-    ra[i] = v;
-  }
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int idx = t + kDThreads * i;
-    int nn, kk;
-    if (!TB) {
-      kk = idx % kDBK;
-      nn = idx / kDBK;
-    } else {
-      nn = idx % kDBN;
-      kk = idx / kDBN;
-    }
-    const int64_t gn = n0 + nn, gk = k0 + kk;
-    double v = 0.0;
-    if (gn < n && gk < k) v = TB ? B[gn + gk * ldb] : B[gk + gn * ldb];
-    rb[i] = v;
+  for (int i = 0; i < kCopies; ++i, src += src_step, dst += kDstStep) {
+    const int in = (g_s + int64_t(i) * kStep < lim_s) ? in_c : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(dst), "l"(in ? src : X), "n"(8 * V),
+                 "r"(8 * in)
+                 : "memory");
   }
 }
 
-template <bool TA, bool TB>
-__device__ __forceinline__ void dstore_tile(DSmem& s, int buf, const double (&ra)[8], const double (&rb)[8]) {
-  const int t = threadIdx.x;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int idx = t + kDThreads * i;
-    int mm, kk;
-    if (!TA) {
-      mm = idx % kDBM;
-      kk = idx / kDBM;
-    } else {
-      kk = idx % kDBK;
-      mm = idx / kDBK;
-    }
-    s.a[buf][kk][mm] = ra[i];
-  }
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int idx = t + kDThreads * i;
-    int nn, kk;
-    if (!TB) {
-      kk = idx % kDBK;
-      nn = idx / kDBK;
-    } else {
-      nn = idx % kDBN;
-      kk = idx / kDBN;
-    }
-    s.b[buf][nn][kk] = rb[i];
-  }
+// Tile t of the grid in groups of kDGroupM tile rows (column-major inside a group), so that
+// the CTAs in flight share A panels in L2 as well as B panels.
+constexpr int kDGroupM = 8;
+__device__ __forceinline__ void dtile_coords(int64_t t, int64_t tiles_m, int64_t tiles_n, int64_t& tm, int64_t& tn) {
+  const int64_t per_group = int64_t(kDGroupM) * tiles_n;
+  const int64_t first_m = (t / per_group) * kDGroupM;
+  const int64_t gm = tiles_m - first_m < kDGroupM ? tiles_m - first_m : kDGroupM;
+  const int64_t r = t % per_group;
+  tm = first_m + r % gm;
+  tn = r / gm;
 }
 
-template <bool TA, bool TB>
+template <bool TA, bool TB, int VA, int VB>
 __global__ void __launch_bounds__(kDThreads, 1)
     dgemm_dmma_kernel(int64_t m, int64_t n, int64_t k, double alpha, const double* __restrict__ A, int64_t lda,
                       const double* __restrict__ B, int64_t ldb, double beta, double* __restrict__ C, int64_t ldc,
-                      const int* only_if_flag) {
+                      const int* only_if_flag, uint32_t* status) {
   if (only_if_flag && *only_if_flag == 0) return;
   extern __shared__ __align__(16) uint8_t dsmem_raw[];
   DSmem& s = *reinterpret_cast<DSmem*>(dsmem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int64_t tm, tn;
+  dtile_coords(blockIdx.x, (m + kDBM - 1) / kDBM, (n + kDBN - 1) / kDBN, tm, tn);
+  const int64_t m0 = tm * kDBM, n0 = tn * kDBN;
+  // op(A) m-contiguous unless transposed; op(B)'s n index is contiguous only when transposed
+  constexpr bool kAmn = !TA, kBmn = TB;
+  uint32_t* const st_word = status ? status : &g_native_status;
+  volatile int* const abort_flag = &s.abort_flag;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kDStages; ++i) {
+      mbar_init(&s.full[i], 32 * kDProducerWarps);  // one cp.async arrival per producer thread
+      mbar_init(&s.empty[i], kDConsumerWarps);  // one arrival per consumer warp
+    }
+    s.abort_flag = 0;
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const int64_t nkt = (k + kDBK - 1) / kDBK;
+
+  if (warp >= kDConsumerWarps) {
+    // producers: tile kt into stage kt % kDStages once the consumers released its previous use
+    const int pt = int(threadIdx.x) - 32 * kDConsumerWarps;
+    for (int64_t kt = 0; kt < nkt; ++kt) {
+      const int stg = int(kt % kDStages);
+      const int64_t use = kt / kDStages;
+      if (use > 0 && !mbar_wait(&s.empty[stg], uint32_t((use - 1) & 1), abort_flag, st_word)) break;
+      dcopy_operand<kAmn, VA>(s.a[stg], A, lda, m, k, m0, kt * kDBK, pt);
+      dcopy_operand<kBmn, VB>(s.b[stg], B, ldb, n, k, n0, kt * kDBK, pt);
+      cp_async_mbar_arrive(&s.full[stg]);
+    }
+    cp_async_wait_all();  // no copy outlives the block
+    return;
+  }
+
   const int wm = warp & 1;   // 2 warps along M (64 rows each)
   const int wn = warp >> 1;  // 4 warps along N (32 cols each)
   const int g = lane >> 2, tig = lane & 3;
-  const int64_t m0 = int64_t(blockIdx.x) * kDBM, n0 = int64_t(blockIdx.y) * kDBN;
-
   double acc[4][4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
@@ -128,33 +155,39 @@ __global__ void __launch_bounds__(kDThreads, 1)
 #pragma unroll
       for (int c = 0; c < 4; ++c) acc[i][j][c] = 0.0;
 
-  double ra[8], rb[8];
-  const int64_t nkt = (k + kDBK - 1) / kDBK;
-  dload_tile<TA, TB>(A, lda, B, ldb, m, n, k, m0, n0, 0, ra, rb);
-  dstore_tile<TA, TB>(s, 0, ra, rb);
-  __syncthreads();
-  for (int64_t kt = 0; kt < nkt; ++kt) {
-    const int buf = int(kt & 1);
-    if (kt + 1 < nkt) dload_tile<TA, TB>(A, lda, B, ldb, m, n, k, m0, n0, (kt + 1) * kDBK, ra, rb);
+  bool ok = true;
+  for (int64_t kt = 0; kt < nkt && ok; ++kt) {
+    const int stg = int(kt % kDStages);
+    if (!mbar_wait(&s.full[stg], uint32_t((kt / kDStages) & 1), abort_flag, st_word)) {
+      ok = false;
+      break;
+    }
+    const double* sa = s.a[stg];
+    const double* sb = s.b[stg];
 #pragma unroll
     for (int ks = 0; ks < kDBK / 4; ++ks) {
       const int kk = ks * 4 + tig;
       double af[4][2], bf[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        af[i][0] = s.a[buf][kk][wm * 64 + i * 16 + g];
-        af[i][1] = s.a[buf][kk][wm * 64 + i * 16 + g + 8];
+        const int r = wm * 64 + i * 16 + g;
+        af[i][0] = kAmn ? sa[kk * kDPadMN + r] : sa[r * kDPadK + kk];
+        af[i][1] = kAmn ? sa[kk * kDPadMN + r + 8] : sa[(r + 8) * kDPadK + kk];
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bf[j] = s.b[buf][wn * 32 + j * 8 + g][kk];
+      for (int j = 0; j < 4; ++j) {
+        const int c = wn * 32 + j * 8 + g;
+        bf[j] = kBmn ? sb[kk * kDPadMN + c] : sb[c * kDPadK + kk];
+      }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) dmma_16x8x4(acc[i][j], af[i][0], af[i][1], bf[j]);
     }
-    if (kt + 1 < nkt) dstore_tile<TA, TB>(s, buf ^ 1, ra, rb);
-    __syncthreads();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&s.empty[stg]);
   }
+  if (!ok) return;  // C is left as it was; the status word records the timeout
 
   // epilogue: C = alpha*acc + beta*C
 #pragma unroll
@@ -304,19 +337,31 @@ cudaError_t launch_dgemm_native(bool transA, bool transB, int64_t m, int64_t n, 
                                 const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
                                 int64_t ldc, const int* only_if_flag, cudaStream_t stream) {
   if (m <= 0 || n <= 0) return cudaSuccess;
-  dim3 grid(unsigned((m + kDBM - 1) / kDBM), unsigned((n + kDBN - 1) / kDBN));
-  if (grid.y > 65535u) return cudaErrorInvalidConfiguration;
+  const int64_t tiles = ((m + kDBM - 1) / kDBM) * ((n + kDBN - 1) / kDBN);
+  if (tiles > 0x7FFFFFFF) return cudaErrorInvalidConfiguration;
   const int smem = int(sizeof(DSmem));
   auto pick = [&](auto kern) -> cudaError_t {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    kern<<<grid, kDThreads, smem, stream>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, only_if_flag);
+    kern<<<unsigned(tiles), kDThreads, smem, stream>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, only_if_flag,
+                                                        nullptr);
     return cudaGetLastError();
   };
-  if (!transA && !transB) return pick(dgemm_dmma_kernel<false, false>);
-  if (transA && !transB) return pick(dgemm_dmma_kernel<true, false>);
-  if (!transA && transB) return pick(dgemm_dmma_kernel<false, true>);
-  return pick(dgemm_dmma_kernel<true, true>);
+  // 16-byte copies where the operand allows them
+  const bool va = reinterpret_cast<uintptr_t>(A) % 16 == 0 && lda % 2 == 0;
+  const bool vb = reinterpret_cast<uintptr_t>(B) % 16 == 0 && ldb % 2 == 0;
+  auto by_vec = [&](auto k11, auto k12, auto k21, auto k22) -> cudaError_t {
+    if (va) return vb ? pick(k22) : pick(k21);
+    return vb ? pick(k12) : pick(k11);
+  };
+#define EB2_DMMA_VARIANTS(TA_, TB_)                                                                       \
+  by_vec(dgemm_dmma_kernel<TA_, TB_, 1, 1>, dgemm_dmma_kernel<TA_, TB_, 1, 2>, dgemm_dmma_kernel<TA_, TB_, 2, 1>, \
+         dgemm_dmma_kernel<TA_, TB_, 2, 2>)
+  if (!transA && !transB) return EB2_DMMA_VARIANTS(false, false);
+  if (transA && !transB) return EB2_DMMA_VARIANTS(true, false);
+  if (!transA && transB) return EB2_DMMA_VARIANTS(false, true);
+  return EB2_DMMA_VARIANTS(true, true);
+#undef EB2_DMMA_VARIANTS
 }
 
 cudaError_t launch_sgemm_native(bool transA, bool transB, int64_t m, int64_t n, int64_t k, float alpha,

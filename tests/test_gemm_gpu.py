@@ -325,3 +325,36 @@ def test_sgemm_emulated_nonfinite_falls_back():
     oracle().oracle_sgemm(b"N", b"N", m, n, k, 1.0, P(A), lda, P(B), ldb, 0.0, P(Co), ldc)
     np.testing.assert_array_equal(np.isnan(Cg), np.isnan(Co))
     np.testing.assert_array_equal(np.isinf(Cg), np.isinf(Co))
+
+
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T"), ("T", "T")])
+@pytest.mark.parametrize("m,n,k", [(130, 258, 37), (1026, 514, 300), (8, 1030, 17)])
+def test_native_copy_width_keeps_bits(ta, tb, m, n, k):
+    """The FP64 kernel copies 16-byte pairs when an operand is 16-byte aligned with an even
+    leading dimension and single elements otherwise (ragged edges zero-filled either way): the
+    same product through both paths, and across the grouped tile raster, is bit-identical and
+    within the FP64 error bound of a float128-free double-double check."""
+    eb.set_dgemm_method(eb.METHOD_NATIVE)
+    rng = np.random.default_rng(m + n + k)
+    rows_a, cols_a = (m, k) if ta == "N" else (k, m)
+    rows_b, cols_b = (k, n) if tb == "N" else (n, k)
+    A = rng.uniform(-1, 1, (rows_a, cols_a))
+    B = rng.uniform(-1, 1, (rows_b, cols_b))
+    out = {}
+    for pad in (0, 1):  # leading dimension rows (even here) or rows + 1 (odd)
+        lda, ldb = rows_a + pad, rows_b + pad
+        tA = torch.zeros((cols_a, lda), dtype=torch.float64, device="cuda")
+        tB = torch.zeros((cols_b, ldb), dtype=torch.float64, device="cuda")
+        tA[:, :rows_a] = torch.from_numpy(A.T.copy()).cuda()
+        tB[:, :rows_b] = torch.from_numpy(B.T.copy()).cuda()
+        tC = torch.zeros((n, m), dtype=torch.float64, device="cuda")
+        rc = eb.dgemm_device(ta, tb, m, n, k, 1.0, tA, lda, tB, ldb, 0.0, tC, m)
+        torch.cuda.synchronize()
+        assert rc == eb.EB2_OK, eb.last_error()
+        out[pad] = tC.cpu().numpy().T.copy()
+    np.testing.assert_array_equal(out[0], out[1])
+    opA = A if ta == "N" else A.T
+    opB = B if tb == "N" else B.T
+    want = opA @ opB
+    bound = 2 * k * U64 * (np.abs(opA) @ np.abs(opB)) + 1e-300
+    assert np.all(np.abs(out[0] - want) <= bound)
