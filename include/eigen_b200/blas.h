@@ -241,7 +241,8 @@ int eb2_set_dgemm_tolerance(double tol);
  * hi*hi + hi*mid + mid*hi ("bf16x3"), 3 adds mid*mid + hi*lo + lo*hi ("bf16x6", default). */
 int eb2_set_sgemm_pieces(int pieces);
 /* Tile configuration of the tcgen05 kernels: 128 or 256 (one CTA per 128 x 128 or
- * 128 x 256 tile), 512 (a CTA pair per 256 x 256 tile) or 0 (= chosen per call). */
+ * 128 x 256 tile), 512 (a CTA pair per 256 x 256 tile), 1024 (one CTA per 256 x 256 tile,
+ * CRT DGEMM only: two M = 128 MMAs per K step share the B tile) or 0 (= chosen per call). */
 int eb2_set_tile_n(int tile_n);
 
 /* Launch-shape knobs of the tcgen05 kernels (normally set by the tuner): row-tiles per
