@@ -154,17 +154,33 @@ constexpr int kNormThreads = 256;
 template <int ROWS, int COLS, int THREADS>
 __device__ __forceinline__ void load_tile(double (&tile)[ROWS][COLS + 1], const double* __restrict__ X, int64_t r0,
                                           int64_t l0, int64_t rows, int64_t cols, int64_t sr, int64_t sl) {
-  static_assert((ROWS * COLS) % THREADS == 0, "whole tile per pass");
+  static_assert(THREADS % ROWS == 0 && THREADS % COLS == 0, "a fixed row or column per thread");
   constexpr int kPer = ROWS * COLS / THREADS;
-  const bool rows_contig = (sr == 1);
+  const int t = int(threadIdx.x);
+  if (sr == 1) {
+    // lanes along the rows (contiguous); each thread keeps its row and steps through columns
+    constexpr int kStep = THREADS / ROWS;
+    const int rr = t % ROWS, l_first = t / ROWS;
+    const int64_t r = r0 + rr;
+    const double* src = X + r + (l0 + l_first) * sl;
+    uint32_t dst = smem_u32(&tile[rr][l_first]);
 #pragma unroll
-  for (int q = 0; q < kPer; ++q) {
-    const int idx = int(threadIdx.x) + q * THREADS;
-    const int rr = rows_contig ? idx % ROWS : idx / COLS;
-    const int ll = rows_contig ? idx / ROWS : idx % COLS;
-    const int64_t r = r0 + rr, l = l0 + ll;
-    const bool valid = r < rows && l < cols;
-    cp_async_elem<8>(smem_u32(&tile[rr][ll]), valid ? X + r * sr + l * sl : X, valid);
+    for (int q = 0; q < kPer; ++q, src += kStep * sl, dst += kStep * 8) {
+      const bool valid = r < rows && l0 + l_first + q * kStep < cols;
+      cp_async_elem<8>(dst, valid ? src : X, valid);
+    }
+  } else {
+    // lanes along the columns; each thread keeps its column and steps through rows
+    constexpr int kStep = THREADS / COLS;
+    const int ll = t % COLS, r_first = t / COLS;
+    const int64_t l = l0 + ll;
+    const double* src = X + (r0 + r_first) * sr + l * sl;
+    uint32_t dst = smem_u32(&tile[r_first][ll]);
+#pragma unroll
+    for (int q = 0; q < kPer; ++q, src += kStep * sr, dst += kStep * (COLS + 1) * 8) {
+      const bool valid = l < cols && r0 + r_first + q * kStep < rows;
+      cp_async_elem<8>(dst, valid ? src : X, valid);
+    }
   }
   cp_async_commit();
   cp_async_wait<0>();
@@ -212,51 +228,43 @@ __global__ void __launch_bounds__(kNormThreads) crt_scan_norm_kernel(const doubl
   const int64_t r = r0 + rr;
   // the spread statistic: the first 64 columns of every 512 (block-uniform)
   const bool stat = spread != nullptr && (l0 & 511) == 0;
-  // maxima of |x| as doubles (their bit patterns order the same way), the largest high word
-  // for NaN / Inf (a NaN drops out of fmax but not out of the high-word maximum)
-  double dmax = 0.0, dmax64 = 0.0;
-  uint32_t hmax = 0u, hmax64 = 0u;
+  // bit patterns of |x| order like the values, NaN above +Inf
+  unsigned long long mb = 0, mb64 = 0;
   int esum = 0, ecnt = 0;
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
-    const double a = fabs(tile[rr][sub + 8 * j]);
-    const uint32_t h = uint32_t(__double2hiint(a));
-    dmax = fmax(dmax, a);
-    hmax = max(hmax, h);
+    const unsigned long long bits =
+        static_cast<unsigned long long>(__double_as_longlong(fabs(tile[rr][sub + 8 * j])));
+    mb = bits > mb ? bits : mb;
     if (stat && j < 8) {
-      dmax64 = fmax(dmax64, a);
-      hmax64 = max(hmax64, h);
-      if (a != 0.0) {
-        esum += int(h >> 20);
+      mb64 = bits > mb64 ? bits : mb64;
+      if (bits) {
+        esum += int(bits >> 52);
         ++ecnt;
       }
     }
   }
 #pragma unroll
   for (int o = 4; o > 0; o >>= 1) {
-    dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
-    hmax = max(hmax, __shfl_xor_sync(0xffffffffu, hmax, o));
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, mb, o);
+    mb = other > mb ? other : mb;
     if (stat) {
-      dmax64 = fmax(dmax64, __shfl_xor_sync(0xffffffffu, dmax64, o));
-      hmax64 = max(hmax64, __shfl_xor_sync(0xffffffffu, hmax64, o));
+      const unsigned long long other64 = __shfl_xor_sync(0xffffffffu, mb64, o);
+      mb64 = other64 > mb64 ? other64 : mb64;
       esum += __shfl_xor_sync(0xffffffffu, esum, o);
       ecnt += __shfl_xor_sync(0xffffffffu, ecnt, o);
     }
   }
-  // bit pattern of the largest |x|, or of at least +Inf when the chunk holds a NaN or an Inf
-  const unsigned long long mb = hmax >= 0x7FF00000u ? (static_cast<unsigned long long>(hmax) << 32)
-                                                     : static_cast<unsigned long long>(__double_as_longlong(dmax));
-  const unsigned long long mb64 = hmax64 >= 0x7FF00000u
-                                      ? (static_cast<unsigned long long>(hmax64) << 32)
-                                      : static_cast<unsigned long long>(__double_as_longlong(dmax64));
   unsigned long long s = 0;
   int e = 0;
   if (mb != 0 && mb < kInfBitsCrt) {
     e = frexp_exp(mb);
+    // scale2(x, -e) with its two power-of-two factors formed once
+    const double f1 = exp2_int((-e) / 2), f2 = exp2_int(-e - (-e) / 2);
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const double x = tile[rr][sub + 8 * j];
-      const double xs = scale2(x, -e);
+      const double xs = __dmul_rn(__dmul_rn(x, f1), f2);
       // ceil(v) for v = rn(x'^2) 2^32 in [0, 2^32]: v + 2^52 rounded up is 2^52 + ceil(v)
       // exactly, read from its bits (no rounding or conversion instruction)
       const double v = __dmul_rn(__dmul_rn(xs, xs), 4294967296.0);
@@ -513,8 +521,10 @@ __global__ void __launch_bounds__(kSplitThreadsCrt, 3) crt_split_kernel(
       for (int l = 0; l < n; ++l) store_residues_wide(kModConst[l], ch, neg, dst + size_t(l) * plane);
     } else {
       SplitEntry e[kSplitEntries];
+      const double f1 = exp2_int(m / 2), f2 = exp2_int(m - m / 2);  // scale2(., m) factors
 #pragma unroll
-      for (int j = 0; j < kSplitEntries; ++j) e[j] = split_entry(__double2ll_rz(scale2(tile[rr][cb + j], m)));  // trunc
+      for (int j = 0; j < kSplitEntries; ++j)
+        e[j] = split_entry(__double2ll_rz(__dmul_rn(__dmul_rn(tile[rr][cb + j], f1), f2)));  // trunc
       if constexpr (NT > 0) {
         store_residues_static<0, NT>(e, dst, plane);
       } else {
