@@ -161,6 +161,29 @@ __global__ void __launch_bounds__(kTriVecs) tri_block_multiply_kernel(const T* _
   }
 }
 
+// Four consecutive elements of a 16-byte aligned shared-memory row as vector accesses.
+__device__ __forceinline__ void load4(double (&v)[4], const double* p) {
+  const double2 lo = *reinterpret_cast<const double2*>(p), hi = *reinterpret_cast<const double2*>(p + 2);
+  v[0] = lo.x;
+  v[1] = lo.y;
+  v[2] = hi.x;
+  v[3] = hi.y;
+}
+__device__ __forceinline__ void load4(float (&v)[4], const float* p) {
+  const float4 q = *reinterpret_cast<const float4*>(p);
+  v[0] = q.x;
+  v[1] = q.y;
+  v[2] = q.z;
+  v[3] = q.w;
+}
+__device__ __forceinline__ void store4(double* p, const double (&v)[4]) {
+  *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+  *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void store4(float* p, const float (&v)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+
 // x := E^-1 x for a diagonal block E of up to kPanelMax rows and `count` vectors (laid out
 // as above), kPanelVecs per CTA, the CTA's vectors resident in shared memory for the whole
 // block.  Blocked substitution over 32-row sub-blocks:
@@ -239,11 +262,23 @@ __global__ void __launch_bounds__(kPanelThreads) tri_panel_solve_kernel(const T*
     // rows below: x[r] -= E'(r, jb..jb+bs) x[jb..jb+bs], kPanelChunk rows per pass
     for (int r0 = jb + bs; r0 < nb; r0 += kPanelChunk) {
       const int rows = nb - r0 < kPanelChunk ? nb - r0 : kPanelChunk;
-      __syncthreads();  // the sub-block solve is done / the previous chunk's Cs is consumed
-      for (int idx = tid; idx < kPanelSub * kPanelChunk; idx += kPanelThreads) {
+      // every thread's coefficient loads are issued before its first shared store
+      constexpr int kPerThread = kPanelSub * kPanelChunk / kPanelThreads;
+      T cv[kPerThread];
+#pragma unroll
+      for (int q = 0; q < kPerThread; ++q) {
+        const int idx = tid + q * kPanelThreads;
         const int rr = row_fast ? idx % kPanelChunk : idx / kPanelSub;
         const int c = row_fast ? idx / kPanelChunk : idx % kPanelSub;
-        Cs[c * kPanelChunk + rr] = (rr < rows && c < bs) ? E[ro(r0 + rr) * er + ro(jb + c) * ec] : T(0);
+        cv[q] = (rr < rows && c < bs) ? E[ro(r0 + rr) * er + ro(jb + c) * ec] : T(0);
+      }
+      __syncthreads();  // the sub-block solve is done / the previous chunk's Cs is consumed
+#pragma unroll
+      for (int q = 0; q < kPerThread; ++q) {
+        const int idx = tid + q * kPanelThreads;
+        const int rr = row_fast ? idx % kPanelChunk : idx / kPanelSub;
+        const int c = row_fast ? idx / kPanelChunk : idx % kPanelSub;
+        Cs[c * kPanelChunk + rr] = cv[q];
       }
       __syncthreads();
       T acc[4][4];
@@ -253,11 +288,10 @@ __global__ void __launch_bounds__(kPanelThreads) tri_panel_solve_kernel(const T*
         for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
 #pragma unroll 8
       for (int c = 0; c < kPanelSub; ++c) {
+        // four consecutive coefficients / vector entries as 16-byte loads (no bank conflicts)
         T a[4], b[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = Cs[c * kPanelChunk + 4 * ty + i];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) b[j] = Xs[(jb + (c < bs ? c : 0)) * kPanelXld + 4 * tx + j];
+        load4(a, Cs + c * kPanelChunk + 4 * ty);
+        load4(b, Xs + (jb + (c < bs ? c : 0)) * kPanelXld + 4 * tx);
         if (c < bs) {
 #pragma unroll
           for (int i = 0; i < 4; ++i)
@@ -269,8 +303,12 @@ __global__ void __launch_bounds__(kPanelThreads) tri_panel_solve_kernel(const T*
       for (int i = 0; i < 4; ++i) {
         const int rr = 4 * ty + i;
         if (rr < rows) {
+          T* xp = Xs + (r0 + rr) * kPanelXld + 4 * tx;
+          T x4[4];
+          load4(x4, xp);
 #pragma unroll
-          for (int j = 0; j < 4; ++j) Xs[(r0 + rr) * kPanelXld + 4 * tx + j] -= acc[i][j];
+          for (int j = 0; j < 4; ++j) x4[j] -= acc[i][j];
+          store4(xp, x4);
         }
       }
     }
