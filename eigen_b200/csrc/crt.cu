@@ -657,7 +657,6 @@ struct CrtRecParams {
   double* save;
   int64_t ld_save;
   int cols_per_block;  // columns one block handles per pass (fewer when the grid would be small)
-  int vec_store;       // C 16-byte aligned with an even ldc (the save array likewise)
   int uplo;            // 0: all of C; 1: i <= j only; 2: i >= j only
 };
 
@@ -951,25 +950,13 @@ __global__ void __launch_bounds__(256, 4) crt_reconstruct128_kernel(const __grid
   if (EST) crt_reduce_energies(R, e_acc, v_acc);
 }
 
-// The exact double of a 32-bit unsigned integer without a conversion instruction: the word
-// under the exponent of 2^52, minus 2^52.
-__device__ __forceinline__ double u32_to_double(uint32_t x) { return __hiloint2double(0x43300000, int(x)) - 0x1p52; }
-
-// RN(C'_ij 2^escale) from the residues rc[0..N) of one entry (8 <= N <= 16), in 32-bit limbs:
-//   * S = sum_g Q_g R_g as four 64-bit limb columns, carried into S mod 2^128 and the part
-//     above 2^128;
-//   * q = rint(S / P) from the bits of S above 2^32 in FP64 (off by one at most, near a
-//     half-integer), R = S - q P modulo 2^128 with signed 64-bit borrows, and the range fix
-//     only when R's top limbs do not already place it in [-P/2, P/2);
-//   * the magnitude rounded to nearest even from its top 64 bits and a sticky bit, written
-//     straight into the bits of the scaled double when that is a normal number (scaling by
-//     2^escale is then exact).  Subnormal and overflowing results take the per-row kernel's
-//     steps (RN of the top 64 bits, then scale_exp), so every result is bit for bit that
-//     kernel's.
 // RN(R 2^escale) for R = (r3 r2 r1 r0) in 128-bit two's complement, congruent to C' modulo P
-// and within one P of [-P/2, P/2): the range fix, the magnitude's top 64 bits with a sticky
-// bit, and the double written from its rounded significand (or, for subnormal and
-// overflowing results, RN of the top bits and scale_exp).
+// and within one P of [-P/2, P/2): the range fix only when R's top 64-bit window does not
+// already place it in [-P/2, P/2); the magnitude's top 64 bits and a sticky bit, rounded to
+// nearest even and written straight into the bits of the scaled double when that is a
+// normal number (scaling by 2^escale is then exact).  Subnormal and overflowing results take
+// the per-row kernel's steps (RN of the top 64 bits, then scale_exp), so every result is bit
+// for bit that kernel's.
 template <int N>
 __device__ __forceinline__ double crt_round(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3, int escale) {
   constexpr uint32_t P0 = kCrtTableC.P[N][0], P1 = kCrtTableC.P[N][1], P2 = kCrtTableC.P[N][2], P3 = kCrtTableC.P[N][3];
@@ -1051,40 +1038,11 @@ __device__ __forceinline__ double crt_round(uint32_t r0, uint32_t r1, uint32_t r
   return __longlong_as_double(static_cast<long long>(bits));
 }
 
-// The second half of crt_entry_fast: RN(C' 2^escale) from S = sum_q acc[q] 2^(32q) (each
-// column below 2^62).
-template <int N>
-__device__ __forceinline__ double crt_finish(const unsigned long long (&acc)[4], double P_inv32, int escale) {
-  static_assert(N >= kCrtMinModuli && N <= 16, "P at least 2^63 and below 2^128");
-  // S = top 2^128 + s3 2^96 + s2 2^64 + s1 2^32 + s0
-  const uint32_t s0 = uint32_t(acc[0]);
-  const unsigned long long t1 = acc[1] + (acc[0] >> 32);
-  const unsigned long long t2 = acc[2] + (t1 >> 32);
-  const unsigned long long t3 = acc[3] + (t2 >> 32);
-  const uint32_t s1 = uint32_t(t1), s2 = uint32_t(t2), s3 = uint32_t(t3), top = uint32_t(t3 >> 32);
-  // S / 2^32 in FP64 (s0 < 2^32 <= 2^-31 P left out), then q in the low word of
-  // rint(S / P) + 1.5 2^52 (0 <= q < 2^31)
-  const double hi = fma(u32_to_double(top), 0x1p32, u32_to_double(s3));
-  const double mid = fma(hi, 0x1p32, u32_to_double(s2));
-  const double sd = fma(mid, 0x1p32, u32_to_double(s1));
-  const uint32_t q = uint32_t(__double2loint(fma(sd, P_inv32, 0x1.8p52)));
-  // R = S - q P modulo 2^128
-  constexpr uint32_t P0 = kCrtTableC.P[N][0], P1 = kCrtTableC.P[N][1], P2 = kCrtTableC.P[N][2], P3 = kCrtTableC.P[N][3];
-  long long d = static_cast<long long>(s0) - static_cast<long long>(static_cast<unsigned long long>(q) * P0);
-  uint32_t r0 = uint32_t(d);
-  d = (d >> 32) + static_cast<long long>(s1) - static_cast<long long>(static_cast<unsigned long long>(q) * P1);
-  uint32_t r1 = uint32_t(d);
-  d = (d >> 32) + static_cast<long long>(s2) - static_cast<long long>(static_cast<unsigned long long>(q) * P2);
-  uint32_t r2 = uint32_t(d);
-  d = (d >> 32) + static_cast<long long>(s3) - static_cast<long long>(static_cast<unsigned long long>(q) * P3);
-  uint32_t r3 = uint32_t(d);
-  return crt_round<N>(r0, r1, r2, r3, escale);
-}
-
-// crt_finish for limb columns below 2^52 (the tensor-core sum gives columns below 2^46): the
-// columns are exact doubles by one integer add and one FP64 subtraction, q comes from
-// acc[1..3] (acc[0] / P < 2^-11 left out; q is off by one at most, which the range fix
-// absorbs), and R = S - q P takes its borrows column by column without carrying S first.
+// RN(C' 2^escale) from S = sum_q acc[q] 2^(32q), limb columns below 2^52 (the tensor-core sum
+// gives columns below 2^46): the columns are exact doubles by one integer add and one FP64
+// subtraction, q = rint(S / P) comes from acc[1..3] (acc[0] / P < 2^-11 left out; q is off
+// by one at most, which the range fix absorbs), and R = S - q P takes its borrows column by
+// column without carrying S first.
 template <int N>
 __device__ __forceinline__ double crt_finish_small(const unsigned long long (&acc)[4], double P_inv32, int escale) {
   static_assert(N >= kCrtMinModuli && N <= 16, "P at least 2^63 and below 2^128");
@@ -1104,19 +1062,6 @@ __device__ __forceinline__ double crt_finish_small(const unsigned long long (&ac
   return crt_round<N>(uint32_t(d0), uint32_t(d1), uint32_t(d2), uint32_t(d3), escale);
 }
 
-template <int N>
-__device__ __forceinline__ double crt_entry_fast(const uint32_t (&rc)[N], double P_inv32, int escale) {
-  unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};
-#pragma unroll
-  for (int g = 0; 2 * g < N; ++g) {
-    uint32_t Rg = rc[2 * g] * kCrtPairs.X[N][2 * g];
-    if (2 * g + 1 < N) Rg += rc[2 * g + 1] * kCrtPairs.X[N][2 * g + 1];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) acc[q] += static_cast<unsigned long long>(Rg) * kCrtPairs.Q[N][g][q];
-  }
-  return crt_finish<N>(acc, P_inv32, escale);
-}
-
 // ---- reconstruction with the weighted residue sum on the tensor cores
 // S = sum_l r_l W_l = sum_b 2^(8b) T_b with T_b = sum_l r_l w_lb, w_lb byte b of W_l (W_l < P <
 // 2^128: 16 bytes) and T_b < 16 * 255 * 255 < 2^20: a [32 entries x 16 moduli] x [16 moduli x 16
@@ -1134,8 +1079,8 @@ __device__ __forceinline__ void mma_u8_16x8x16(int (&d)[4], uint32_t a0, uint32_
 // the MMAs leave with lane (g, c) the byte sums T_2c, T_2c+1, T_8+2c, T_9+2c of those four
 // rows.  The warp passes them through its own rows of shared memory so that lane L reads all
 // sixteen sums of row i0 + L and forms S in four 32-bit-aligned columns with multiply-adds;
-// the tail (crt_finish) and the store follow.  Bit for bit the other reconstruction kernels:
-// S is the same integer.
+// the tail (crt_finish_small) and the store follow.  Bit for bit the per-row kernel: S is the
+// same integer and it is rounded the same way.
 constexpr int kRecStageStride = 18;  // words per staged row (16 byte sums + 2)
 template <int N, bool EST>
 __global__ void __launch_bounds__(256, 4) crt_reconstruct_mma_kernel(const __grid_constant__ CrtRecParams R) {
@@ -1249,126 +1194,6 @@ __global__ void __launch_bounds__(256, 4) crt_reconstruct_mma_kernel(const __gri
   if (EST) crt_reduce_energies(R, e_acc, v_acc);
 }
 
-// The same, four consecutive rows per thread: one 32-bit load per modulus and column brings
-// the residues of rows i0 .. i0+3 (a warp reads 128 contiguous bytes of a residue plane), the
-// row scales stay in registers across the columns, the entries go through crt_entry_fast,
-// the estimate's exponent terms are summed once per group of four rows, and interior groups
-// store C (and read the old C) as two 16-byte vectors.  Needs the residue base, ld_res and the
-// plane size to be multiples of 4 and ld_res >= m rounded up to 4 (the launcher checks).  Bit
-// for bit the per-row kernel; only the order of the estimate's partial sums differs.
-constexpr int kRecRowsPerThread = 4;
-template <int N, bool EST>
-__global__ void __launch_bounds__(256, 2) crt_reconstruct128x4_kernel(const __grid_constant__ CrtRecParams R) {
-  if (R.skip_if_flag && *R.skip_if_flag) return;
-  CrtStoreCtx sc = store_ctx(R);
-  sc.estimate = EST;
-  const uint8_t* const res = R.res;
-  const int64_t ld_res = R.ld_res, plane = R.plane, m = R.m, ncols = R.ncols;
-  const int uplo = R.uplo;
-  const bool vec = R.vec_store != 0;
-  const double P_inv32 = R.P_inv * 0x1p32;
-  const int64_t i0 = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) * kRecRowsPerThread;
-  double e_acc = 0.0, v_acc = 0.0;
-  int mu_i[kRecRowsPerThread];
-#pragma unroll
-  for (int q = 0; q < kRecRowsPerThread; ++q) mu_i[q] = i0 + q < m ? sc.mu_a[i0 + q] : kCrtZeroRow;
-  // estimate: sum_q 2^(2(b - mu_q - nu_j)) = rowsum 2^(2(T - nu_j)) over the nonzero rows of
-  // the group, T the largest b - mu_q (every term of rowsum at most 1)
-  int T = -0x40000000;
-  double rowsum = 0.0;
-  if (EST) {
-#pragma unroll
-    for (int q = 0; q < kRecRowsPerThread; ++q)
-      if (mu_i[q] != kCrtZeroRow) T = max(T, sc.b - mu_i[q]);
-#pragma unroll
-    for (int q = 0; q < kRecRowsPerThread; ++q)
-      if (mu_i[q] != kCrtZeroRow) rowsum += exp2_int(2 * (sc.b - mu_i[q] - T));
-  }
-  const int cpb = R.cols_per_block;
-  const int64_t jstep = int64_t(gridDim.y) * cpb;
-  for (int64_t j0 = int64_t(blockIdx.y) * cpb; i0 < m && j0 < ncols; j0 += jstep) {
-    // the columns that some row of the group keeps
-    int64_t jb = j0, j1 = j0 + cpb < ncols ? j0 + cpb : ncols;
-    if (uplo == 1 && jb < i0) jb = i0;                                          // i <= j
-    if (uplo == 2 && j1 > i0 + kRecRowsPerThread) j1 = i0 + kRecRowsPerThread;  // i >= j
-    if (jb >= j1) continue;
-    uint32_t wn[N];
-#pragma unroll
-    for (int l = 0; l < N; ++l) wn[l] = __ldg(reinterpret_cast<const uint32_t*>(res + jb * ld_res + i0 + l * plane));
-    for (int64_t j = jb; j < j1; ++j) {
-      uint32_t wc[N];
-#pragma unroll
-      for (int l = 0; l < N; ++l) wc[l] = wn[l];
-      if (j + 1 < j1) {
-#pragma unroll
-        for (int l = 0; l < N; ++l)
-          wn[l] = __ldg(reinterpret_cast<const uint32_t*>(res + (j + 1) * ld_res + i0 + l * plane));
-      }
-      const int nu_j = sc.mu_b[j];
-      double v[kRecRowsPerThread];
-      bool all = true;
-      uint32_t keep = 0;
-#pragma unroll
-      for (int q = 0; q < kRecRowsPerThread; ++q) {
-        const int64_t i = i0 + q;
-        const bool k = i < m && (uplo == 0 || (uplo == 1 ? i <= j : i >= j));
-        all = all && k;
-        v[q] = 0.0;
-        if (k) {
-          keep |= 1u << q;
-          uint32_t rc[N];
-#pragma unroll
-          for (int l = 0; l < N; ++l) rc[l] = (wc[l] >> (8 * q)) & 0xFFu;
-          v[q] = __dmul_rn(sc.alpha, crt_entry_fast<N>(rc, P_inv32, -mu_i[q] - nu_j));
-          if (EST) v_acc += v[q] * v[q];
-        }
-      }
-      if (EST && nu_j != kCrtZeroRow) {
-        if (all) {
-          if (rowsum != 0.0) e_acc += rowsum * exp2_int(2 * (T - nu_j));
-        } else {
-#pragma unroll
-          for (int q = 0; q < kRecRowsPerThread; ++q)
-            if (((keep >> q) & 1u) && mu_i[q] != kCrtZeroRow) e_acc += exp2_int(2 * (sc.b - mu_i[q] - nu_j));
-        }
-      }
-      if (!sc.write_c) continue;
-      double* c = sc.C + j * sc.ldc + i0;
-      if (all && vec) {
-        double2* c2 = reinterpret_cast<double2*>(c);
-        if (sc.beta == 0.0) {
-          c2[0] = make_double2(v[0], v[1]);
-          c2[1] = make_double2(v[2], v[3]);
-        } else {
-          const double2 o0 = c2[0], o1 = c2[1];
-          if (sc.save) {
-            double* s = sc.save + j * sc.ld_save + i0;
-            s[0] = o0.x;
-            s[1] = o0.y;
-            s[2] = o1.x;
-            s[3] = o1.y;
-          }
-          c2[0] = make_double2(__fma_rn(sc.beta, o0.x, v[0]), __fma_rn(sc.beta, o0.y, v[1]));
-          c2[1] = make_double2(__fma_rn(sc.beta, o1.x, v[2]), __fma_rn(sc.beta, o1.y, v[3]));
-        }
-      } else {
-#pragma unroll
-        for (int q = 0; q < kRecRowsPerThread; ++q) {
-          if (!((keep >> q) & 1u)) continue;
-          if (sc.beta == 0.0) {
-            c[q] = v[q];
-          } else {
-            const double old = c[q];
-            if (sc.save) sc.save[j * sc.ld_save + i0 + q] = old;
-            c[q] = __fma_rn(sc.beta, old, v[q]);
-          }
-        }
-      }
-    }
-  }
-  if (EST) crt_reduce_energies(R, e_acc, v_acc);
-}
-
 // Split-K: residue planes (l, s), s = 0 .. splits-1, of modulus l added modulo p_l into
 // plane (l, 0); 16 bytes per thread, one modulus per grid row.
 __global__ void __launch_bounds__(256) crt_merge_splits_kernel(uint8_t* __restrict__ cres, int64_t plane, int splits) {
@@ -1395,20 +1220,13 @@ __global__ void __launch_bounds__(256) crt_merge_splits_kernel(uint8_t* __restri
 }
 
 template <int N>
-void launch_rec128(bool est, bool x4, bool mma, dim3 grid, cudaStream_t stream, const CrtRecParams& R) {
+void launch_rec128(bool est, bool mma, dim3 grid, cudaStream_t stream, const CrtRecParams& R) {
   if constexpr (N >= kCrtMinModuli) {
     if (mma) {
       if (est)
         crt_reconstruct_mma_kernel<N, true><<<grid, 256, 0, stream>>>(R);
       else
         crt_reconstruct_mma_kernel<N, false><<<grid, 256, 0, stream>>>(R);
-      return;
-    }
-    if (x4) {
-      if (est)
-        crt_reconstruct128x4_kernel<N, true><<<grid, 256, 0, stream>>>(R);
-      else
-        crt_reconstruct128x4_kernel<N, false><<<grid, 256, 0, stream>>>(R);
       return;
     }
   }
@@ -1571,15 +1389,11 @@ cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t 
   R.save = args.save;
   R.ld_save = args.ld_save;
   R.uplo = args.uplo;
-  // four rows per thread where the residue planes allow 32-bit loads
-  const bool x4 = args.moduli >= kCrtMinModuli && args.moduli <= 16 && reinterpret_cast<uintptr_t>(args.cres) % 4 == 0 &&
-                  args.ld_res % 4 == 0 && args.plane % 4 == 0 && args.ld_res >= (args.m + 3) / 4 * 4;
-  // the tensor-core sum: whole warps of 32 rows read residues, so the planes must hold them
-  const bool mma = x4 && args.ld_res % 32 == 0 && args.ld_res >= (args.m + 31) / 32 * 32;
-  const int64_t rows_per_block = mma ? 256 : (x4 ? 256 * kRecRowsPerThread : 256);
-  const bool c_vec = reinterpret_cast<uintptr_t>(args.C) % 16 == 0 && args.ldc % 2 == 0;
-  const bool s_vec = args.save == nullptr || (reinterpret_cast<uintptr_t>(args.save) % 16 == 0 && args.ld_save % 2 == 0);
-  R.vec_store = (c_vec && s_vec) ? 1 : 0;
+  // the tensor-core sum: whole warps of 32 rows read the residue planes 32 bits at a time, so
+  // the planes must be 4-byte aligned and hold every row of those warps
+  const bool mma = args.moduli >= kCrtMinModuli && args.moduli <= 16 && reinterpret_cast<uintptr_t>(args.cres) % 4 == 0 &&
+                   args.ld_res % 32 == 0 && args.plane % 4 == 0 && args.ld_res >= (args.m + 31) / 32 * 32;
+  const int64_t rows_per_block = 256;
   const unsigned gx = unsigned((args.m + rows_per_block - 1) / rows_per_block);
   // up to kRecCols columns per block, fewer while the grid is under ~4 blocks per SM
   int64_t cpb = int64_t(gx) * args.n / (4 * 148);
@@ -1590,15 +1404,15 @@ cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t 
   const dim3 grid(gx, gy);
   const bool est = args.err_sq != nullptr;
   switch (args.moduli) {
-    case 8: launch_rec128<8>(est, x4, mma, grid, stream, R); break;
-    case 9: launch_rec128<9>(est, x4, mma, grid, stream, R); break;
-    case 10: launch_rec128<10>(est, x4, mma, grid, stream, R); break;
-    case 11: launch_rec128<11>(est, x4, mma, grid, stream, R); break;
-    case 12: launch_rec128<12>(est, x4, mma, grid, stream, R); break;
-    case 13: launch_rec128<13>(est, x4, mma, grid, stream, R); break;
-    case 14: launch_rec128<14>(est, x4, mma, grid, stream, R); break;
-    case 15: launch_rec128<15>(est, x4, mma, grid, stream, R); break;
-    case 16: launch_rec128<16>(est, x4, mma, grid, stream, R); break;
+    case 8: launch_rec128<8>(est, mma, grid, stream, R); break;
+    case 9: launch_rec128<9>(est, mma, grid, stream, R); break;
+    case 10: launch_rec128<10>(est, mma, grid, stream, R); break;
+    case 11: launch_rec128<11>(est, mma, grid, stream, R); break;
+    case 12: launch_rec128<12>(est, mma, grid, stream, R); break;
+    case 13: launch_rec128<13>(est, mma, grid, stream, R); break;
+    case 14: launch_rec128<14>(est, mma, grid, stream, R); break;
+    case 15: launch_rec128<15>(est, mma, grid, stream, R); break;
+    case 16: launch_rec128<16>(est, mma, grid, stream, R); break;
     default: crt_reconstruct_kernel<<<grid, 256, 0, stream>>>(R); break;  // other counts: 192-bit path
   }
   return cudaGetLastError();
