@@ -470,14 +470,42 @@ __device__ __forceinline__ void store_residues(const CrtModConst& k, const Split
   *reinterpret_cast<uint32_t*>(dst) = pack_low_bytes(r[0], r[1], r[2], r[3]);
 }
 
-// Moduli L .. NT-1 with their constants as compile-time immediates.
+// The residues of two odd moduli pa, pb from one s = hi c + lo, c = 2^32 mod pa pb (< 2^16):
+// |s| < 2^47 is exact and congruent to t modulo both, and |s / p| < 2^40 keeps RN(1/p)'s
+// error below 2^-13, under the 1/(2p) distance of s/p from a half-integer, so each q is
+// again the exact rounding.  Per modulus 1.5 FMAs and 1.5 multiply-adds instead of 2 and 2.
+template <int LA>
+__device__ __forceinline__ void store_residue_pair(const SplitEntry (&e)[kSplitEntries], int8_t* dst_a,
+                                                   int8_t* dst_b) {
+  constexpr CrtModConst ka = crt_mod_const(LA), kb = crt_mod_const(LA + 1);
+  static_assert((ka.p & 1u) && (kb.p & 1u) && ka.p * kb.p < 65536u, "two odd moduli, product below 2^16");
+  constexpr uint32_t c = pow2_mod_const(32, ka.p * kb.p);
+  uint32_t ra[kSplitEntries], rb[kSplitEntries];
+#pragma unroll
+  for (int j = 0; j < kSplitEntries; ++j) {
+    const double s = fma(e[j].dh, double(c), e[j].dl);
+    const uint32_t u = e[j].lo + uint32_t(e[j].hi) * c;
+    ra[j] = u - uint32_t(__double2loint(fma(s, ka.inv_p, 0x1.8p52))) * ka.p;
+    rb[j] = u - uint32_t(__double2loint(fma(s, kb.inv_p, 0x1.8p52))) * kb.p;
+  }
+  *reinterpret_cast<uint32_t*>(dst_a) = pack_low_bytes(ra[0], ra[1], ra[2], ra[3]);
+  *reinterpret_cast<uint32_t*>(dst_b) = pack_low_bytes(rb[0], rb[1], rb[2], rb[3]);
+}
+
+// Moduli L .. NT-1 with their constants as compile-time immediates; consecutive odd moduli
+// in pairs.
 template <int L, int NT>
 __device__ __forceinline__ void store_residues_static(const SplitEntry (&e)[kSplitEntries], int8_t* dst,
                                                       size_t plane) {
   if constexpr (L < NT) {
     constexpr CrtModConst k = crt_mod_const(L);
-    store_residues(k, e, dst + size_t(L) * plane);
-    store_residues_static<L + 1, NT>(e, dst, plane);
+    if constexpr ((k.p & 1u) != 0u && L + 1 < NT) {
+      store_residue_pair<L>(e, dst + size_t(L) * plane, dst + size_t(L + 1) * plane);
+      store_residues_static<L + 2, NT>(e, dst, plane);
+    } else {
+      store_residues(k, e, dst + size_t(L) * plane);
+      store_residues_static<L + 1, NT>(e, dst, plane);
+    }
   }
 }
 
@@ -950,43 +978,12 @@ __global__ void __launch_bounds__(256, 4) crt_reconstruct128_kernel(const __grid
   if (EST) crt_reduce_energies(R, e_acc, v_acc);
 }
 
-// RN(R 2^escale) for R = (r3 r2 r1 r0) in 128-bit two's complement, congruent to C' modulo P
-// and within one P of [-P/2, P/2): the range fix only when R's top 64-bit window does not
-// already place it in [-P/2, P/2); the magnitude's top 64 bits and a sticky bit, rounded to
-// nearest even and written straight into the bits of the scaled double when that is a
-// normal number (scaling by 2^escale is then exact).  Subnormal and overflowing results take
-// the per-row kernel's steps (RN of the top 64 bits, then scale_exp), so every result is bit
-// for bit that kernel's.
-template <int N>
-__device__ __forceinline__ double crt_round(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3, int escale) {
-  constexpr uint32_t P0 = kCrtTableC.P[N][0], P1 = kCrtTableC.P[N][1], P2 = kCrtTableC.P[N][2], P3 = kCrtTableC.P[N][3];
-  // R lies in [-half, half) when the 64-bit window of R at half's two top limbs is in
-  // [-Hw, Hw) and the limbs above the window extend its sign: nothing to fix then
-  constexpr int kW = kCrtTableC.half[N][3] != 0 ? 2 : (kCrtTableC.half[N][2] != 0 ? 1 : 0);
-  constexpr long long Hw = static_cast<long long>((static_cast<unsigned long long>(kCrtTableC.half[N][kW + 1]) << 32) |
-                                                  kCrtTableC.half[N][kW]);
-  const uint32_t rl[4] = {r0, r1, r2, r3};
-  const long long win = static_cast<long long>((static_cast<unsigned long long>(rl[kW + 1]) << 32) | rl[kW]);
-  const uint32_t ext = win < 0 ? 0xFFFFFFFFu : 0u;
-  bool in_range = win >= -Hw && win < Hw;
-#pragma unroll
-  for (int t = kW + 2; t < 4; ++t) in_range = in_range && rl[t] == ext;
-  if (!in_range) {
-    using u128 = unsigned __int128;
-    using s128 = __int128;
-    const u128 P = (u128(P3) << 96) | (u128(P2) << 64) | (u128(P1) << 32) | u128(P0);
-    const s128 half = s128(P >> 1);
-    s128 r = s128((u128(r3) << 96) | (u128(r2) << 64) | (u128(r1) << 32) | u128(r0));
-    if (r > half)
-      r -= s128(P);
-    else if (r < -half)
-      r += s128(P);
-    const u128 ur = u128(r);
-    r0 = uint32_t(ur);
-    r1 = uint32_t(ur >> 32);
-    r2 = uint32_t(ur >> 64);
-    r3 = uint32_t(ur >> 96);
-  }
+// RN(|R| 2^escale) with its sign, for R = (r3 r2 r1 r0) in [-P/2, P/2) (128-bit two's
+// complement): the magnitude's top 64 bits and a sticky bit, rounded to nearest even and
+// written straight into the bits of the scaled double when that is a normal number (scaling
+// by 2^escale is then exact).  Subnormal and overflowing results take the per-row kernel's
+// steps (RN of the top 64 bits, then scale_exp), so every result is bit for bit that kernel's.
+__device__ __forceinline__ double crt_round_magnitude(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3, int escale) {
   const bool negative = int(r3) < 0;
   // |R| = (hi64, lo64)
   unsigned long long lo64 = (static_cast<unsigned long long>(r1) << 32) | r0;
@@ -1038,6 +1035,98 @@ __device__ __forceinline__ double crt_round(uint32_t r0, uint32_t r1, uint32_t r
   return __longlong_as_double(static_cast<long long>(bits));
 }
 
+// RN(R 2^escale) for R = (r3 r2 r1 r0) in 128-bit two's complement, congruent to C' modulo P
+// and within one P of [-P/2, P/2).  The range fix runs only when R's top 64-bit window does
+// not already place it in [-P/2, P/2).  Then, with hi = the signed 64-bit window of R at limbs
+// kW, kW+1 (|R| < 2^(63 + 32 kW)) and lo the limbs below it, R = hi 2^(32 kW) + lo, and two
+// one-rounding forms cover all but tiny |R|:
+//   * |hi| >= 2^54: RN(hi | [lo != 0]) 2^(32 kW).  The sticky bit sits below the guard bit
+//     (hi has at least 55 significant bits), and hi and hi | 1 lie strictly between the same
+//     two even integers, so both round like R;
+//   * 8 <= |hi| < 2^54: R = h 2^(32 kW + 1) + X with h = hi >> 1 (|h| < 2^53, exact in a
+//     double) and X = (hi & 1) 2^(32 kW) + lo.  For kW = 1, X < 2^33 is exact and
+//     RN(R) = fma(h, 2^33, X).  For kW = 2, X >> 12 with a sticky bit in its lowest place is
+//     below 2^53 and exact, and R, at least 2^67 in magnitude, has its guard bit at 2^13 or
+//     above, so RN(R) = fma(h, 2^53, (X >> 12) | [X mod 2^12 != 0]) 2^12;
+//   * kW = 0 (P < 2^64): R = hi exactly.
+// The result is scaled by adding to the exponent field when it stays normal.  Everything else
+// (|hi| < 8, subnormal or overflowing results) takes crt_round_magnitude, the per-row kernel's
+// steps, so every result is bit for bit that kernel's.
+template <int N>
+__device__ __forceinline__ double crt_round(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3, int escale) {
+  constexpr uint32_t P0 = kCrtTableC.P[N][0], P1 = kCrtTableC.P[N][1], P2 = kCrtTableC.P[N][2], P3 = kCrtTableC.P[N][3];
+  // R lies in [-half, half) when the 64-bit window of R at half's two top limbs is in
+  // [-Hw, Hw) and the limbs above the window extend its sign: nothing to fix then
+  constexpr int kW = kCrtTableC.half[N][3] != 0 ? 2 : (kCrtTableC.half[N][2] != 0 ? 1 : 0);
+  constexpr long long Hw = static_cast<long long>((static_cast<unsigned long long>(kCrtTableC.half[N][kW + 1]) << 32) |
+                                                  kCrtTableC.half[N][kW]);
+  const uint32_t rl[4] = {r0, r1, r2, r3};
+  const long long win = static_cast<long long>((static_cast<unsigned long long>(rl[kW + 1]) << 32) | rl[kW]);
+  const uint32_t ext = win < 0 ? 0xFFFFFFFFu : 0u;
+  bool in_range = win >= -Hw && win < Hw;
+#pragma unroll
+  for (int t = kW + 2; t < 4; ++t) in_range = in_range && rl[t] == ext;
+  if (!in_range) {
+    using u128 = unsigned __int128;
+    using s128 = __int128;
+    const u128 P = (u128(P3) << 96) | (u128(P2) << 64) | (u128(P1) << 32) | u128(P0);
+    const s128 half = s128(P >> 1);
+    s128 r = s128((u128(r3) << 96) | (u128(r2) << 64) | (u128(r1) << 32) | u128(r0));
+    if (r > half)
+      r -= s128(P);
+    else if (r < -half)
+      r += s128(P);
+    const u128 ur = u128(r);
+    r0 = uint32_t(ur);
+    r1 = uint32_t(ur >> 32);
+    r2 = uint32_t(ur >> 64);
+    r3 = uint32_t(ur >> 96);
+  }
+  const uint32_t rl2[4] = {r0, r1, r2, r3};
+  const long long hi = static_cast<long long>((static_cast<unsigned long long>(rl2[kW + 1]) << 32) | rl2[kW]);
+  double d;
+  int s;
+  bool fast;
+  if constexpr (kW == 0) {
+    d = __ll2double_rn(hi);
+    s = 0;
+    fast = hi != 0;
+  } else if constexpr (kW == 1) {
+    if (static_cast<unsigned long long>(hi + (1ll << 54)) >= (1ull << 55)) {
+      d = __ll2double_rn(hi | (r0 != 0u ? 1ll : 0ll));
+      s = 32;
+    } else {
+      const long long h = hi >> 1;
+      const unsigned long long X = (static_cast<unsigned long long>(hi & 1) << 32) | r0;
+      d = fma(__ll2double_rn(h), 0x1p33, __ull2double_rn(X));
+      s = 0;
+    }
+    fast = static_cast<unsigned long long>(hi + 8) >= 16ull;
+  } else {
+    if (static_cast<unsigned long long>(hi + (1ll << 54)) >= (1ull << 55)) {
+      d = __ll2double_rn(hi | ((r0 | r1) != 0u ? 1ll : 0ll));
+      s = 64;
+    } else {
+      const long long h = hi >> 1;
+      // x = (X >> 12) | sticky = (hi & 1) 2^52 + X', X' = (lo >> 12) | [lo mod 2^12 != 0] below
+      // 2^52: the bits of 2^52 + X' assembled directly, minus 2^52 unless hi is odd (exact)
+      const uint32_t xlo = (r1 << 20) | (r0 >> 12) | ((r0 & 0xFFFu) != 0u ? 1u : 0u);
+      const double x = __hiloint2double(static_cast<int>(0x43300000u | (r1 >> 12)), static_cast<int>(xlo)) -
+                       ((hi & 1) != 0 ? 0.0 : 0x1p52);
+      d = fma(__ll2double_rn(h), 0x1p53, x);
+      s = 12;
+    }
+    fast = static_cast<unsigned long long>(hi + 8) >= 16ull;
+  }
+  const int k = s + escale;
+  const int hw = __double2hiint(d);
+  const int be = ((hw >> 20) & 0x7FF) + k;  // biased exponent of d 2^k
+  if (fast && static_cast<unsigned>(be - 1) < 2046u)
+    return __hiloint2double(static_cast<int>(static_cast<unsigned>(hw) + (static_cast<unsigned>(k) << 20)),
+                            __double2loint(d));
+  return crt_round_magnitude(r0, r1, r2, r3, escale);
+}
+
 // RN(C' 2^escale) from S = sum_q acc[q] 2^(32q), limb columns below 2^52 (the tensor-core sum
 // gives columns below 2^46): the columns are exact doubles by one integer add and one FP64
 // subtraction, q = rint(S / P) comes from acc[1..3] (acc[0] / P < 2^-11 left out; q is off
@@ -1065,12 +1154,12 @@ __device__ __forceinline__ double crt_finish_small(const unsigned long long (&ac
 // ---- reconstruction with the weighted residue sum on the tensor cores
 // S = sum_l r_l W_l = sum_b 2^(8b) T_b with T_b = sum_l r_l w_lb, w_lb byte b of W_l (W_l < P <
 // 2^128: 16 bytes) and T_b < 16 * 255 * 255 < 2^20: a [32 entries x 16 moduli] x [16 moduli x 16
-// bytes] product of unsigned bytes with exact INT32 sums, four mma.sync m16n8k16 per warp.
+// bytes] product of unsigned bytes with exact INT32 sums, four mma.sync m16n8k16 per warp, each
+// from a zero accumulator.
 __device__ __forceinline__ void mma_u8_16x8x16(int (&d)[4], uint32_t a0, uint32_t a1, uint32_t b0) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.s32.u8.u8.s32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
-      : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
-      : "r"(a0), "r"(a1), "r"(b0));
+  asm("mma.sync.aligned.m16n8k16.row.col.s32.u8.u8.s32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%7,%7,%7,%7};"
+      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3])
+      : "r"(a0), "r"(a1), "r"(b0), "r"(0));
 }
 
 // Rows i0 .. i0+31 of one column per warp.  Lane (g, c) = (lane / 4, lane % 4) loads moduli
@@ -1141,7 +1230,7 @@ __global__ void __launch_bounds__(256, 4) crt_reconstruct_mma_kernel(const __gri
       const uint32_t v0 = __byte_perm(t0, t2, 0x5410), v1 = __byte_perm(t0, t2, 0x7632);
       const uint32_t v2 = __byte_perm(t1, t3, 0x5410), v3 = __byte_perm(t1, t3, 0x7632);
       // rows 4g+0 / 4g+1 (MMA row slots g / g+8), then rows 4g+2 / 4g+3; bytes 0..7, then 8..15
-      int d0[4] = {0, 0, 0, 0}, d1[4] = {0, 0, 0, 0}, d2[4] = {0, 0, 0, 0}, d3[4] = {0, 0, 0, 0};
+      int d0[4], d1[4], d2[4], d3[4];  // the byte sums start from zero (C operand 0)
       mma_u8_16x8x16(d0, v0, v1, bfrag[0]);
       mma_u8_16x8x16(d1, v0, v1, bfrag[1]);
       mma_u8_16x8x16(d2, v2, v3, bfrag[0]);

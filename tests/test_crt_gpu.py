@@ -100,6 +100,60 @@ def test_crt_subnormal_and_huge_rows():
     assert np.all(Cg[2, :n] == 0.0) and np.all(Cg[:m, 3] == 0.0)
 
 
+def _rounding_operands(m, n, rng):
+    """op(A) (m x 4) and op(B) (4 x n) with C_ij = y_i x_j + z_i w_j exactly: the first two
+    products cancel (1 - 1), y_i = 2^-a_i (1 + 2^-c_i) and x_j = 2^-f_j (1 + 2^-d_j), so C'
+    has its top bit where the row and column scales put it and its lowest bit c_i + d_j below
+    that: c_i + d_j = 53 is a rounding tie (to even unless c_i or d_j is 52); the lone bit
+    z_i w_j below it, in half of the rows, makes it a sticky bit instead.  The column
+    exponents f_j spread |C'| over every magnitude window of the rounding, zero rows included."""
+    c = rng.integers(1, 53, size=m)
+    y = 2.0 ** -rng.integers(0, 3, size=m) * (1 + 2.0 ** -c)
+    y[rng.random(m) < 0.05] = 0.0
+    z = np.where(rng.random(m) < 0.5, 2.0 ** -rng.integers(56, 60, size=m), 0.0)
+    d = rng.integers(1, 53, size=n)
+    f = np.array([rng.integers(0, 59 - dj) for dj in d])
+    x = 2.0 ** -f * (1 + 2.0 ** -d)
+    w = 2.0 ** -rng.integers(0, 3, size=n)
+    sign = rng.choice([-1.0, 1.0], size=m)
+    A = np.asfortranarray(np.stack([np.ones(m), -np.ones(m), sign * y, z], axis=1))
+    B = np.asfortranarray(np.stack([np.ones(n), np.ones(n), x, w], axis=0))
+    return A, B
+
+
+@pytest.mark.parametrize("moduli", [16, 11, 8])
+def test_crt_rounds_ties_and_sticky_bits_exactly(moduli):
+    """C' on exact ties (rounded to even), one sticky bit above a tie, and every magnitude
+    window of the rounding (with 16 moduli: |C'| from below 2^67 up to P/2; 11 and 8 moduli
+    take the narrower windows): bit for bit the model, which rounds the exact integer once."""
+    m, n, k = 96, 80, 4
+    rng = np.random.default_rng(23)
+    A, B = _rounding_operands(m, n, rng)
+    model = crt_model()
+    b = model.bits(moduli)
+    _, Ai = model.scaled_integers(A, b)
+    _, Bi = model.scaled_integers(B.T, b)
+    Cp = Ai.dot(Bi.T)
+    lengths = np.vectorize(lambda x: abs(int(x)).bit_length())(Cp)
+
+    def tie(x):
+        x = abs(int(x))
+        L = x.bit_length()
+        return L > 54 and x & ((1 << (L - 53)) - 1) == 1 << (L - 54)
+
+    if moduli == 16:
+        assert int(np.vectorize(tie)(Cp).sum()) >= 10
+        assert (lengths >= 119).sum() > 0 and ((lengths >= 68) & (lengths < 119)).sum() > 0
+        assert ((lengths > 0) & (lengths < 68)).sum() > 0
+    eb.set_dgemm_moduli(moduli)
+    eb.set_dgemm_tolerance(1.0)
+    C = np.asfortranarray(rng.standard_normal((m, n)))
+    for beta in (0.0, -0.5):
+        rc, Cg = _device_call("N", "N", m, n, k, 1.0, A, m, B, k, beta, C, m, check=False)
+        assert rc == eb.EB2_OK
+        np.testing.assert_array_equal(Cg, _model(A, "N", B, "N", m, n, k, 1.0, beta, C, moduli))
+
+
 @pytest.mark.parametrize("tile_n", [0, 1024])
 def test_crt_long_k_accumulates_in_chunks(tile_n):
     """K beyond one exact INT32 unit (1023 x 128): the epilogue adds residues mod p (with the
