@@ -800,6 +800,7 @@ __device__ __forceinline__ void crt_reduce_energies(const CrtRecParams& R, doubl
 }
 
 constexpr int kRecCols = 8;  // most columns per block and pass
+static_assert(kRecCols <= 32, "the estimate's column sum takes a lane per column");
 
 // One thread per row i, cols_per_block columns per pass: C'_ij from its residues, then C_ij.
 __global__ void __launch_bounds__(256) crt_reconstruct_kernel(const __grid_constant__ CrtRecParams R) {
@@ -1162,21 +1163,31 @@ __device__ __forceinline__ void mma_u8_16x8x16(int (&d)[4], uint32_t a0, uint32_
       : "r"(a0), "r"(a1), "r"(b0), "r"(0));
 }
 
-// Rows i0 .. i0+31 of one column per warp.  Lane (g, c) = (lane / 4, lane % 4) loads moduli
-// 4c .. 4c+3 at rows i0 + 4g .. i0 + 4g + 3 (one 32-bit word per modulus), transposes the
-// 4 x 4 bytes so that each word holds the four moduli of one row (the A fragment rows), and
+// Rows i0 .. i0+31 of one column per warp.  The warp streams the residues of its columns
+// through its own ring of kRecStages shared-memory slots (a column's 16 moduli x 32 rows, 512
+// bytes), kRecStages - 1 columns ahead with 16-byte cp.async copies (lane L copies rows
+// 16 (L & 1) .. +15 of modulus L / 2): four times the bytes in flight of register loads one
+// column ahead, which left the kernel waiting on memory.  Lane (g, c) = (lane / 4, lane % 4)
+// reads moduli 4c .. 4c+3 at rows i0 + 4g .. i0 + 4g + 3 (one 32-bit word per modulus; the
+// slot's words are swizzled, word w at w ^ ((w >> 2) & 0x18), so that these reads hit 32
+// distinct banks), transposes the 4 x 4 bytes so that each word holds the four moduli of one
+// row (the A fragment rows), and
 // the MMAs leave with lane (g, c) the byte sums T_2c, T_2c+1, T_8+2c, T_9+2c of those four
 // rows.  The warp passes them through its own rows of shared memory so that lane L reads all
 // sixteen sums of row i0 + L and forms S in four 32-bit-aligned columns with multiply-adds;
 // the tail (crt_finish_small) and the store follow.  Bit for bit the per-row kernel: S is the
 // same integer and it is rounded the same way.
 constexpr int kRecStageStride = 18;  // words per staged row (16 byte sums + 2)
+constexpr int kRecStages = 4;        // columns of residues in each warp's ring
+__device__ __forceinline__ int rec_swizzle(int w) { return w ^ ((w >> 2) & 0x18); }
 template <int N, bool EST>
 __global__ void __launch_bounds__(256, 4) crt_reconstruct_mma_kernel(const __grid_constant__ CrtRecParams R) {
   static_assert(N >= kCrtMinModuli && N <= 16, "16 moduli per MMA K step");
   __shared__ __align__(16) uint32_t stage[8][32 * kRecStageStride];
+  __shared__ __align__(16) uint32_t ring[8][kRecStages][128];
   if (R.skip_if_flag && *R.skip_if_flag) return;
   uint32_t* const wstage = stage[threadIdx.x >> 5];
+  const uint32_t (*const wring)[128] = ring[threadIdx.x >> 5];
   CrtStoreCtx sc = store_ctx(R);
   const uint8_t* const res = R.res;
   const int64_t ld_res = R.ld_res, plane = R.plane, m = R.m, ncols = R.ncols;
@@ -1202,7 +1213,14 @@ __global__ void __launch_bounds__(256, 4) crt_reconstruct_mma_kernel(const __gri
   }
   const int mu_i = i < m ? sc.mu_a[i] : kCrtZeroRow;
   double e_acc = 0.0, v_acc = 0.0;
-  const uint8_t* const rbase = res + i0 + 4 * g + int64_t(4 * c) * plane;
+  // copies: lane L takes rows 16 (L & 1) .. +15 of modulus L / 2 (16-byte aligned: the planes,
+  // the leading dimension and i0 are multiples of 16)
+  const bool copier = (lane >> 1) < N;
+  const uint8_t* const cbase = res + i0 + 16 * (lane & 1) + int64_t(lane >> 1) * plane;
+  const uint32_t cdst = smem_u32(&wring[0][rec_swizzle(8 * (lane >> 1) + 4 * (lane & 1))]);
+  int rword[4];  // this lane's four words of a slot
+#pragma unroll
+  for (int k = 0; k < 4; ++k) rword[k] = rec_swizzle(8 * (4 * c + k) + g);
   const int cpb = R.cols_per_block;
   const int64_t jstep = int64_t(gridDim.y) * cpb;
   for (int64_t j0 = int64_t(blockIdx.y) * cpb; i0 < m && j0 < ncols; j0 += jstep) {
@@ -1211,19 +1229,41 @@ __global__ void __launch_bounds__(256, 4) crt_reconstruct_mma_kernel(const __gri
     if (uplo == 1 && jb < i0) jb = i0;            // i <= j
     if (uplo == 2 && j1 > i0 + 32) j1 = i0 + 32;  // i >= j
     if (jb >= j1) continue;
-    uint32_t wn[4];
+    if (EST && uplo == 0) {
+      // sum_j 2^(2(b - mu_i - nu_j)) over the pass's nonzero columns = 2^(2(b - mu_i - nu_min))
+      // sum_j 2^(-2(nu_j - nu_min)): the column sum is the same for every row of the warp, so
+      // lane t takes column jb + t (at most kRecCols of them) and the warp adds them up
+      const int cnt = int(j1 - jb);
+      const int nu = lane < cnt ? sc.mu_b[jb + lane] : kCrtZeroRow;
+      const bool nz = nu != kCrtZeroRow;
+      const int nu_min = __reduce_min_sync(0xffffffffu, nz ? nu : INT_MAX);
+      double t = nz ? exp2_int(-2 * (nu - nu_min)) : 0.0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-      wn[k] = 4 * c + k < N ? __ldg(reinterpret_cast<const uint32_t*>(rbase + jb * ld_res + k * plane)) : 0u;
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (mu_i != kCrtZeroRow && nu_min != INT_MAX) e_acc = fma(exp2_int(2 * (sc.b - mu_i - nu_min)), t, e_acc);
+    }
+    // one commit group per column (empty past j1), so that waiting for all but the newest
+    // kRecStages - 1 groups leaves column j landed; every lane reads a slot before the
+    // __syncwarp that precedes any copy into it
+#pragma unroll
+    for (int t = 0; t < kRecStages - 1; ++t) {
+      if (copier && jb + t < j1) cp_async_16(cdst + t * 512u, cbase + (jb + t) * ld_res);
+      cp_async_commit();
+    }
+    int slot = 0;
     for (int64_t j = jb; j < j1; ++j) {
+      {
+        const int64_t jn = j + kRecStages - 1;
+        const int sn = slot == 0 ? kRecStages - 1 : slot - 1;  // (slot + kRecStages - 1) % kRecStages
+        if (copier && jn < j1) cp_async_16(cdst + uint32_t(sn) * 512u, cbase + jn * ld_res);
+        cp_async_commit();
+      }
+      cp_async_wait<kRecStages - 1>();
+      __syncwarp();
       uint32_t w[4];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) w[k] = wn[k];
-      if (j + 1 < j1) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-          wn[k] = 4 * c + k < N ? __ldg(reinterpret_cast<const uint32_t*>(rbase + (j + 1) * ld_res + k * plane)) : 0u;
-      }
+      for (int k = 0; k < 4; ++k) w[k] = 4 * c + k < N ? wring[slot][rword[k]] : 0u;
+      slot = slot == kRecStages - 1 ? 0 : slot + 1;
       // 4 x 4 byte transpose: w[k] byte e (modulus 4c+k, row 4g+e) -> v[e] byte k
       const uint32_t t0 = __byte_perm(w[0], w[1], 0x5140), t1 = __byte_perm(w[0], w[1], 0x7362);
       const uint32_t t2 = __byte_perm(w[2], w[3], 0x5140), t3 = __byte_perm(w[2], w[3], 0x7362);
@@ -1265,7 +1305,7 @@ __global__ void __launch_bounds__(256, 4) crt_reconstruct_mma_kernel(const __gri
       const int nu_j = sc.mu_b[j];
       const double v = __dmul_rn(sc.alpha, crt_finish_small<N>(acc, P_inv32, -mu_i - nu_j));
       if (EST) {
-        if (mu_i != kCrtZeroRow && nu_j != kCrtZeroRow) e_acc += exp2_int(2 * (sc.b - mu_i - nu_j));
+        if (uplo != 0 && mu_i != kCrtZeroRow && nu_j != kCrtZeroRow) e_acc += exp2_int(2 * (sc.b - mu_i - nu_j));
         v_acc += v * v;
       }
       if (sc.write_c) {
@@ -1478,10 +1518,10 @@ cudaError_t launch_crt_reconstruct(const CrtReconstructArgs& args, cudaStream_t 
   R.save = args.save;
   R.ld_save = args.ld_save;
   R.uplo = args.uplo;
-  // the tensor-core sum: whole warps of 32 rows read the residue planes 32 bits at a time, so
-  // the planes must be 4-byte aligned and hold every row of those warps
-  const bool mma = args.moduli >= kCrtMinModuli && args.moduli <= 16 && reinterpret_cast<uintptr_t>(args.cres) % 4 == 0 &&
-                   args.ld_res % 32 == 0 && args.plane % 4 == 0 && args.ld_res >= (args.m + 31) / 32 * 32;
+  // the tensor-core sum: whole warps of 32 rows copy the residue planes 16 bytes at a time, so
+  // the planes must be 16-byte aligned and hold every row of those warps
+  const bool mma = args.moduli >= kCrtMinModuli && args.moduli <= 16 && reinterpret_cast<uintptr_t>(args.cres) % 16 == 0 &&
+                   args.ld_res % 32 == 0 && args.plane % 16 == 0 && args.ld_res >= (args.m + 31) / 32 * 32;
   const int64_t rows_per_block = 256;
   const unsigned gx = unsigned((args.m + rows_per_block - 1) / rows_per_block);
   // up to kRecCols columns per block, fewer while the grid is under ~4 blocks per SM

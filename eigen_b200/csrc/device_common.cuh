@@ -319,6 +319,10 @@ __device__ __forceinline__ void cp_async_mbar_arrive(uint64_t* bar) {
   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// 16 bytes global -> shared through L2 only (both addresses 16-byte aligned)
+__device__ __forceinline__ void cp_async_16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+}
 // one element global -> shared, zero-filled when !valid (nothing is read then)
 template <int BYTES>
 __device__ __forceinline__ void cp_async_elem(uint32_t dst, const void* src, bool valid) {
