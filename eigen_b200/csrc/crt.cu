@@ -1173,20 +1173,24 @@ __device__ __forceinline__ void mma_u8_16x8x16(int (&d)[4], uint32_t a0, uint32_
 // distinct banks), transposes the 4 x 4 bytes so that each word holds the four moduli of one
 // row (the A fragment rows), and
 // the MMAs leave with lane (g, c) the byte sums T_2c, T_2c+1, T_8+2c, T_9+2c of those four
-// rows.  The warp passes them through its own rows of shared memory so that lane L reads all
-// sixteen sums of row i0 + L and forms S in four 32-bit-aligned columns with multiply-adds;
-// the tail (crt_finish_small) and the store follow.  Bit for bit the per-row kernel: S is the
-// same integer and it is rounded the same way.
-constexpr int kRecStageStride = 18;  // words per staged row (16 byte sums + 2)
+// rows.  The lane packs them in pairs, X_c = T_2c + 2^8 T_2c+1 and Y_c = T_8+2c + 2^8 T_9+2c
+// (each below 2^29), and the warp passes the pairs through its own rows of shared memory (two
+// buffers, alternating by column, so that writing one never waits for the reads of the
+// other) so that lane L reads the eight of row i0 + L and forms S in four 32-bit-aligned
+// columns, X_0 + 2^16 X_1, X_2 + 2^16 X_3, Y_0 + 2^16 Y_1, Y_2 + 2^16 Y_3; the tail
+// (crt_finish_small) and the store follow.  Bit for bit the per-row kernel: S is the same
+// integer and it is rounded the same way.
+constexpr int kRecStageStride = 10;  // words per staged row: X_0 Y_0 .. X_3 Y_3 and 2 of padding
 constexpr int kRecStages = 4;        // columns of residues in each warp's ring
 __device__ __forceinline__ int rec_swizzle(int w) { return w ^ ((w >> 2) & 0x18); }
 template <int N, bool EST>
 __global__ void __launch_bounds__(256, 4) crt_reconstruct_mma_kernel(const __grid_constant__ CrtRecParams R) {
   static_assert(N >= kCrtMinModuli && N <= 16, "16 moduli per MMA K step");
-  __shared__ __align__(16) uint32_t stage[8][32 * kRecStageStride];
+  __shared__ __align__(16) uint32_t stage[8][2][32 * kRecStageStride];
   __shared__ __align__(16) uint32_t ring[8][kRecStages][128];
   if (R.skip_if_flag && *R.skip_if_flag) return;
-  uint32_t* const wstage = stage[threadIdx.x >> 5];
+  uint32_t (*const wstage)[32 * kRecStageStride] = stage[threadIdx.x >> 5];
+  int sbuf = 0;
   const uint32_t (*const wring)[128] = ring[threadIdx.x >> 5];
   CrtStoreCtx sc = store_ctx(R);
   const uint8_t* const res = R.res;
@@ -1275,31 +1279,27 @@ __global__ void __launch_bounds__(256, 4) crt_reconstruct_mma_kernel(const __gri
       mma_u8_16x8x16(d1, v0, v1, bfrag[1]);
       mma_u8_16x8x16(d2, v2, v3, bfrag[0]);
       mma_u8_16x8x16(d3, v2, v3, bfrag[1]);
-      // byte sums of rows 4g+e through the warp's shared-memory rows (stride 18 words: the
-      // 64-bit reads below are free of bank conflicts): row 4g+e, words 2c, 2c+1 (bytes 0..7
-      // half) and 8+2c, 9+2c (bytes 8..15 half)
+      // (X_c, Y_c) of rows 4g+e to words 2c, 2c+1 of those rows (stride 10 words: the 64-bit
+      // writes of a half-warp and the 64-bit reads below hit distinct banks)
+      uint32_t* w0 = wstage[sbuf] + (4 * g) * kRecStageStride + 2 * c;
+      *reinterpret_cast<uint2*>(w0) = make_uint2(uint32_t(d0[0]) + uint32_t(d0[1]) * 256u,
+                                                 uint32_t(d1[0]) + uint32_t(d1[1]) * 256u);
+      *reinterpret_cast<uint2*>(w0 + kRecStageStride) = make_uint2(uint32_t(d0[2]) + uint32_t(d0[3]) * 256u,
+                                                                   uint32_t(d1[2]) + uint32_t(d1[3]) * 256u);
+      *reinterpret_cast<uint2*>(w0 + 2 * kRecStageStride) = make_uint2(uint32_t(d2[0]) + uint32_t(d2[1]) * 256u,
+                                                                       uint32_t(d3[0]) + uint32_t(d3[1]) * 256u);
+      *reinterpret_cast<uint2*>(w0 + 3 * kRecStageStride) = make_uint2(uint32_t(d2[2]) + uint32_t(d2[3]) * 256u,
+                                                                       uint32_t(d3[2]) + uint32_t(d3[3]) * 256u);
       __syncwarp();
-      uint32_t* w0 = wstage + (4 * g) * kRecStageStride + 2 * c;
-      *reinterpret_cast<uint2*>(w0) = make_uint2(uint32_t(d0[0]), uint32_t(d0[1]));
-      *reinterpret_cast<uint2*>(w0 + 8) = make_uint2(uint32_t(d1[0]), uint32_t(d1[1]));
-      *reinterpret_cast<uint2*>(w0 + kRecStageStride) = make_uint2(uint32_t(d0[2]), uint32_t(d0[3]));
-      *reinterpret_cast<uint2*>(w0 + kRecStageStride + 8) = make_uint2(uint32_t(d1[2]), uint32_t(d1[3]));
-      *reinterpret_cast<uint2*>(w0 + 2 * kRecStageStride) = make_uint2(uint32_t(d2[0]), uint32_t(d2[1]));
-      *reinterpret_cast<uint2*>(w0 + 2 * kRecStageStride + 8) = make_uint2(uint32_t(d3[0]), uint32_t(d3[1]));
-      *reinterpret_cast<uint2*>(w0 + 3 * kRecStageStride) = make_uint2(uint32_t(d2[2]), uint32_t(d2[3]));
-      *reinterpret_cast<uint2*>(w0 + 3 * kRecStageStride + 8) = make_uint2(uint32_t(d3[2]), uint32_t(d3[3]));
-      __syncwarp();
-      // this lane's row: S = sum_b T_b 2^(8b) as four 32-bit-aligned columns (each < 2^45)
-      unsigned long long acc[4];
-      const uint32_t* rrow = wstage + lane * kRecStageStride;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const uint2 p0 = *reinterpret_cast<const uint2*>(rrow + 4 * q);
-        const uint2 p1 = *reinterpret_cast<const uint2*>(rrow + 4 * q + 2);
-        const uint32_t low = p0.x + p0.y * 256u;  // < 2^29
-        acc[q] = static_cast<unsigned long long>(p1.x) * 65536ull + low;
-        acc[q] += static_cast<unsigned long long>(p1.y) * 16777216ull;
-      }
+      // this lane's row: S = sum_b T_b 2^(8b) as four 32-bit-aligned columns (each < 2^46)
+      const uint32_t* rrow = wstage[sbuf] + lane * kRecStageStride;
+      sbuf ^= 1;
+      const uint2 q0 = *reinterpret_cast<const uint2*>(rrow), q1 = *reinterpret_cast<const uint2*>(rrow + 2);
+      const uint2 q2 = *reinterpret_cast<const uint2*>(rrow + 4), q3 = *reinterpret_cast<const uint2*>(rrow + 6);
+      const unsigned long long acc[4] = {static_cast<unsigned long long>(q1.x) * 65536ull + q0.x,
+                                         static_cast<unsigned long long>(q3.x) * 65536ull + q2.x,
+                                         static_cast<unsigned long long>(q1.y) * 65536ull + q0.y,
+                                         static_cast<unsigned long long>(q3.y) * 65536ull + q2.y};
       const bool keep = i < m && (uplo == 0 || (uplo == 1 ? i <= j : i >= j));
       if (!keep) continue;
       const int nu_j = sc.mu_b[j];
