@@ -1249,17 +1249,21 @@ __global__ void __launch_bounds__(256, 4) crt_reconstruct_mma_kernel(const __gri
     // one commit group per column (empty past j1), so that waiting for all but the newest
     // kRecStages - 1 groups leaves column j landed; every lane reads a slot before the
     // __syncwarp that precedes any copy into it
+    // (32-bit column offsets jj from jb and pointers stepped by their leading dimensions)
+    const int cnt = int(j1 - jb);
+    const uint8_t* csrc = cbase + jb * ld_res;
 #pragma unroll
-    for (int t = 0; t < kRecStages - 1; ++t) {
-      if (copier && jb + t < j1) cp_async_16(cdst + t * 512u, cbase + (jb + t) * ld_res);
+    for (int t = 0; t < kRecStages - 1; ++t, csrc += ld_res) {
+      if (copier && t < cnt) cp_async_16(cdst + t * 512u, csrc);
       cp_async_commit();
     }
+    double* cp = sc.C + jb * sc.ldc + i;
+    const int32_t* const nup = sc.mu_b + jb;
     int slot = 0;
-    for (int64_t j = jb; j < j1; ++j) {
+    for (int jj = 0; jj < cnt; ++jj, csrc += ld_res, cp += sc.ldc) {
       {
-        const int64_t jn = j + kRecStages - 1;
         const int sn = slot == 0 ? kRecStages - 1 : slot - 1;  // (slot + kRecStages - 1) % kRecStages
-        if (copier && jn < j1) cp_async_16(cdst + uint32_t(sn) * 512u, cbase + jn * ld_res);
+        if (copier && jj + kRecStages - 1 < cnt) cp_async_16(cdst + uint32_t(sn) * 512u, csrc);
         cp_async_commit();
       }
       cp_async_wait<kRecStages - 1>();
@@ -1300,16 +1304,16 @@ __global__ void __launch_bounds__(256, 4) crt_reconstruct_mma_kernel(const __gri
                                          static_cast<unsigned long long>(q3.x) * 65536ull + q2.x,
                                          static_cast<unsigned long long>(q1.y) * 65536ull + q0.y,
                                          static_cast<unsigned long long>(q3.y) * 65536ull + q2.y};
+      const int64_t j = jb + jj;
       const bool keep = i < m && (uplo == 0 || (uplo == 1 ? i <= j : i >= j));
       if (!keep) continue;
-      const int nu_j = sc.mu_b[j];
+      const int nu_j = nup[jj];
       const double v = __dmul_rn(sc.alpha, crt_finish_small<N>(acc, P_inv32, -mu_i - nu_j));
       if (EST) {
         if (uplo != 0 && mu_i != kCrtZeroRow && nu_j != kCrtZeroRow) e_acc += exp2_int(2 * (sc.b - mu_i - nu_j));
         v_acc += v * v;
       }
       if (sc.write_c) {
-        double* cp = sc.C + j * sc.ldc + i;
         if (sc.beta == 0.0) {
           *cp = v;
         } else {
