@@ -420,8 +420,7 @@ __device__ __forceinline__ void store_residues_wide(const CrtModConst& k, const 
 }
 
 // An entry t = trunc(2^mu x) with |t| <= 2^62 (at most 16 moduli) as hi 2^32 + lo (hi signed,
-// lo unsigned) and as the exact doubles of hi and lo.  1.5 2^52 + k has the bit pattern of
-// 1.5 2^52 plus k for |k| < 2^51, so each conversion is one integer add and one FP64 add.
+// lo unsigned) and as the exact doubles of hi and lo.
 struct SplitEntry {
   int32_t hi;
   uint32_t lo;
@@ -431,8 +430,8 @@ __device__ __forceinline__ SplitEntry split_entry(long long t) {
   SplitEntry e;
   e.hi = int32_t(t >> 32);
   e.lo = uint32_t(t);
-  e.dh = __longlong_as_double(0x4338000000000000ll + e.hi) - 0x1.8p52;
-  e.dl = __longlong_as_double(0x4338000000000000ll + e.lo) - 0x1.8p52;
+  e.dh = __int2double_rn(e.hi);  // 32-bit integers convert exactly
+  e.dl = __uint2double_rn(e.lo);
   return e;
 }
 
@@ -549,10 +548,20 @@ __global__ void __launch_bounds__(kSplitThreadsCrt, 3) crt_split_kernel(
       for (int l = 0; l < n; ++l) store_residues_wide(kModConst[l], ch, neg, dst + size_t(l) * plane);
     } else {
       SplitEntry e[kSplitEntries];
-      const double f1 = exp2_int(m / 2), f2 = exp2_int(m - m / 2);  // scale2(., m) factors
+      if (m >= -1022 && m <= 1023) {
+        // 2^m is a normal double: one product.  It is exact where the two-step scale2 is exact,
+        // and where a tiny x makes scale2's first product round, |2^m x| < 1 and the
+        // truncation is 0 either way
+        const double f = __hiloint2double((m + 1023) << 20, 0);
 #pragma unroll
-      for (int j = 0; j < kSplitEntries; ++j)
-        e[j] = split_entry(__double2ll_rz(__dmul_rn(__dmul_rn(tile[rr][cb + j], f1), f2)));  // trunc
+        for (int j = 0; j < kSplitEntries; ++j)
+          e[j] = split_entry(__double2ll_rz(__dmul_rn(tile[rr][cb + j], f)));  // trunc
+      } else {
+        const double f1 = exp2_int(m / 2), f2 = exp2_int(m - m / 2);  // scale2(., m) factors
+#pragma unroll
+        for (int j = 0; j < kSplitEntries; ++j)
+          e[j] = split_entry(__double2ll_rz(__dmul_rn(__dmul_rn(tile[rr][cb + j], f1), f2)));  // trunc
+      }
       if constexpr (NT > 0) {
         store_residues_static<0, NT>(e, dst, plane);
       } else {
