@@ -1174,21 +1174,19 @@ __device__ __forceinline__ void mma_u8_16x8x16(int (&d)[4], uint32_t a0, uint32_
 
 // Rows i0 .. i0+31 of one column per warp.  The warp streams the residues of its columns
 // through its own ring of kRecStages shared-memory slots (a column's 16 moduli x 32 rows, 512
-// bytes), kRecStages - 1 columns ahead with 16-byte cp.async copies (lane L copies rows
-// 16 (L & 1) .. +15 of modulus L / 2): four times the bytes in flight of register loads one
-// column ahead, which left the kernel waiting on memory.  Lane (g, c) = (lane / 4, lane % 4)
-// reads moduli 4c .. 4c+3 at rows i0 + 4g .. i0 + 4g + 3 (one 32-bit word per modulus; the
-// slot's words are swizzled, word w at w ^ ((w >> 2) & 0x18), so that these reads hit 32
-// distinct banks), transposes the 4 x 4 bytes so that each word holds the four moduli of one
-// row (the A fragment rows), and
-// the MMAs leave with lane (g, c) the byte sums T_2c, T_2c+1, T_8+2c, T_9+2c of those four
-// rows.  The lane packs them in pairs, X_c = T_2c + 2^8 T_2c+1 and Y_c = T_8+2c + 2^8 T_9+2c
-// (each below 2^29), and the warp passes the pairs through its own rows of shared memory (two
-// buffers, alternating by column, so that writing one never waits for the reads of the
-// other) so that lane L reads the eight of row i0 + L and forms S in four 32-bit-aligned
-// columns, X_0 + 2^16 X_1, X_2 + 2^16 X_3, Y_0 + 2^16 Y_1, Y_2 + 2^16 Y_3; the tail
-// (crt_finish_small) and the store follow.  Bit for bit the per-row kernel: S is the same
-// integer and it is rounded the same way.
+// bytes), kRecStages - 1 columns ahead, with 16-byte cp.async copies (lane L copies rows
+// 16 (L & 1) .. +15 of modulus L / 2), so that no registers hold loads in flight.  Lane
+// (g, c) = (lane / 4, lane % 4) reads moduli 4c .. 4c+3 at rows i0 + 4g .. i0 + 4g + 3 (one
+// 32-bit word per modulus; the slot's words are swizzled, word w at w ^ ((w >> 2) & 0x18), so
+// that these reads hit 32 distinct banks) and transposes the 4 x 4 bytes so that each word
+// holds the four moduli of one row (the A fragment rows).  The MMAs leave with lane (g, c) the
+// byte sums T_2c, T_2c+1, T_8+2c, T_9+2c of those four rows.  The lane packs them in pairs,
+// X_c = T_2c + 2^8 T_2c+1 and Y_c = T_8+2c + 2^8 T_9+2c (each below 2^29), and the warp passes
+// the pairs through its own rows of shared memory (two buffers, alternating by column, so that
+// writing one never waits for the reads of the other), so that lane L reads the eight of row
+// i0 + L and forms S in four 32-bit-aligned columns, X_0 + 2^16 X_1, X_2 + 2^16 X_3,
+// Y_0 + 2^16 Y_1, Y_2 + 2^16 Y_3; the tail (crt_finish_small) and the store follow.  Bit for
+// bit the per-row kernel: S is the same integer and it is rounded the same way.
 constexpr int kRecStageStride = 10;  // words per staged row: X_0 Y_0 .. X_3 Y_3 and 2 of padding
 constexpr int kRecStages = 4;        // columns of residues in each warp's ring
 __device__ __forceinline__ int rec_swizzle(int w) { return w ^ ((w >> 2) & 0x18); }
