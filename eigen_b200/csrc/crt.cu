@@ -1139,17 +1139,25 @@ __device__ __forceinline__ double crt_round(uint32_t r0, uint32_t r1, uint32_t r
 
 // RN(C' 2^escale) from S = sum_q acc[q] 2^(32q), limb columns below 2^52 (the tensor-core sum
 // gives columns below 2^46): the columns are exact doubles by one integer add and one FP64
-// subtraction, q = rint(S / P) comes from acc[1..3] (acc[0] / P < 2^-11 left out; q is off
-// by one at most, which the range fix absorbs), and R = S - q P takes its borrows column by
-// column without carrying S first.
+// subtraction, q = rint(S / P) comes from acc[1..3] (acc[0] / P < 2^-11 left out), or from
+// acc[2..3] for 13 moduli and more (q is off by one at most either way, which the range fix
+// absorbs), and R = S - q P takes its borrows column by column without carrying S first.
 template <int N>
 __device__ __forceinline__ double crt_finish_small(const unsigned long long (&acc)[4], double P_inv32, int escale) {
   static_assert(N >= kCrtMinModuli && N <= 16, "P at least 2^63 and below 2^128");
   auto exact = [](unsigned long long x) {  // x < 2^52
     return __longlong_as_double(static_cast<long long>(x + 0x4330000000000000ull)) - 0x1p52;
   };
-  const double sd = fma(fma(exact(acc[3]), 0x1p32, exact(acc[2])), 0x1p32, exact(acc[1]));
-  const uint32_t q = uint32_t(__double2loint(fma(sd, P_inv32, 0x1.8p52)));
+  uint32_t q;
+  if constexpr (N >= 13) {
+    // P >= 2^102: acc[1] 2^32 + acc[0] < 2^79 moves S / P by less than 2^-23, so S / 2^64 is
+    // taken from acc[3] and acc[2] alone
+    const double sd = fma(exact(acc[3]), 0x1p32, exact(acc[2]));
+    q = uint32_t(__double2loint(fma(sd, P_inv32 * 0x1p32, 0x1.8p52)));
+  } else {
+    const double sd = fma(fma(exact(acc[3]), 0x1p32, exact(acc[2])), 0x1p32, exact(acc[1]));
+    q = uint32_t(__double2loint(fma(sd, P_inv32, 0x1.8p52)));
+  }
   constexpr uint32_t P0 = kCrtTableC.P[N][0], P1 = kCrtTableC.P[N][1], P2 = kCrtTableC.P[N][2], P3 = kCrtTableC.P[N][3];
   const long long d0 = static_cast<long long>(acc[0]) - static_cast<long long>(static_cast<unsigned long long>(q) * P0);
   const long long d1 = static_cast<long long>(acc[1]) - static_cast<long long>(static_cast<unsigned long long>(q) * P1) +
